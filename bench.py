@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the FDTD time-stepping path (courant.h cem_step).
+
+Workload (default, the every-kernel lossy 2-port configuration): a grounded
+coplanar waveguide on a Djordjevic-Sarkar substrate (eps_r 4.3, tan d 0.02 at
+1 GHz) fitted by 6 Debye poles, 35 um copper with Huray-rough surface
+impedance (sigma 5.8e7 S/m), a 20 um solder mask (eps_r 3.5), 2D eigenmode
+ports, on a 416 x 161 x 86 (5.76 M cell) non-uniform grid with 8-cell CPML,
+400 DFT frequencies to 40 GHz. Synthetic geometry generated here; fields
+start at zero.
+
+One benchmark step = `chunk` FDTD time steps (default 500, the run-control
+interval of the reference's GCPW driver). `value` = cell-updates per second
+(cells nx*ny*nz x time steps x ranks / max-over-ranks device time), timed
+with CUDA events on the engine's stream. The field state (~1.5 GB) exceeds
+L2, so no flush is needed between steps. `e2e` = the same metric through the
+C ABI for one whole excitation (40 000 steps) with the plan and state
+uploaded from host memory inside the timed region and the spectra read back
+to the host after every chunk.
+
+--impl reference times the reference's own CPU core (oracle/_ref, OpenMP on
+all host cores) on the same workload, a bounded sample of steps per
+benchmark step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    "c2": dict(desc="lossy GCPW 2-port: DS substrate (6 Debye poles), 35um Cu + Huray SIBC, 20um mask, mode ports",
+               kw=dict(hmin=10e-6, hmax=30e-6, dx=45e-6, yair=1.2e-3, zair=1.8e-3, tcu=35e-6, mask=20e-6,
+                       debye_poles=6, sigma_cu=5.8e7, huray=(0.5e-6, 2.0e11), modeports=True, steps=40000)),
+    "c1": dict(desc="lossless GCPW, lumped 50-ohm ports, er 4.3, h 254um, w 450um, gap 200um, 10 mm",
+               kw=dict(hmin=25e-6, hmax=200e-6, dx=100e-6, steps=20000)),
+}
+# Huray: sphere radius 0.5 um, 2e11 spheres per m^2 of flat area (K(inf) = 1 + 4 pi a^2 N = 1.63), standing in
+# for Rq = 1 um
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+        self.f.flush()
+
+    def summary(self) -> dict:
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            v = [x.strip() for x in line.split(",")]
+            if len(v) >= 9:
+                rows.append(v)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes(z: dict) -> dict:
+    """Compulsory DRAM bytes per time step (FP32 state): each field component,
+    CPML auxiliary, Debye current and SIBC state read once and written once;
+    coefficients, material indices and probe traffic excluded."""
+    P = z["npole"]
+    return {
+        # whole step, all state read once + written once (the H/E-fused minimum)
+        "step": 48 * z["cells"] + 8 * (z["psiE"] + z["psiH"]) + 8 * P * z["ndisp"] + 8 * z["sibc_terms"] * z["nsibc"],
+        # E update as a kernel of its own: E read+write, H read, psi_E, Debye J
+        "update_e": 36 * z["cells"] + 8 * z["psiE"] + 8 * P * z["ndisp"],
+        # H update: H read+write, E read, psi_H
+        "update_h": 36 * z["cells"] + 8 * z["psiH"],
+    }
+
+
+def build_sim(lib, workload: str):
+    from courant_b200 import scenes
+    t = time.time()
+    s, meta = scenes.gcpw_line(lib, **WORKLOADS[workload]["kw"])
+    meta["setup_s"] = time.time() - t
+    return s, meta
+
+
+def cpu_baseline(workload: str, steps_per_sample: int, samples: int) -> dict:
+    """The reference core on the host cores, a bounded sample of the workload."""
+    import oracle
+    from courant_b200.api import Courant
+    ref = Courant(oracle.REF_LIB)
+    s, meta = build_sim(ref, workload)
+    s.step(2)   # warm caches / thread pool
+    t = time.perf_counter()
+    for _ in range(samples):
+        s.step(steps_per_sample)
+    dt = time.perf_counter() - t
+    cells = meta["cells"]
+    return {"value": cells * steps_per_sample * samples / dt, "unit": "cell-updates/s",
+            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())), "kind": "reference",
+            "sample": f"{samples} x cem_step({steps_per_sample}) of the {meta['dims']} workload "
+                      f"({dt:.1f} s), setup excluded",
+            "setup_s": meta["setup_s"]}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.REF_LIB.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcourant_ref.so was not built"}))
+        return
+    from courant_b200.api import Courant
+    ref = Courant(oracle.REF_LIB)
+    s, meta = build_sim(ref, args.workload)
+    per = args.ref_chunk
+    for _ in range(args.warmup):
+        s.step(per)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        s.step(per)
+    dt = time.perf_counter() - t
+    v = meta["cells"] * per * args.steps / dt
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    line = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOADS[args.workload]["desc"], "dims": meta["dims"], "cells": meta["cells"],
+                       "time_steps_per_step": per, "setup_s": meta["setup_s"], "threads": cores},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "reference",
+                             "sample": f"{args.steps} x cem_step({per}) after {args.warmup} warm-up"},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_b200(args) -> None:
+    import torch
+    import torch.distributed as dist
+    from courant_b200.api import Courant
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    lib = Courant()
+    lib.selectDevice(local)
+    s, meta = build_sim(lib, args.workload)
+    log(f"rank {rank}: setup {meta['setup_s']:.1f} s, grid {meta['dims']}")
+    chunk = args.chunk
+    for _ in range(args.warmup):
+        s.step(chunk)
+    s.synchronize()
+    z = s.sizes()
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        gpu_ms = s.stepTimed(args.steps * chunk)
+        torch.cuda.synchronize()
+        barrier()
+    gpu_ms = max_over_ranks(gpu_ms)
+    cells = meta["cells"]
+    value = world * cells * chunk * args.steps / (gpu_ms / 1e3)
+
+    # per-kernel device time (event pair per launch) for the roofline
+    prof = s.profileSteps(args.profile_steps)
+    ab = algorithmic_bytes(z)
+    kern = {k: v for k, v in prof.items() if v["launches"]}
+    dominant = max(kern, key=lambda k: kern[k]["ms"])
+    tot = sum(v["ms"] for v in kern.values())
+    peak, peak_kind = measured_peaks()
+    dom_ms = kern[dominant]["ms"] / kern[dominant]["launches"]
+    dom_bytes = ab.get(dominant)
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_bytes else None
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        try:
+            t = json.loads(tf.read_text()).get(f"{args.workload}:{dominant}")
+            traffic = t["dram_bytes_per_launch"] if t else None
+        except Exception:
+            traffic = None
+
+    # end to end through the C ABI: upload plan + state, one whole excitation, spectra read every chunk
+    e2e = None
+    if not args.no_e2e:
+        s.releaseDevice()
+        e2e_steps = meta["steps"] if args.e2e_steps is None else args.e2e_steps
+        n_chunks = max(1, e2e_steps // chunk)
+        ex = s.c.ex
+        nvp, nip, nport = ex.cem_plan_nvprobe(s.h), ex.cem_plan_niprobe(s.h), ex.cem_plan_nport(s.h)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d2h = 0
+        for _ in range(n_chunks):
+            s.step(chunk)
+            specs = [s.vprobe(p) for p in range(nvp)] + [s.iprobe(p) for p in range(nip)]
+            specs += [s.portV(p) for p in range(nport)] + [s.portI(p) for p in range(nport)]
+            specs.append(s.sourceSpectrum())
+            d2h += sum(a.size * 16 for a in specs)
+        torch.cuda.synchronize()
+        wall = max_over_ranks(time.perf_counter() - t0)
+        barrier()
+        z2 = s.sizes()
+        e2e = {"value": world * cells * chunk * n_chunks / wall, "unit": "cell-updates/s",
+               "h2d_bytes_per_step": int(z2["device_bytes"] / n_chunks), "d2h_bytes_per_step": int(d2h / n_chunks),
+               "steps": n_chunks, "time_steps": n_chunks * chunk,
+               "note": "first step uploads plan and state (device_bytes); spectra read after every step"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.REF_LIB.exists():
+            cpu = cpu_baseline(args.workload, args.ref_chunk, args.ref_samples)
+
+    if rank == 0:
+        launches = z["launches_per_step"] * args.steps * chunk + math.ceil(args.steps * chunk / 1024)
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": gpu_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 DFT)",
+            "data": "synthetic",
+            "config": {"workload": WORKLOADS[args.workload]["desc"], "dims": meta["dims"], "cells": cells,
+                       "time_steps_per_step": chunk, "nf": len(meta["freqs"]), "ndisp": z["ndisp"],
+                       "npole": z["npole"], "nsibc": z["nsibc"], "psi": z["psiE"] + z["psiH"],
+                       "parallelism": f"replicas x{world}", "l2": "state (>1 GB) exceeds L2; no flush",
+                       "setup_s": round(meta["setup_s"], 1)},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None, "peak_kind": peak_kind,
+                         "traffic": traffic, "bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
+                         "share": kern[dominant]["ms"] / tot,
+                         "step_bytes": ab["step"], "step_frac": ab["step"] / (gpu_ms / 1e3 / (args.steps * chunk)) / 1e9 / peak},
+            "kernels": {k: {"ms_per_launch": v["ms"] / v["launches"], "share": v["ms"] / tot} for k, v in kern.items()},
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
+    ap.add_argument("--chunk", type=int, default=500, help="FDTD time steps per benchmark step")
+    ap.add_argument("--ref-chunk", type=int, default=20, help="time steps per step of the CPU reference")
+    ap.add_argument("--ref-samples", type=int, default=10, help="CPU-baseline samples in the b200 arm")
+    ap.add_argument("--profile-steps", type=int, default=100)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

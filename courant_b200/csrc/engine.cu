@@ -1,0 +1,1368 @@
+// Device time stepping for libcourant_b200 (NVIDIA B200, sm_100a).
+//
+// Replaces the reference time loop (skyhoffert/CourantEM solver/src/sim.c:569-960,
+// dispersive.c:89-112, sibc.c:256-269, modeport.c:124-135) with four kernels
+// per step, all in stream order:
+//
+//   k_update_h   H bulk curl fused with the CPML psi_H recursions
+//   k_update_e   E bulk curl fused with the CPML psi_E recursions, PEC/sheet
+//                masking, the lumped and mode sources and the Debye ADE
+//                currents (correction and update in one pass per edge)
+//   k_sibc       surface-impedance edges (recursive convolution), if any
+//   k_post       probe/port line integrals by warp reductions into a sample
+//                ring; k_dft folds the ring into FP64 DFT accumulators
+//
+// Layout in HBM: fields and auxiliary states are FP32, structure of arrays,
+// in the reference index space q = i*si + j*sj + k (k fastest), so a warp
+// reads 32 consecutive words of a (j,k) plane. Each E edge carries a 16-bit
+// material index into a per-component coefficient table (ca-1, cb, source
+// coefficient, Debye beta/dt per pole). Coefficients that are close to 1 are
+// stored as their difference from 1 (ca-1, b-1, 1-k, 1-e) so FP32 keeps the
+// decay rates accurate over tens of thousands of steps.
+#include "sim.hpp"
+#include "../../include/courant_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+namespace cb2 {
+
+constexpr int kRing = 1024;          // sample rows kept on the device between DFT flushes
+constexpr int kBlock = 256;
+constexpr int kMaxSlots = 2 * kMaxProbes + kMaxPorts;
+constexpr unsigned kFlagDisp = 1, kFlagSrc = 2;
+
+// ---------------------------------------------------------------- arguments
+
+struct Geom {
+    int n[3];
+    long long si;
+    int sj, plane;
+    unsigned long long sj_magic;   // j = (m * sj_magic) >> 40 for m < plane
+};
+
+struct PmlAxis {
+    const int *plane_h, *plane_e;        // CPML plane of a cell / node, -1 outside
+    const float *bm1_h, *cid_h;          // b-1 and c/d at cells (H auxiliaries)
+    const float *bm1_e, *cid_e;          // b-1 and c/dd at nodes (E auxiliaries)
+    long long per;                       // points per plane
+};
+
+struct StepArgs {
+    Geom g;
+    float *E[3], *H[3];
+    const float *hc[3];      // dt/mu0 * idh per axis (cells)
+    const float *ec[3];      // ide per axis (nodes)
+    float dth;
+    int has_pml;
+    PmlAxis pml[3];
+    float *psiH[3][2], *psiE[3][2];
+    const unsigned short *mat[3];
+    const float *tab[3];
+    const unsigned char *tflag[3];
+    int ntab[3];
+    int npole;
+    float omk[kMaxPoles], hk[kMaxPoles];
+    float *J[3];
+    int jbox[3][6];          // i0, j0, k0, ni, nj, nk of each component's Debye box
+    double dt;
+    double src_amp, src_t0, src_tau;   // lumped Gaussian (amp 0 when none)
+    int msrc_on, i_src;
+    double m_t0, m_tau;
+    const float *wsrc[2];    // mode-source weights of Ey and Ez on plane i_src
+    const long long *dstep;
+};
+
+struct SibcArgs {
+    int ns, K;
+    const int *ecomp;
+    const long long *eidx;
+    const int *hcomp;        // 4 per edge
+    const long long *hidx;   // 4 per edge
+    const float *hw;         // 4 per edge (0 beyond the face count)
+    float *y;                // K * ns, term-major
+    float c[kSibcTerms], ome[kSibcTerms];
+    float *E[3];
+    const float *H[3];
+};
+
+struct PostArgs {
+    int nin;                 // input slots: nip current probes, nport ports, nvp voltage probes
+    int nip, nport, nvp, nslot;
+    const int *off;          // nin + 1 entry offsets
+    const unsigned char *ecomp;   // 0..5
+    const long long *eidx;
+    const double *ew;
+    const double *R;
+    double *vold;
+    int src_port;
+    double src_amp, src_t0, src_tau, dt;
+    int msrc_on;
+    double m_t0, m_tau;
+    double *ring;            // kRing * nslot
+    const float *F[6];
+    long long *dstep;
+    int advance;             // 1: count this step
+};
+
+// --------------------------------------------------------------- helpers
+
+template <int A>
+__device__ __forceinline__ long long axis_stride(const Geom &g) {
+    return A == 0 ? g.si : (A == 1 ? (long long)g.sj : 1LL);
+}
+
+template <int A>
+__device__ __forceinline__ int axis_index(int i, int j, int k) {
+    return A == 0 ? i : (A == 1 ? j : k);
+}
+
+// compact CPML index for derivative axis A (reference sim.c:655-678 layout)
+template <int A>
+__device__ __forceinline__ long long psi_index(const StepArgs &a, int plane, int i, int j, int k) {
+    const long long in_plane = A == 0 ? (long long)j * (a.g.n[2] + 1) + k
+                             : A == 1 ? (long long)i * (a.g.n[2] + 1) + k
+                                      : (long long)i * (a.g.n[1] + 1) + j;
+    return plane * a.pml[A].per + in_plane;
+}
+
+__device__ __forceinline__ double gauss(double t, double amp, double t0, double tau) {
+    const double x = (t - t0) / tau;
+    return amp * exp(-x * x);
+}
+
+__device__ __forceinline__ double dgauss(double t, double t0, double tau) {
+    const double x = (t - t0) / tau;
+    return -2 * x * exp(-x * x);
+}
+
+// ---------------------------------------------------------------- H update
+
+// H_C -= dt/mu0 [ (dE_{C+2}/dx_{C+1} + psi0) - (dE_{C+1}/dx_{C+2} + psi1) ]
+template <int C>
+__device__ __forceinline__ void h_component(const StepArgs &a, int i, int j, int k, long long q) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    const int idx[3] = {i, j, k};
+    // H_C exists for idx(A) < n(A) on both transverse axes
+    if (idx[A1] >= a.g.n[A1] || idx[A2] >= a.g.n[A2]) return;
+    const float *EA2 = a.E[A2], *EA1 = a.E[A1];
+    const float d1 = EA2[q + axis_stride<A1>(a.g)] - EA2[q];
+    const float d2 = EA1[q + axis_stride<A2>(a.g)] - EA1[q];
+    float t1 = d1 * a.hc[A1][idx[A1]];
+    float t2 = d2 * a.hc[A2][idx[A2]];
+    if (a.has_pml) {
+        const int p1 = a.pml[A1].plane_h[idx[A1]];
+        if (p1 >= 0) {
+            const long long pi = psi_index<A1>(a, p1, i, j, k);
+            float psi = a.psiH[C][0][pi];
+            psi = psi + a.pml[A1].bm1_h[idx[A1]] * psi + a.pml[A1].cid_h[idx[A1]] * d1;
+            a.psiH[C][0][pi] = psi;
+            t1 += a.dth * psi;
+        }
+        const int p2 = a.pml[A2].plane_h[idx[A2]];
+        if (p2 >= 0) {
+            const long long pi = psi_index<A2>(a, p2, i, j, k);
+            float psi = a.psiH[C][1][pi];
+            psi = psi + a.pml[A2].bm1_h[idx[A2]] * psi + a.pml[A2].cid_h[idx[A2]] * d2;
+            a.psiH[C][1][pi] = psi;
+            t2 += a.dth * psi;
+        }
+    }
+    a.H[C][q] -= t1 - t2;
+}
+
+__global__ void __launch_bounds__(kBlock) k_update_h(const StepArgs a, int i0) {
+    const int i = i0 + blockIdx.y;
+    const int m = blockIdx.x * kBlock + threadIdx.x;
+    if (m >= a.g.plane) return;
+    const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
+    const int k = m - j * a.g.sj;
+    const long long q = (long long)i * a.g.si + m;
+    h_component<0>(a, i, j, k, q);
+    h_component<1>(a, i, j, k, q);
+    h_component<2>(a, i, j, k, q);
+}
+
+// ---------------------------------------------------------------- E update
+
+// E_C = E + (ca-1) E + cb [ (dH_{C+2}/dx_{C+1} + psi0) - (dH_{C+1}/dx_{C+2} + psi1) - sum_p hk_p J_p ]
+//       + cs Vs(t) + w Vm(t);   J_p += -(1-k_p) J_p + beta_p/dt (E_new - E_old)
+template <int C>
+__device__ __forceinline__ void e_component(const StepArgs &a, int i, int j, int k, long long q, long long step) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    const int idx[3] = {i, j, k};
+    if (idx[C] >= a.g.n[C]) return;
+    if (idx[A1] < 1 || idx[A1] >= a.g.n[A1] || idx[A2] < 1 || idx[A2] >= a.g.n[A2]) return;
+    const float *HA2 = a.H[A2], *HA1 = a.H[A1];
+    const float d1 = HA2[q] - HA2[q - axis_stride<A1>(a.g)];
+    const float d2 = HA1[q] - HA1[q - axis_stride<A2>(a.g)];
+    float t1 = d1 * a.ec[A1][idx[A1]];
+    float t2 = d2 * a.ec[A2][idx[A2]];
+    if (a.has_pml) {
+        const int p1 = a.pml[A1].plane_e[idx[A1]];
+        if (p1 >= 0) {
+            const long long pi = psi_index<A1>(a, p1, i, j, k);
+            float psi = a.psiE[C][0][pi];
+            psi = psi + a.pml[A1].bm1_e[idx[A1]] * psi + a.pml[A1].cid_e[idx[A1]] * d1;
+            a.psiE[C][0][pi] = psi;
+            t1 += psi;
+        }
+        const int p2 = a.pml[A2].plane_e[idx[A2]];
+        if (p2 >= 0) {
+            const long long pi = psi_index<A2>(a, p2, i, j, k);
+            float psi = a.psiE[C][1][pi];
+            psi = psi + a.pml[A2].bm1_e[idx[A2]] * psi + a.pml[A2].cid_e[idx[A2]] * d2;
+            a.psiE[C][1][pi] = psi;
+            t2 += psi;
+        }
+    }
+    const int mi = a.mat[C][q];
+    const int nt = a.ntab[C];
+    const float *tab = a.tab[C];
+    const float cam1 = __ldg(tab + mi), cb = __ldg(tab + nt + mi);
+    const unsigned flag = __ldg(a.tflag[C] + mi);
+    const float e_old = a.E[C][q];
+    float curl = t1 - t2;
+    long long jo = 0, jvol = 0;
+    if (flag & kFlagDisp) {
+        const int *bx = a.jbox[C];
+        jvol = (long long)bx[3] * bx[4] * bx[5];
+        jo = ((long long)(i - bx[0]) * bx[4] + (j - bx[1])) * bx[5] + (k - bx[2]);
+        float acc = 0.f;
+        for (int p = 0; p < a.npole; p++) acc += a.hk[p] * a.J[C][p * jvol + jo];
+        curl -= acc;
+    }
+    float e = fmaf(cam1, e_old, e_old) + cb * curl;
+    if (flag & kFlagSrc) {
+        const double tH = ((double)step + 0.5) * a.dt;
+        e += __ldg(tab + 2 * nt + mi) * (float)gauss(tH, a.src_amp, a.src_t0, a.src_tau);
+    }
+    if (C > 0 && a.msrc_on && i == a.i_src) {
+        const float w = a.wsrc[C - 1][(long long)j * (a.g.n[2] + 1) + k];
+        if (w != 0.f) {
+            const double tH = ((double)step + 0.5) * a.dt;
+            e += w * (float)dgauss(tH, a.m_t0, a.m_tau);
+        }
+    }
+    if (flag & kFlagDisp) {
+        const float de = e - e_old;
+        for (int p = 0; p < a.npole; p++) {
+            const float bidt = __ldg(tab + (3 + p) * nt + mi);
+            const float jp = a.J[C][p * jvol + jo];
+            a.J[C][p * jvol + jo] = jp - a.omk[p] * jp + bidt * de;
+        }
+    }
+    a.E[C][q] = e;
+}
+
+__global__ void __launch_bounds__(kBlock) k_update_e(const StepArgs a, int i0) {
+    const int i = i0 + blockIdx.y;
+    const int m = blockIdx.x * kBlock + threadIdx.x;
+    if (m >= a.g.plane) return;
+    const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
+    const int k = m - j * a.g.sj;
+    const long long q = (long long)i * a.g.si + m;
+    const long long step = *a.dstep;
+    e_component<0>(a, i, j, k, q, step);
+    e_component<1>(a, i, j, k, q, step);
+    e_component<2>(a, i, j, k, q, step);
+}
+
+// ------------------------------------------------------------------- SIBC
+
+// E = sum_k c_k (J - y_k) with y_k += (1 - e_k)(J - y_k), J from the faces' H.
+// (reference sibc.c:256-269)
+__global__ void __launch_bounds__(kBlock) k_sibc(const SibcArgs a) {
+    const int e = blockIdx.x * kBlock + threadIdx.x;
+    if (e >= a.ns) return;
+    float J = 0.f;
+    for (int f = 0; f < 4; f++) {
+        const float w = a.hw[4 * e + f];
+        if (w != 0.f) J += w * a.H[a.hcomp[4 * e + f]][a.hidx[4 * e + f]];
+    }
+    float E = 0.f;
+    for (int k = 0; k < a.K; k++) {
+        float y = a.y[(long long)k * a.ns + e];
+        y += a.ome[k] * (J - y);
+        a.y[(long long)k * a.ns + e] = y;
+        E += a.c[k] * (J - y);
+    }
+    a.E[a.ecomp[e]][a.eidx[e]] = E;
+}
+
+// ------------------------------------------------- probes, ports, DFT ring
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Line integrals of every input slot (warp per slot), then port V/I and the
+// source value, written as one row of the sample ring. With advance = 0 it
+// only refreshes the port voltages before the E update (vold).
+__global__ void __launch_bounds__(kBlock) k_post(const PostArgs a) {
+    __shared__ double res[kMaxSlots];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int first = a.advance ? 0 : a.nip, last = a.advance ? a.nin : a.nip + a.nport;
+    for (int s = first + warp; s < last; s += kBlock / 32) {
+        double v = 0;
+        for (int e = a.off[s] + lane; e < a.off[s + 1]; e += 32)
+            v += (double)a.F[a.ecomp[e]][a.eidx[e]] * a.ew[e];
+        v = warp_sum(v);
+        if (lane == 0) res[s] = v;
+    }
+    __syncthreads();
+    const long long step = *a.dstep;
+    if (!a.advance) {
+        if (threadIdx.x < a.nport) a.vold[threadIdx.x] = res[a.nip + threadIdx.x];
+        return;
+    }
+    double *row = a.ring + (long long)(step % kRing) * a.nslot;
+    const double tH = ((double)step + 0.5) * a.dt;
+    const double vs = a.src_port >= 0 ? gauss(tH, a.src_amp, a.src_t0, a.src_tau) : 0.0;
+    for (int s = threadIdx.x; s < a.nip; s += kBlock) row[s] = res[s];
+    for (int p = threadIdx.x; p < a.nport; p += kBlock) {
+        const double vnew = res[a.nip + p];
+        const double V = 0.5 * (vnew + a.vold[p]);
+        a.vold[p] = vnew;
+        const double I = ((p == a.src_port ? vs : 0.0) - V) / a.R[p];
+        row[a.nip + 2 * p] = V;
+        row[a.nip + 2 * p + 1] = I;
+    }
+    if (threadIdx.x == 0) {
+        double src = a.src_port >= 0 ? vs : 0.0;
+        if (a.msrc_on) src += dgauss(tH, a.m_t0, a.m_tau);
+        row[a.nip + 2 * a.nport] = src;
+    }
+    for (int s = threadIdx.x; s < a.nvp; s += kBlock) row[a.nip + 2 * a.nport + 1 + s] = res[a.nip + a.nport + s];
+    __syncthreads();
+    if (threadIdx.x == 0) *a.dstep = step + 1;
+}
+
+// acc[slot][f] += sum over the pending rows of (sample * dt) e^{-j w t}, t the
+// slot's sampling time: (n + 1/2) dt for H-time slots, (n + 1) dt for the
+// voltage probes (reference sim.c:840-861,872-933).
+__global__ void k_dft(const double *ring, int nslot, int first_e_slot, long long step0, int count, double dt,
+                      const double *omega, int nf, double *acc) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.y;
+    if (f >= nf) return;
+    const double w = omega[f];
+    const double toff = s >= first_e_slot ? 1.0 : 0.5;
+    double re = 0, im = 0;
+    for (int r = 0; r < count; r++) {
+        const long long n = step0 + r;
+        const double v = ring[(n % kRing) * nslot + s] * dt;
+        double sn, cs;
+        sincos(w * (((double)n + toff) * dt), &sn, &cs);
+        re += v * cs;
+        im += v * -sn;
+    }
+    acc[(long long)s * 2 * nf + 2 * f] += re;
+    acc[(long long)s * 2 * nf + 2 * f + 1] += im;
+}
+
+// ----------------------------------------------------------------- energy
+
+struct EnergyArgs {
+    Geom g;
+    const float *F[6];
+    const unsigned short *mat[3];
+    const double *cb64[3];
+    const double *d[3], *dd[3];
+    double dt;
+    double *partial;
+};
+
+// W = 1/2 sum eps E^2 dV + 1/2 sum mu0 H^2 dV with eps = dt/cb (reference sim.c:970-994)
+__global__ void __launch_bounds__(kBlock) k_energy(const EnergyArgs a) {
+    __shared__ double red[kBlock / 32];
+    const int i = blockIdx.y;
+    const int m = blockIdx.x * kBlock + threadIdx.x;
+    double acc = 0;
+    if (m < a.g.plane) {
+        const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
+        const int k = m - j * a.g.sj;
+        const long long q = (long long)i * a.g.si + m;
+        const int idx[3] = {i, j, k};
+        for (int c = 0; c < 3; c++) {
+            const int ua = (c + 1) % 3, va = (c + 2) % 3;
+            if (idx[c] < a.g.n[c]) {
+                const double cb = a.cb64[c][a.mat[c][q]];
+                if (cb != 0) {
+                    const double vol = a.d[c][idx[c]] * a.dd[ua][idx[ua]] * a.dd[va][idx[va]];
+                    const double e = a.F[c][q];
+                    acc += 0.5 * (a.dt / cb) * e * e * vol;
+                }
+            }
+            if (idx[ua] < a.g.n[ua] && idx[va] < a.g.n[va]) {
+                const double vol = a.dd[c][idx[c]] * a.d[ua][idx[ua]] * a.d[va][idx[va]];
+                const double h = a.F[3 + c][q];
+                acc += 0.5 * CEM_MU0 * h * h * vol;
+            }
+        }
+    }
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < kBlock / 32; w++) s += red[w];
+        a.partial[(long long)blockIdx.y * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// fixed-order sum of the block partials (deterministic)
+__global__ void k_sum(const double *partial, long long n, double *out) {
+    __shared__ double red[1024];
+    double s = 0;
+    for (long long q = threadIdx.x; q < n; q += blockDim.x) s += partial[q];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+// ------------------------------------------------------------ device state
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { if (p) cudaFree(p); }
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+};
+
+struct Device {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool failed = false;
+    std::string error;
+
+    Geom g{};
+    DevBuf<float> E[3], H[3];
+    DevBuf<float> hc[3], ec[3];
+    DevBuf<int> plane_h[3], plane_e[3];
+    DevBuf<float> bm1_h[3], cid_h[3], bm1_e[3], cid_e[3];
+    DevBuf<float> psiH[3][2], psiE[3][2];
+    size_t psi_len_h[3][2] = {}, psi_len_e[3][2] = {};
+    DevBuf<unsigned short> mat[3];
+    DevBuf<float> tab[3];
+    DevBuf<unsigned char> tflag[3];
+    DevBuf<double> cb64[3];
+    int ntab[3] = {0, 0, 0};
+    DevBuf<float> J[3];
+    int jbox[3][6] = {};
+    DevBuf<float> wsrc[2];
+    // SIBC
+    DevBuf<int> sb_ecomp, sb_hcomp;
+    DevBuf<long long> sb_eidx, sb_hidx;
+    DevBuf<float> sb_hw, sb_y;
+    // probes
+    int nip = 0, nport = 0, nvp = 0, nin = 0, nslot = 0;
+    DevBuf<int> off;
+    DevBuf<unsigned char> ecomp;
+    DevBuf<long long> eidx;
+    DevBuf<double> ew, R, vold, ring, acc, omega;
+    DevBuf<long long> dstep;
+    // energy
+    DevBuf<double> d64[3], dd64[3], partial, scalar;
+    // pending DFT rows [ring_first, ring_first + ring_count)
+    long long ring_first = 0;
+    int ring_count = 0;
+    bool vold_valid = false;
+
+    StepArgs sa{};
+    SibcArgs sb{};
+    PostArgs pa{};
+    EnergyArgs ea{};
+
+    ~Device() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+void device_release(Device *d) { delete d; }
+
+namespace {
+
+// optional per-kernel timing: when set, an event pair brackets every launch
+struct KernelTimer {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kind;
+    cudaStream_t stream = nullptr;
+    void begin(int k) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, stream);
+        ev.push_back(e);
+        kind.push_back(k);
+    }
+    void end() {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, stream);
+        ev.push_back(e);
+        kind.push_back(-1);
+    }
+};
+KernelTimer *g_timer = nullptr;
+thread_local int g_selected_device = -1;
+
+inline void t_begin(int k) { if (g_timer) g_timer->begin(k); }
+inline void t_end() { if (g_timer) g_timer->end(); }
+
+bool fail(cem_sim *s, const char *what, cudaError_t e) {
+    char msg[256];
+    std::snprintf(msg, sizeof msg, "CUDA %s: %s", what, cudaGetErrorString(e));
+    set_error(msg);
+    std::fprintf(stderr, "courant-b200: %s\n", msg);
+    if (s->dev) {
+        s->dev->failed = true;
+        s->dev->error = msg;
+    }
+    return false;
+}
+
+#define CB2_CHECK(s, call)                                  \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return fail((s), #call, e_); \
+    } while (0)
+
+// All copies and fills are ordered on the engine stream (a non-blocking
+// stream does not synchronise with the legacy default stream).
+bool h2d(cem_sim *s, void *dst, const void *src, size_t bytes) {
+    if (!bytes) return true;
+    CB2_CHECK(s, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->dev->stream));
+    CB2_CHECK(s, cudaStreamSynchronize(s->dev->stream));   // src may be a temporary
+    return true;
+}
+
+bool d2h(cem_sim *s, void *dst, const void *src, size_t bytes) {
+    if (!bytes) return true;
+    CB2_CHECK(s, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->dev->stream));
+    CB2_CHECK(s, cudaStreamSynchronize(s->dev->stream));
+    return true;
+}
+
+template <class T>
+bool dev_alloc(cem_sim *s, DevBuf<T> &b, size_t n) {
+    b.n = n;
+    if (!n) return true;
+    CB2_CHECK(s, cudaMalloc(&b.p, n * sizeof(T)));
+    return true;
+}
+
+template <class T>
+bool dev_upload(cem_sim *s, DevBuf<T> &b, const std::vector<T> &v) {
+    if (!dev_alloc(s, b, v.size())) return false;
+    return h2d(s, b.p, v.data(), v.size() * sizeof(T));
+}
+
+std::vector<float> to_f32(const std::vector<double> &v) {
+    std::vector<float> o(v.size());
+    for (size_t i = 0; i < v.size(); i++) o[i] = (float)v[i];
+    return o;
+}
+
+// Material tables: deduplicate the FP32 coefficient tuples of every E edge of
+// one component. Entry 0 is PEC (ca-1 = -1, cb = 0).
+struct TableBuilder {
+    int nf;   // fields per entry
+    std::vector<float> rows;        // entry-major while building
+    std::vector<unsigned char> flags;
+    std::vector<double> cb64;
+    std::unordered_map<std::string, int> index;
+    explicit TableBuilder(int nfields) : nf(nfields) {
+        std::vector<float> pec(nf, 0.f);
+        pec[0] = -1.f;
+        add(pec.data(), 0, 0.0);
+    }
+    int add(const float *row, unsigned char flag, double cb) {
+        std::string key(reinterpret_cast<const char *>(row), nf * sizeof(float));
+        key.push_back((char)flag);
+        auto it = index.find(key);
+        if (it != index.end()) return it->second;
+        const int id = (int)flags.size();
+        index.emplace(std::move(key), id);
+        rows.insert(rows.end(), row, row + nf);
+        flags.push_back(flag);
+        cb64.push_back(cb);
+        return id;
+    }
+    std::vector<float> field_major() const {
+        const size_t n = flags.size();
+        std::vector<float> o(n * nf);
+        for (size_t e = 0; e < n; e++)
+            for (int f = 0; f < nf; f++) o[f * n + e] = rows[e * nf + f];
+        return o;
+    }
+};
+
+bool build_tables(cem_sim *s, Device &D) {
+    const int P = s->npole;
+    const int nfields = 3 + P;
+    // per-edge extras: lumped source coefficient (excited port only), Debye beta/dt
+    std::vector<std::unordered_map<size_t, double>> src(3);
+    if (s->src_port >= 0) {
+        const LumpedPort &pt = s->port[s->src_port];
+        for (size_t e = 0; e < pt.edge.size(); e++) src[pt.axis][pt.edge[e]] = pt.cs[e];
+    }
+    std::vector<std::unordered_map<size_t, int>> disp(3);
+    for (int e = 0; e < s->ndisp; e++) disp[s->d_comp[e]][s->d_idx[e]] = e;
+    const int *n = s->n;
+    for (int c = 0; c < 3; c++) {
+        TableBuilder tb(nfields);
+        std::vector<unsigned short> mat(s->N, 0);
+        std::vector<float> row(nfields);
+        int box_lo[3] = {n[0], n[1], n[2]}, box_hi[3] = {-1, -1, -1};
+        std::string last_key;
+        for (int i = 0; i <= n[0]; i++)
+            for (int j = 0; j <= n[1]; j++)
+                for (int k = 0; k <= n[2]; k++) {
+                    const int ijk[3] = {i, j, k};
+                    if (ijk[c] >= n[c]) continue;
+                    const size_t q = idx3(s, i, j, k);
+                    const double ca = s->ca[c][q], cb = s->cb[c][q];
+                    if (cb == 0 && ca == 0) continue;   // PEC: entry 0
+                    std::fill(row.begin(), row.end(), 0.f);
+                    row[0] = (float)(ca - 1.0);
+                    row[1] = (float)cb;
+                    unsigned char flag = 0;
+                    auto it = src[c].find(q);
+                    if (it != src[c].end()) { row[2] = (float)it->second; flag |= kFlagSrc; }
+                    auto dt_ = disp[c].find(q);
+                    if (dt_ != disp[c].end()) {
+                        flag |= kFlagDisp;
+                        for (int p = 0; p < P; p++)
+                            row[3 + p] = (float)(s->d_beta[(size_t)p * s->ndisp + dt_->second] / s->dt);
+                        for (int a = 0; a < 3; a++) {
+                            box_lo[a] = std::min(box_lo[a], ijk[a]);
+                            box_hi[a] = std::max(box_hi[a], ijk[a]);
+                        }
+                    }
+                    const int id = tb.add(row.data(), flag, cb);
+                    if (id > 65535) {
+                        set_error("more than 65535 distinct update coefficients on one component");
+                        return false;
+                    }
+                    mat[q] = (unsigned short)id;
+                }
+        D.ntab[c] = (int)tb.flags.size();
+        if (!dev_upload(s, D.mat[c], mat)) return false;
+        if (!dev_upload(s, D.tab[c], tb.field_major())) return false;
+        if (!dev_upload(s, D.tflag[c], tb.flags)) return false;
+        if (!dev_upload(s, D.cb64[c], tb.cb64)) return false;
+        if (box_hi[0] >= 0) {
+            for (int a = 0; a < 3; a++) {
+                D.jbox[c][a] = box_lo[a];
+                D.jbox[c][3 + a] = box_hi[a] - box_lo[a] + 1;
+            }
+            const size_t vol = (size_t)D.jbox[c][3] * D.jbox[c][4] * D.jbox[c][5];
+            if (!dev_alloc(s, D.J[c], vol * P)) return false;
+        }
+    }
+    return true;
+}
+
+bool build_pml(cem_sim *s, Device &D) {
+    for (int a = 0; a < 3; a++) {
+        const int n = s->n[a];
+        std::vector<int> ph(n, -1), pe(n + 1, -1);
+        std::vector<float> bh(n, 0.f), chh(n, 0.f), be(n + 1, 0.f), cee(n + 1, 0.f);
+        int r[2][2];
+        pml_ranges(s, a, 0, r);
+        const int lo_h = r[0][1] >= r[0][0] ? r[0][1] - r[0][0] + 1 : 0;
+        for (int sd = 0; sd < 2; sd++)
+            for (int i = r[sd][0]; i <= r[sd][1]; i++) ph[i] = sd == 0 ? i - r[0][0] : lo_h + (i - r[1][0]);
+        pml_ranges(s, a, 1, r);
+        const int lo_e = r[0][1] >= r[0][0] ? r[0][1] - r[0][0] + 1 : 0;
+        for (int sd = 0; sd < 2; sd++)
+            for (int i = r[sd][0]; i <= r[sd][1]; i++) pe[i] = sd == 0 ? i - r[0][0] : lo_e + (i - r[1][0]);
+        for (int i = 0; i < n; i++) {
+            bh[i] = (float)(s->bh[a][i] - 1.0);
+            chh[i] = (float)(s->ch[a][i] * (1.0 / s->d[a][i]));
+        }
+        for (int i = 0; i <= n; i++) {
+            be[i] = (float)(s->be[a][i] - 1.0);
+            cee[i] = (float)(s->ce[a][i] * (s->dd[a][i] > 0 ? 1.0 / s->dd[a][i] : 0.0));
+        }
+        if (!s->has_pml) {
+            std::fill(ph.begin(), ph.end(), -1);
+            std::fill(pe.begin(), pe.end(), -1);
+        }
+        if (!dev_upload(s, D.plane_h[a], ph) || !dev_upload(s, D.plane_e[a], pe) || !dev_upload(s, D.bm1_h[a], bh) ||
+            !dev_upload(s, D.cid_h[a], chh) || !dev_upload(s, D.bm1_e[a], be) || !dev_upload(s, D.cid_e[a], cee))
+            return false;
+    }
+    for (int c = 0; c < 3; c++)
+        for (int w = 0; w < 2; w++) {
+            D.psi_len_h[c][w] = psi_len(s, 0, c, w);
+            D.psi_len_e[c][w] = psi_len(s, 1, c, w);
+            if (!dev_alloc(s, D.psiH[c][w], D.psi_len_h[c][w] + 1) || !dev_alloc(s, D.psiE[c][w], D.psi_len_e[c][w] + 1))
+                return false;
+        }
+    return true;
+}
+
+bool build_probes(cem_sim *s, Device &D) {
+    D.nip = (int)s->ip.size();
+    D.nport = (int)s->port.size();
+    D.nvp = (int)s->vp.size();
+    D.nin = D.nip + D.nport + D.nvp;
+    D.nslot = D.nip + 2 * D.nport + 1 + D.nvp;
+    std::vector<int> off{0};
+    std::vector<unsigned char> comp;
+    std::vector<long long> idx;
+    std::vector<double> w;
+    for (const CurrentProbe &p : s->ip) {
+        for (size_t e = 0; e < p.idx.size(); e++) {
+            comp.push_back((unsigned char)p.comp[e]); idx.push_back((long long)p.idx[e]); w.push_back(p.w[e]);
+        }
+        off.push_back((int)idx.size());
+    }
+    for (const LumpedPort &p : s->port) {
+        for (size_t e = 0; e < p.edge.size(); e++) {
+            comp.push_back((unsigned char)p.axis); idx.push_back((long long)p.edge[e]); w.push_back(p.dl[e] * p.dir);
+        }
+        off.push_back((int)idx.size());
+    }
+    for (const VoltageProbe &p : s->vp) {
+        for (size_t e = 0; e < p.edge.size(); e++) {
+            comp.push_back((unsigned char)p.axis); idx.push_back((long long)p.edge[e]); w.push_back(p.dl[e]);
+        }
+        off.push_back((int)idx.size());
+    }
+    std::vector<double> R;
+    for (const LumpedPort &p : s->port) R.push_back(p.R);
+    std::vector<double> omega(s->nf);
+    for (int f = 0; f < s->nf; f++) omega[f] = 2 * M_PI * s->freq[f];
+    if (!dev_upload(s, D.off, off) || !dev_upload(s, D.ecomp, comp) || !dev_upload(s, D.eidx, idx) ||
+        !dev_upload(s, D.ew, w) || !dev_upload(s, D.R, R) || !dev_upload(s, D.omega, omega))
+        return false;
+    if (!dev_alloc(s, D.vold, std::max(D.nport, 1)) || !dev_alloc(s, D.ring, (size_t)kRing * D.nslot) ||
+        !dev_alloc(s, D.acc, (size_t)D.nslot * 2 * s->nf) || !dev_alloc(s, D.dstep, 1))
+        return false;
+    return true;
+}
+
+bool build_sibc(cem_sim *s, Device &D) {
+    if (!s->nsb) return true;
+    std::vector<int> ecomp(s->sb_comp), hcomp(s->sb_hc);
+    std::vector<long long> eidx(s->nsb), hidx(4 * (size_t)s->nsb);
+    std::vector<float> hw(4 * (size_t)s->nsb);
+    for (int e = 0; e < s->nsb; e++) {
+        eidx[e] = (long long)s->sb_idx[e];
+        for (int f = 0; f < 4; f++) {
+            hidx[4 * e + f] = (long long)s->sb_hi[4 * e + f];
+            hw[4 * e + f] = f < s->sb_nf[e] ? (float)s->sb_sg[4 * e + f] : 0.f;
+        }
+    }
+    return dev_upload(s, D.sb_ecomp, ecomp) && dev_upload(s, D.sb_hcomp, hcomp) && dev_upload(s, D.sb_eidx, eidx) &&
+           dev_upload(s, D.sb_hidx, hidx) && dev_upload(s, D.sb_hw, hw) &&
+           dev_alloc(s, D.sb_y, (size_t)s->nsb * s->sibc_npole);
+}
+
+bool build_sources(cem_sim *s, Device &D) {
+    const size_t plane = (size_t)(s->n[1] + 1) * (s->n[2] + 1);
+    if (s->msrc >= 0) {
+        const ModePort &p = s->mport[s->msrc];
+        std::vector<float> w[2] = {std::vector<float>(plane, 0.f), std::vector<float>(plane, 0.f)};
+        for (size_t e = 0; e < p.src_idx.size(); e++) {
+            const size_t q = p.src_idx[e];
+            const size_t jk = q % s->si;   // j*sj + k on the i_src plane
+            w[p.src_comp[e] - 1][jk] += (float)p.src_w[e];
+        }
+        if (!dev_upload(s, D.wsrc[0], w[0]) || !dev_upload(s, D.wsrc[1], w[1])) return false;
+    }
+    return true;
+}
+
+void fill_args(cem_sim *s, Device &D) {
+    StepArgs &a = D.sa;
+    a = StepArgs{};
+    a.g = D.g;
+    for (int c = 0; c < 3; c++) {
+        a.E[c] = D.E[c].p;
+        a.H[c] = D.H[c].p;
+        a.hc[c] = D.hc[c].p;
+        a.ec[c] = D.ec[c].p;
+        a.pml[c] = PmlAxis{D.plane_h[c].p, D.plane_e[c].p, D.bm1_h[c].p, D.cid_h[c].p, D.bm1_e[c].p, D.cid_e[c].p,
+                           (long long)pml_per(s, c)};
+        for (int w = 0; w < 2; w++) {
+            a.psiH[c][w] = D.psiH[c][w].p;
+            a.psiE[c][w] = D.psiE[c][w].p;
+        }
+        a.mat[c] = D.mat[c].p;
+        a.tab[c] = D.tab[c].p;
+        a.tflag[c] = D.tflag[c].p;
+        a.ntab[c] = D.ntab[c];
+        a.J[c] = D.J[c].p;
+        for (int q = 0; q < 6; q++) a.jbox[c][q] = D.jbox[c][q];
+    }
+    a.dth = (float)(s->dt / CEM_MU0);
+    a.has_pml = s->has_pml;
+    a.npole = s->npole;
+    for (int p = 0; p < s->npole; p++) {
+        const double tau = 1.0 / (2 * M_PI * s->pole_f[p]);
+        const double r = s->dt / (2 * tau);
+        a.omk[p] = (float)(2 * r / (1 + r));   // 1 - k_p
+        a.hk[p] = (float)(0.5 * (1 + s->d_k[p]));
+    }
+    a.dt = s->dt;
+    a.src_amp = s->src_port >= 0 ? s->src_amp : 0.0;
+    a.src_t0 = s->src_t0;
+    a.src_tau = s->src_tau;
+    a.msrc_on = s->msrc >= 0;
+    if (a.msrc_on) {
+        a.i_src = s->mport[s->msrc].def.i_src;
+        a.m_t0 = s->msrc_t0;
+        a.m_tau = s->msrc_tau;
+        a.wsrc[0] = D.wsrc[0].p;
+        a.wsrc[1] = D.wsrc[1].p;
+    }
+    a.dstep = D.dstep.p;
+
+    SibcArgs &b = D.sb;
+    b = SibcArgs{};
+    b.ns = s->nsb;
+    b.K = s->sibc_npole;
+    b.ecomp = D.sb_ecomp.p; b.eidx = D.sb_eidx.p; b.hcomp = D.sb_hcomp.p; b.hidx = D.sb_hidx.p; b.hw = D.sb_hw.p;
+    b.y = D.sb_y.p;
+    for (int k = 0; k < s->sibc_npole; k++) {
+        b.c[k] = (float)s->sibc_c[k];
+        b.ome[k] = (float)(-std::expm1(-s->sibc_a[k] * s->dt));   // 1 - e_k without cancellation
+    }
+    for (int c = 0; c < 3; c++) { b.E[c] = D.E[c].p; b.H[c] = D.H[c].p; }
+
+    PostArgs &p = D.pa;
+    p = PostArgs{};
+    p.nin = D.nin; p.nip = D.nip; p.nport = D.nport; p.nvp = D.nvp; p.nslot = D.nslot;
+    p.off = D.off.p; p.ecomp = D.ecomp.p; p.eidx = D.eidx.p; p.ew = D.ew.p; p.R = D.R.p; p.vold = D.vold.p;
+    p.src_port = s->src_port;
+    p.src_amp = s->src_amp; p.src_t0 = s->src_t0; p.src_tau = s->src_tau; p.dt = s->dt;
+    p.msrc_on = s->msrc >= 0; p.m_t0 = s->msrc_t0; p.m_tau = s->msrc_tau;
+    p.ring = D.ring.p;
+    for (int c = 0; c < 3; c++) { p.F[c] = D.E[c].p; p.F[3 + c] = D.H[c].p; }
+    p.dstep = D.dstep.p;
+
+    EnergyArgs &e = D.ea;
+    e.g = D.g;
+    for (int c = 0; c < 3; c++) {
+        e.F[c] = D.E[c].p; e.F[3 + c] = D.H[c].p;
+        e.mat[c] = D.mat[c].p; e.cb64[c] = D.cb64[c].p;
+        e.d[c] = D.d64[c].p; e.dd[c] = D.dd64[c].p;
+    }
+    e.dt = s->dt;
+    e.partial = D.partial.p;
+}
+
+bool create_device_impl(cem_sim *s);
+
+// a device that failed to build is dropped, so the next call starts over
+bool create_device(cem_sim *s) {
+    if (s->dev) return !s->dev->failed;
+    if (create_device_impl(s)) return true;
+    s->dev.reset();
+    return false;
+}
+
+bool create_device_impl(cem_sim *s) {
+    if (!s->finalized) { set_error("not finalized"); return false; }
+    int ndev = 0;
+    cudaError_t err = cudaGetDeviceCount(&ndev);
+    if (err != cudaSuccess || ndev == 0) {
+        set_error("no CUDA device: libcourant_b200 steps only on the GPU");
+        std::fprintf(stderr, "courant-b200: no CUDA device: libcourant_b200 steps only on the GPU\n");
+        return false;
+    }
+    s->dev.reset(new Device);
+    Device &D = *s->dev;
+    if (g_selected_device >= 0) CB2_CHECK(s, cudaSetDevice(g_selected_device));
+    CB2_CHECK(s, cudaGetDevice(&D.device));
+    CB2_CHECK(s, cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking));
+    Geom &g = D.g;
+    for (int a = 0; a < 3; a++) g.n[a] = s->n[a];
+    g.si = (long long)s->si;
+    g.sj = (int)s->sj;
+    g.plane = (int)s->si;
+    g.sj_magic = ((1ull << 40) + s->sj - 1) / s->sj;
+    if ((double)g.plane * (double)g.sj >= 1099511627776.0) {
+        set_error("grid plane too large");
+        return false;
+    }
+    for (int c = 0; c < 3; c++) {
+        if (!dev_alloc(s, D.E[c], s->N) || !dev_alloc(s, D.H[c], s->N)) return false;
+        std::vector<double> hc(s->n[c]);
+        for (int i = 0; i < s->n[c]; i++) hc[i] = s->dt / CEM_MU0 * s->idh[c][i];
+        if (!dev_upload(s, D.hc[c], to_f32(hc)) || !dev_upload(s, D.ec[c], to_f32(s->ide[c]))) return false;
+        if (!dev_upload(s, D.d64[c], s->d[c]) || !dev_upload(s, D.dd64[c], s->dd[c])) return false;
+    }
+    if (!build_pml(s, D) || !build_tables(s, D) || !build_probes(s, D) || !build_sibc(s, D) || !build_sources(s, D))
+        return false;
+    const long long nblk = (long long)((g.plane + kBlock - 1) / kBlock) * (s->n[0] + 1);
+    if (!dev_alloc(s, D.partial, (size_t)nblk) || !dev_alloc(s, D.scalar, 1)) return false;
+    fill_args(s, D);
+    return true;
+}
+
+// ----------------------------------------------------- host <-> device moves
+
+bool upload_f32(cem_sim *s, float *dst, const std::vector<double> &src, size_t n) {
+    if (!n) return true;
+    std::vector<float> tmp(n);
+    for (size_t i = 0; i < n; i++) tmp[i] = (float)src[i];
+    return h2d(s, dst, tmp.data(), n * sizeof(float));
+}
+
+bool download_f32(cem_sim *s, std::vector<double> &dst, const float *src, size_t n) {
+    dst.resize(n);
+    if (!n) return true;
+    std::vector<float> tmp(n);
+    if (!d2h(s, tmp.data(), src, n * sizeof(float))) return false;
+    for (size_t i = 0; i < n; i++) dst[i] = tmp[i];
+    return true;
+}
+
+bool zero_dev(cem_sim *s, void *p, size_t bytes) {
+    if (!bytes || !p) return true;
+    CB2_CHECK(s, cudaMemsetAsync(p, 0, bytes, s->dev->stream));
+    return true;
+}
+
+// pack the host DFT accumulators in slot order: I probes, port V/I, source, V probes
+std::vector<double *> dft_slots(cem_sim *s) {
+    std::vector<double *> v;
+    for (CurrentProbe &p : s->ip) v.push_back(p.acc.data());
+    for (LumpedPort &p : s->port) { v.push_back(p.V.data()); v.push_back(p.I.data()); }
+    v.push_back(s->src_acc.data());
+    for (VoltageProbe &p : s->vp) v.push_back(p.acc.data());
+    return v;
+}
+
+bool flush_dft(cem_sim *s) {
+    Device &D = *s->dev;
+    if (!D.ring_count) return true;
+    dim3 grid((s->nf + 127) / 128, D.nslot);
+    t_begin(4);
+    k_dft<<<grid, 128, 0, D.stream>>>(D.ring.p, D.nslot, D.nip + 2 * D.nport + 1, D.ring_first, D.ring_count, s->dt,
+                                      D.omega.p, s->nf, D.acc.p);
+    t_end();
+    CB2_CHECK(s, cudaGetLastError());
+    D.ring_first += D.ring_count;
+    D.ring_count = 0;
+    return true;
+}
+
+bool upload_group(cem_sim *s, unsigned g, bool from_host) {
+    Device &D = *s->dev;
+    const size_t N = s->N;
+    for (int c = 0; c < 3; c++) {
+        if (g & (kGroupE0 << c)) {
+            if (from_host) { if (!upload_f32(s, D.E[c].p, s->E[c], N)) return false; }
+            else if (!zero_dev(s, D.E[c].p, N * sizeof(float))) return false;
+            D.vold_valid = false;
+        }
+        if (g & (kGroupH0 << c)) {
+            if (from_host) { if (!upload_f32(s, D.H[c].p, s->H[c], N)) return false; }
+            else if (!zero_dev(s, D.H[c].p, N * sizeof(float))) return false;
+        }
+    }
+    if (g & kGroupPsi)
+        for (int c = 0; c < 3; c++)
+            for (int w = 0; w < 2; w++) {
+                if (from_host) {
+                    if (!upload_f32(s, D.psiE[c][w].p, s->psiE[c][w], D.psi_len_e[c][w]) ||
+                        !upload_f32(s, D.psiH[c][w].p, s->psiH[c][w], D.psi_len_h[c][w]))
+                        return false;
+                } else if (!zero_dev(s, D.psiE[c][w].p, D.psiE[c][w].n * 4) ||
+                           !zero_dev(s, D.psiH[c][w].p, D.psiH[c][w].n * 4)) {
+                    return false;
+                }
+            }
+    if (g & kGroupDebye)
+        for (int c = 0; c < 3; c++) {
+            if (!D.J[c].p) continue;
+            if (!from_host) { if (!zero_dev(s, D.J[c].p, D.J[c].n * 4)) return false; continue; }
+            const int *bx = D.jbox[c];
+            const size_t vol = (size_t)bx[3] * bx[4] * bx[5];
+            std::vector<float> box(D.J[c].n, 0.f);
+            for (int e = 0; e < s->ndisp; e++) {
+                if (s->d_comp[e] != c) continue;
+                const size_t q = s->d_idx[e];
+                const int i = (int)(q / s->si), j = (int)((q % s->si) / s->sj), k = (int)(q % s->sj);
+                const size_t o = ((size_t)(i - bx[0]) * bx[4] + (j - bx[1])) * bx[5] + (k - bx[2]);
+                for (int p = 0; p < s->npole; p++) box[p * vol + o] = (float)s->d_J[(size_t)p * s->ndisp + e];
+            }
+            if (!h2d(s, D.J[c].p, box.data(), box.size() * 4)) return false;
+        }
+    if ((g & kGroupSibc) && s->nsb) {
+        if (!from_host) {
+            if (!zero_dev(s, D.sb_y.p, D.sb_y.n * 4)) return false;
+        } else {
+            const int K = s->sibc_npole, ns = s->nsb;
+            std::vector<float> y((size_t)K * ns);
+            for (int e = 0; e < ns; e++)
+                for (int k = 0; k < K; k++) y[(size_t)k * ns + e] = (float)s->sb_y[(size_t)e * K + k];
+            if (!h2d(s, D.sb_y.p, y.data(), y.size() * 4)) return false;
+        }
+    }
+    if (g & kGroupDft) {
+        const size_t len = 2 * (size_t)s->nf;
+        std::vector<double> acc((size_t)D.nslot * len, 0.0);
+        if (from_host) {
+            std::vector<double *> slots = dft_slots(s);
+            for (size_t q = 0; q < slots.size(); q++) std::memcpy(&acc[q * len], slots[q], len * sizeof(double));
+        }
+        if (!h2d(s, D.acc.p, acc.data(), acc.size() * sizeof(double))) return false;
+        D.ring_first = s->step;
+        D.ring_count = 0;
+    }
+    return true;
+}
+
+bool download_group(cem_sim *s, unsigned g) {
+    Device &D = *s->dev;
+    const size_t N = s->N;
+    if ((g & kGroupDft) && !flush_dft(s)) return false;
+    CB2_CHECK(s, cudaStreamSynchronize(D.stream));
+    for (int c = 0; c < 3; c++) {
+        if ((g & (kGroupE0 << c)) && !download_f32(s, s->E[c], D.E[c].p, N)) return false;
+        if ((g & (kGroupH0 << c)) && !download_f32(s, s->H[c], D.H[c].p, N)) return false;
+    }
+    if (g & kGroupPsi)
+        for (int c = 0; c < 3; c++)
+            for (int w = 0; w < 2; w++)
+                if (!download_f32(s, s->psiE[c][w], D.psiE[c][w].p, D.psi_len_e[c][w]) ||
+                    !download_f32(s, s->psiH[c][w], D.psiH[c][w].p, D.psi_len_h[c][w]))
+                    return false;
+    if (g & kGroupDebye) {
+        s->d_J.assign((size_t)s->npole * s->ndisp, 0.0);
+        if (s->d_Eold.size() != (size_t)s->ndisp) s->d_Eold.assign(s->ndisp, 0.0);
+        for (int c = 0; c < 3; c++) {
+            if (!D.J[c].p) continue;
+            std::vector<float> box(D.J[c].n);
+            if (!d2h(s, box.data(), D.J[c].p, box.size() * 4)) return false;
+            const int *bx = D.jbox[c];
+            const size_t vol = (size_t)bx[3] * bx[4] * bx[5];
+            for (int e = 0; e < s->ndisp; e++) {
+                if (s->d_comp[e] != c) continue;
+                const size_t q = s->d_idx[e];
+                const int i = (int)(q / s->si), j = (int)((q % s->si) / s->sj), k = (int)(q % s->sj);
+                const size_t o = ((size_t)(i - bx[0]) * bx[4] + (j - bx[1])) * bx[5] + (k - bx[2]);
+                for (int p = 0; p < s->npole; p++) s->d_J[(size_t)p * s->ndisp + e] = box[p * vol + o];
+            }
+        }
+    }
+    if ((g & kGroupSibc) && s->nsb) {
+        const int K = s->sibc_npole, ns = s->nsb;
+        std::vector<float> y((size_t)K * ns);
+        if (!d2h(s, y.data(), D.sb_y.p, y.size() * 4)) return false;
+        s->sb_y.resize((size_t)K * ns);
+        for (int e = 0; e < ns; e++)
+            for (int k = 0; k < K; k++) s->sb_y[(size_t)e * K + k] = y[(size_t)k * ns + e];
+    }
+    if (g & kGroupDft) {
+        const size_t len = 2 * (size_t)s->nf;
+        std::vector<double> acc((size_t)D.nslot * len);
+        if (!d2h(s, acc.data(), D.acc.p, acc.size() * sizeof(double))) return false;
+        std::vector<double *> slots = dft_slots(s);
+        for (size_t q = 0; q < slots.size(); q++) std::memcpy(slots[q], &acc[q * len], len * sizeof(double));
+    }
+    return true;
+}
+
+// Make the device state current before a device operation.
+bool begin_device_op(cem_sim *s) {
+    if (!create_device(s)) return false;
+    Device &D = *s->dev;
+    if (D.failed) { set_error(D.error.c_str()); return false; }
+    CB2_CHECK(s, cudaSetDevice(D.device));
+    CB2_CHECK(s, cudaStreamSynchronize(D.stream));
+    const unsigned need = (~s->dev_valid | s->exposed) & kGroupAll;
+    for (unsigned g = 1; g & kGroupAll; g <<= 1) {
+        if (!(need & g)) continue;
+        if (!upload_group(s, g, (s->host_valid & g) != 0)) return false;
+    }
+    s->dev_valid = kGroupAll;
+    if (D.ring_count == 0) D.ring_first = s->step;
+    long long st = s->step;
+    CB2_CHECK(s, cudaMemcpyAsync(D.dstep.p, &st, sizeof st, cudaMemcpyHostToDevice, D.stream));
+    CB2_CHECK(s, cudaStreamSynchronize(D.stream));
+    if (!D.vold_valid && D.nport) {
+        D.pa.advance = 0;
+        k_post<<<1, kBlock, 0, D.stream>>>(D.pa);
+        CB2_CHECK(s, cudaGetLastError());
+        D.vold_valid = true;
+    }
+    s->host_valid = 0;
+    return true;
+}
+
+// After a device operation: refresh what callers hold pointers to.
+bool end_device_op(cem_sim *s) {
+    if (s->exposed) {
+        if (!download_group(s, s->exposed)) return false;
+        s->host_valid |= s->exposed;
+    }
+    return true;
+}
+
+bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
+    Device &D = *s->dev;
+    const int nx = s->n[0];
+    const dim3 blk(kBlock);
+    const int gx = (D.g.plane + kBlock - 1) / kBlock;
+    if (phase_mask & 1) {   // H over node planes [i0, i1) within [0, nx]
+        const int a = std::max(0, i0), b = std::min(nx + 1, i1);
+        if (b > a) { t_begin(0); k_update_h<<<dim3(gx, b - a), blk, 0, D.stream>>>(D.sa, a); t_end(); }
+    }
+    if (phase_mask & 2) {   // port voltages before the E update
+        D.pa.advance = 0;
+        if (D.nport) k_post<<<1, kBlock, 0, D.stream>>>(D.pa);
+    }
+    if (phase_mask & 4) {   // E over node planes [i0, i1) within [0, nx)
+        const int a = std::max(0, i0), b = std::min(nx, i1);
+        if (b > a) { t_begin(1); k_update_e<<<dim3(gx, b - a), blk, 0, D.stream>>>(D.sa, a); t_end(); }
+    }
+    if (phase_mask & 8) {   // surface impedance, probes, step count
+        if (D.ring_count == kRing && !flush_dft(s)) return false;
+        if (s->nsb) { t_begin(2); k_sibc<<<(s->nsb + kBlock - 1) / kBlock, blk, 0, D.stream>>>(D.sb); t_end(); }
+        D.pa.advance = 1;
+        t_begin(3);
+        k_post<<<1, kBlock, 0, D.stream>>>(D.pa);
+        t_end();
+        D.ring_count++;
+        s->step++;
+    }
+    CB2_CHECK(s, cudaGetLastError());
+    return true;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ engine API
+
+void host_state_alloc(cem_sim *s, unsigned groups) {
+    for (int c = 0; c < 3; c++) {
+        if ((groups & (kGroupE0 << c)) && s->E[c].size() != s->N) s->E[c].assign(s->N, 0.0);
+        if ((groups & (kGroupH0 << c)) && s->H[c].size() != s->N) s->H[c].assign(s->N, 0.0);
+    }
+    if ((groups & kGroupPsi) && s->finalized)
+        for (int c = 0; c < 3; c++)
+            for (int w = 0; w < 2; w++) {
+                if (s->psiE[c][w].size() != psi_len(s, 1, c, w)) s->psiE[c][w].assign(psi_len(s, 1, c, w), 0.0);
+                if (s->psiH[c][w].size() != psi_len(s, 0, c, w)) s->psiH[c][w].assign(psi_len(s, 0, c, w), 0.0);
+            }
+    if ((groups & kGroupDebye) && s->finalized) {
+        if (s->d_J.size() != (size_t)s->npole * s->ndisp) s->d_J.assign((size_t)s->npole * s->ndisp, 0.0);
+        if (s->d_Eold.size() != (size_t)s->ndisp) s->d_Eold.assign(s->ndisp, 0.0);
+    }
+    if ((groups & kGroupSibc) && s->finalized && s->sb_y.size() != (size_t)s->nsb * s->sibc_npole)
+        s->sb_y.assign((size_t)s->nsb * s->sibc_npole, 0.0);
+}
+
+bool engine_has_device(const cem_sim *s) { return s->dev != nullptr; }
+
+int engine_pull(const cem_sim *cs, unsigned groups) {
+    cem_sim *s = const_cast<cem_sim *>(cs);
+    const unsigned missing = groups & ~s->host_valid & kGroupAll;
+    if (!missing) return 0;
+    host_state_alloc(s, missing);
+    const unsigned from_dev = s->dev && !s->dev->failed ? missing & s->dev_valid : 0u;
+    if (from_dev && !download_group(s, from_dev)) return -1;
+    // groups valid nowhere are all zero: the freshly allocated host copies
+    if (missing & ~from_dev) {
+        for (int c = 0; c < 3; c++) {
+            if (missing & ~from_dev & (kGroupE0 << c)) std::fill(s->E[c].begin(), s->E[c].end(), 0.0);
+            if (missing & ~from_dev & (kGroupH0 << c)) std::fill(s->H[c].begin(), s->H[c].end(), 0.0);
+        }
+    }
+    s->host_valid |= missing;
+    return 0;
+}
+
+void engine_expose(const cem_sim *cs, unsigned groups) { const_cast<cem_sim *>(cs)->exposed |= groups; }
+
+void engine_host_modified(cem_sim *s, unsigned groups) {
+    s->host_valid |= groups;
+    s->dev_valid &= ~groups;
+}
+
+int engine_step(cem_sim *s, long n) {
+    if (n <= 0) return 0;
+    if (!begin_device_op(s)) return -1;
+    for (long it = 0; it < n; it++)
+        if (!launch_step(s, 1 | 4 | 8, 0, s->n[0] + 1)) return -1;
+    if (!end_device_op(s)) return -1;
+    return 0;
+}
+
+int engine_phase(cem_sim *s, int phase, int i0, int i1) {
+    if (!begin_device_op(s)) return -1;
+    static const int masks[5] = {0, 1, 2, 4, 8};
+    if (phase < 0 || phase > 4) return 0;
+    if (phase == 2) s->dev->vold_valid = true;
+    if (!launch_step(s, masks[phase], i0, i1)) return -1;
+    if (!end_device_op(s)) return -1;
+    return 0;
+}
+
+namespace {
+bool energy_on_device(cem_sim *s, double *out) {
+    if (!begin_device_op(s)) return false;
+    Device &D = *s->dev;
+    const int gx = (D.g.plane + kBlock - 1) / kBlock;
+    k_energy<<<dim3(gx, s->n[0] + 1), kBlock, 0, D.stream>>>(D.ea);
+    k_sum<<<1, 1024, 0, D.stream>>>(D.partial.p, (long long)gx * (s->n[0] + 1), D.scalar.p);
+    CB2_CHECK(s, cudaGetLastError());
+    CB2_CHECK(s, cudaMemcpyAsync(out, D.scalar.p, sizeof(double), cudaMemcpyDeviceToHost, D.stream));
+    CB2_CHECK(s, cudaStreamSynchronize(D.stream));
+    return end_device_op(s);
+}
+}  // namespace
+
+int engine_energy(const cem_sim *cs, double *out) {
+    return energy_on_device(const_cast<cem_sim *>(cs), out) ? 0 : -1;
+}
+
+}  // namespace cb2
+
+using namespace cb2;
+
+namespace {
+bool timed_steps(cem_sim *s, long n, double *ms) {
+    if (!begin_device_op(s)) return false;
+    Device &D = *s->dev;
+    cudaEvent_t e0, e1;
+    CB2_CHECK(s, cudaEventCreate(&e0));
+    CB2_CHECK(s, cudaEventCreate(&e1));
+    CB2_CHECK(s, cudaEventRecord(e0, D.stream));
+    for (long it = 0; it < n; it++)
+        if (!launch_step(s, 1 | 4 | 8, 0, s->n[0] + 1)) return false;
+    CB2_CHECK(s, cudaEventRecord(e1, D.stream));
+    CB2_CHECK(s, cudaEventSynchronize(e1));
+    float t = 0;
+    CB2_CHECK(s, cudaEventElapsedTime(&t, e0, e1));
+    *ms = t;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return end_device_op(s);
+}
+
+bool profiled_steps(cem_sim *s, long n, double *kernel_ms, long *launches) {
+    if (!begin_device_op(s)) return false;
+    Device &D = *s->dev;
+    KernelTimer timer;
+    timer.stream = D.stream;
+    g_timer = &timer;
+    bool ok = true;
+    for (long it = 0; it < n && ok; it++) ok = launch_step(s, 1 | 4 | 8, 0, s->n[0] + 1);
+    if (ok) ok = flush_dft(s);
+    g_timer = nullptr;
+    if (!ok) return false;
+    CB2_CHECK(s, cudaStreamSynchronize(D.stream));
+    for (int k = 0; k < 5; k++) { kernel_ms[k] = 0; launches[k] = 0; }
+    for (size_t q = 0; q + 1 < timer.ev.size(); q += 2) {
+        float t = 0;
+        CB2_CHECK(s, cudaEventElapsedTime(&t, timer.ev[q], timer.ev[q + 1]));
+        kernel_ms[timer.kind[q]] += t;
+        launches[timer.kind[q]]++;
+    }
+    for (cudaEvent_t e : timer.ev) cudaEventDestroy(e);
+    return end_device_op(s);
+}
+}  // namespace
+
+extern "C" {
+
+int cemx_step_timed(cem_sim *s, long n, double *gpu_ms) {
+    if (!s->finalized) { set_error("not finalized"); return -1; }
+    return timed_steps(s, n, gpu_ms) ? 0 : -1;
+}
+
+int cemx_profile_steps(cem_sim *s, long n, double *kernel_ms, long *launches) {
+    if (!s->finalized) { set_error("not finalized"); return -1; }
+    return profiled_steps(s, n, kernel_ms, launches) ? 0 : -1;
+}
+
+int cemx_sizes(const cem_sim *s, long long *out, int n) {
+    if (!s->finalized) { set_error("not finalized"); return -1; }
+    long long v[13] = {0};
+    v[0] = (long long)s->n[0] * s->n[1] * s->n[2];
+    v[1] = (long long)s->N;
+    for (int c = 0; c < 3; c++)
+        for (int w = 0; w < 2; w++) {
+            v[2] += (long long)psi_len(s, 1, c, w);
+            v[3] += (long long)psi_len(s, 0, c, w);
+        }
+    v[4] = s->ndisp;
+    v[5] = s->npole;
+    v[6] = s->nsb;
+    v[7] = s->sibc_npole;
+    if (s->dev) {
+        for (int c = 0; c < 3; c++) v[8 + c] = s->dev->ntab[c];
+        size_t free_b = 0, total_b = 0;
+        (void)free_b; (void)total_b;
+        long long bytes = 0;
+        const Device &D = *s->dev;
+        for (int c = 0; c < 3; c++) {
+            bytes += (long long)(D.E[c].n + D.H[c].n + D.hc[c].n + D.ec[c].n) * 4 + (long long)D.mat[c].n * 2 +
+                     (long long)D.tab[c].n * 4 + (long long)D.J[c].n * 4;
+            for (int w = 0; w < 2; w++) bytes += (long long)(D.psiE[c][w].n + D.psiH[c][w].n) * 4;
+        }
+        bytes += (long long)(D.sb_y.n + D.sb_hw.n) * 4 + (long long)(D.sb_eidx.n + D.sb_hidx.n) * 8 +
+                 (long long)(D.ring.n + D.acc.n) * 8;
+        v[11] = bytes;
+    }
+    v[12] = 3 + (s->nsb ? 1 : 0);
+    for (int q = 0; q < n && q < 13; q++) out[q] = v[q];
+    return 0;
+}
+
+int cemx_select_device(int device) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        set_error("no such CUDA device");
+        return -1;
+    }
+    g_selected_device = device;
+    return 0;
+}
+
+int cemx_release_device(cem_sim *s) {
+    if (!s->dev) return 0;
+    if (engine_pull(s, kGroupAll)) return -1;
+    s->dev.reset();
+    s->dev_valid = 0;
+    return 0;
+}
+
+int cemx_synchronize(cem_sim *s) {
+    if (!s->dev) return 0;
+    cudaError_t e = cudaStreamSynchronize(s->dev->stream);
+    if (e != cudaSuccess) {
+        set_error(cudaGetErrorString(e));
+        return -1;
+    }
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,178 @@
+"""GPU engine against the oracle (f64 CPU restatement of the reference step,
+itself pinned to the reference bit for bit).
+
+Tolerances: fields relative L2 <= 1e-5 per component at matching steps (the
+FP32 engine against the f64 core); probe and port spectra relative to their
+peak <= 1e-5; energy <= 1e-5; S-parameters within 1e-3 dB and 0.01 degree
+where |S| > -40 dB, f >= 1 GHz. Checkpoint resume and slab-split phased
+stepping must match straight stepping bit for bit."""
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from courant_b200 import scenes
+from tests_util import db_deg, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-5
+SPEC_TOL = 1e-5
+
+
+def spectra(s, meta):
+    out = {}
+    for p in meta.get("ports", []):
+        out[f"V{p}"], out[f"I{p}"] = s.portV(p), s.portI(p)
+    for p in meta.get("vprobes", []):
+        out[f"vp{p}"] = s.vprobe(p)
+    for p in meta.get("iprobes", []):
+        out[f"ip{p}"] = s.iprobe(p)
+    out["src"] = s.sourceSpectrum()
+    return out
+
+
+def compare(gpu, orc, meta, steps, field_tol=FIELD_TOL, spec_tol=SPEC_TOL):
+    worst = {}
+    for c in range(6):
+        worst[f"field{c}"] = rel_l2(gpu.field(c), orc.field(c))
+    sg, so = spectra(gpu, meta), spectra(orc, meta)
+    for k in sg:
+        worst[k] = float(np.max(np.abs(sg[k] - so[k])) / max(np.max(np.abs(so[k])), 1e-300))
+    worst["energy"] = abs(gpu.energy() - orc.energy()) / orc.energy()
+    bad = {k: v for k, v in worst.items() if v > (field_tol if k.startswith("field") else spec_tol)}
+    assert not bad, (bad, worst)
+    return worst
+
+
+@pytest.mark.parametrize("fn", [scenes.parity_scene, scenes.lossy_scene], ids=["parity", "lossy"])
+def test_scene_against_oracle(lib, oracle_lib, fn):
+    s, meta = fn(lib)
+    n = meta["steps"]
+    o = oracle_lib.OracleSim.from_sim(s, meta["freqs"], n)
+    s.step(n)
+    o.step(n)
+    assert s.steps == o.steps == n
+    compare(s, o, meta, n)
+
+
+def test_parity_scene_against_reference_printout(lib):
+    """The reference known-answer printout (tests/golden/parity_scene.txt)."""
+    s, meta = scenes.parity_scene(lib)
+    s.step(1500)
+    ref = {}
+    for line in (ROOT / "tests" / "golden" / "parity_scene.txt").read_text().splitlines():
+        k, *v = line.split()
+        ref[k] = [float(x) for x in v]
+    assert s.dt == ref["dt"][0]
+    assert abs(s.energy() - ref["energy"][0]) / ref["energy"][0] < 1e-5
+    arrs = {"V1": s.portV(0), "V2": s.portV(1), "Vp": s.vprobe(0), "Ip": s.iprobe(0)}
+    for name, a in arrs.items():
+        r = np.array([complex(*ref[f"{name}[{q}]"]) for q in range(3)])
+        assert np.max(np.abs(a - r)) / np.max(np.abs(r)) < SPEC_TOL, name
+
+
+def test_checkpoint_resume_bit_exact(lib):
+    A, _ = scenes.lossy_scene(lib)
+    B, _ = scenes.lossy_scene(lib)
+    C, meta = scenes.lossy_scene(lib)
+    A.step(900)
+    B.step(400)
+    buf = B.checkpoint()
+    C.restore(buf)
+    C.step(500)
+    for c in range(6):
+        assert np.array_equal(A.field(c), C.field(c)), c
+    for p in meta["ports"]:
+        assert np.array_equal(A.portV(p), C.portV(p))
+    assert np.array_equal(A.vprobe(0), C.vprobe(0))
+
+
+def test_checkpoint_from_reference_resumes(lib, ref_lib):
+    """A checkpoint written by the reference core resumes on the GPU engine."""
+    R, meta = scenes.lossy_scene(ref_lib)
+    R.step(400)
+    buf = R.checkpoint()
+    G, _ = scenes.lossy_scene(lib)
+    G.restore(buf)
+    G.step(500)
+    R.step(500)
+    for c in range(6):
+        assert rel_l2(G.field(c), R.field(c)) < FIELD_TOL, c
+    assert np.max(np.abs(G.portV(1) - R.portV(1))) / np.max(np.abs(R.portV(1))) < SPEC_TOL
+
+
+def test_phased_stepping_matches_cem_step(lib):
+    A, _ = scenes.parity_scene(lib)
+    B, _ = scenes.parity_scene(lib)
+    A.step(50)
+    nx = B.nx
+    for _ in range(50):
+        B.c.ex.cem_mt_pre(B.h)
+        B.c.ex.cem_mt_H(B.h, 0, nx // 3)
+        B.c.ex.cem_mt_H(B.h, nx // 3, nx + 1)
+        B.c.ex.cem_mt_mid(B.h)
+        B.c.ex.cem_mt_E(B.h, 0, 7)
+        B.c.ex.cem_mt_E(B.h, 7, nx)
+        B.c.ex.cem_mt_post(B.h)
+    assert B.steps == 50
+    for c in range(6):
+        assert np.array_equal(A.field(c), B.field(c)), c
+    assert np.array_equal(A.portV(0), B.portV(0))
+
+
+def test_field_initial_condition_and_live_pointer(lib, oracle_lib):
+    """Initial E written through cem_field is taken up; the pointer stays live."""
+    s, meta = scenes.parity_scene(lib)
+    o = oracle_lib.OracleSim.from_sim(s, meta["freqs"], 300)
+    view = s.fieldView(1)
+    rng = np.random.default_rng(3)
+    init = np.zeros(s.N)
+    idx = rng.integers(0, s.N, 400)
+    init[idx] = rng.normal(size=400)
+    view[:] = init
+    o.field_view(1)[:] = np.float32(init)   # the engine holds FP32 fields
+    for _ in range(3):
+        s.step(100)
+        o.step(100)
+        assert rel_l2(view, o.field(1)) < FIELD_TOL
+
+
+def test_run_stops_on_energy_decay(lib, oracle_lib):
+    s, meta = scenes.parity_scene(lib)
+    n = s.run(20000, 1e-3, 100)
+    assert 0 < n < 20000 and n % 100 == 0
+    o = oracle_lib.OracleSim.from_sim(s, meta["freqs"], n)
+    o.step(n)
+    assert abs(s.energy() - o.energy()) / o.energy() < 1e-4
+
+
+def test_gcpw_lumped_sparams(lib, oracle_lib):
+    """S11/S21 of a short lumped-port GCPW within 1e-3 dB / 0.01 degree of the f64 oracle."""
+    kw = dict(length=3e-3, hmin=50e-6, hmax=200e-6, dx=100e-6, yair=0.6e-3, zair=0.8e-3, npml=6, df=1e9, steps=3000)
+    s, meta = scenes.gcpw_line(lib, **kw)
+    n = meta["steps"]
+    o = oracle_lib.OracleSim.from_sim(s, meta["freqs"], n)
+    s.step(n)
+    o.step(n)
+    from courant_b200.api import s_params
+    p1, p2 = meta["ports"]
+    g11, g21 = s_params(s.portV(p1), s.portI(p1), s.portV(p2), s.portI(p2), 50.0)
+    r11, r21 = s_params(o.portV(p1), o.portI(p1), o.portV(p2), o.portI(p2), 50.0)
+    f = np.asarray(meta["freqs"])
+    for g, r in ((g11, r11), (g21, r21)):
+        sel = (f >= 1e9) & (np.abs(r) > 0.01)
+        ddb, ddeg = db_deg(g[sel], r[sel])
+        assert ddb.max() < 1e-3 and ddeg.max() < 0.01, (ddb.max(), ddeg.max())
+
+
+@pytest.mark.parametrize("prog", ["test_checkpoint", "test_mode2d", "test_cavity", "test_cpml", "test_sibc"])
+def test_reference_program_links_and_passes(prog):
+    """The reference's own known-answer programs, linked unchanged against libcourant_b200."""
+    exe = ROOT / "oracle" / "_ref" / f"dropin_{prog}"
+    if not exe.exists():
+        pytest.skip(f"{exe.name} not built (make -C oracle dropin)")
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    print(r.stdout)
+    assert r.returncode == 0 and f"{prog} passed" in r.stdout, r.stdout + r.stderr

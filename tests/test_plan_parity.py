@@ -1,0 +1,79 @@
+"""The FP64 plan built on the host by libcourant_b200 equals the reference
+plan to the bit: every cem_plan_* array, the fits and the mode solver
+(golden digests from tests/golden/make_golden.py, and live against the
+reference library when it is built)."""
+import numpy as np
+import pytest
+
+from courant_b200 import scenes
+from tests_util import cmp_plans, plan_digest
+
+
+@pytest.mark.parametrize("name,fn", [("parity", scenes.parity_scene), ("lossy", scenes.lossy_scene)])
+def test_plan_digest_matches_reference(lib, golden, name, fn):
+    s, _ = fn(lib)
+    assert plan_digest(s.plan()) == golden[name]["plan"]
+    assert s.dt == golden[name]["dt"]
+
+
+@pytest.mark.parametrize("fn", [scenes.parity_scene, scenes.lossy_scene])
+def test_plan_live_against_reference(lib, ref_lib, fn):
+    a, _ = fn(ref_lib)
+    b, _ = fn(lib)
+    assert cmp_plans(a.plan(), b.plan()) == []
+
+
+def test_gcpw_plan_live_against_reference(lib, ref_lib):
+    kw = dict(length=2e-3, hmin=100e-6, hmax=400e-6, dx=200e-6, yair=0.6e-3, zair=0.8e-3, npml=6, nf=5,
+              tcu=35e-6, mask=20e-6, debye_poles=4, sigma_cu=5.8e7, huray=(0.5e-6, 2.0e11))
+    a, _ = scenes.gcpw_line(ref_lib, **kw)
+    b, _ = scenes.gcpw_line(lib, **kw)
+    assert cmp_plans(a.plan(), b.plan()) == []
+    assert a.conductorFitError() == b.conductorFitError()
+
+
+def test_djordjevic_sarkar_fit(lib, golden):
+    g = golden["ds_fit"]
+    m = lib.fitDjordjevicSarkar(*g["args"])
+    assert m.eps_inf == g["eps_inf"] and m.fp == g["fp"] and m.deps == g["deps"] and m.tan_delta_error == g["err"]
+
+
+def test_mode2d_wr28(lib, golden):
+    import ctypes as C
+    g = golden["mode2d_wr28"]
+    a, b, NY, NZ = 7.112e-3, 3.556e-3, 48, 24
+    y = np.array([a * j / NY for j in range(NY + 1)])
+    z = np.array([b * k / NZ for k in range(NZ + 1)])
+    dp = C.POINTER(C.c_double)
+    m = lib.ex.cem_mode2d_create(NY, NZ, y.ctypes.data_as(dp), z.ctypes.data_as(dp))
+    f = 35e9
+    k0 = 2 * np.pi * f / 299792458.0
+    beta = np.sqrt(k0 ** 2 - (np.pi / a) ** 2)
+    assert lib.ex.cem_mode2d_solve(m, f, beta / k0, None, 300, 1e-13) == g["rc"] == 0
+    Rs = np.sqrt(2 * np.pi * f * 1.25663706212e-6 / (2 * 5.8e7))
+    assert lib.ex.cem_mode2d_beta(m) == g["beta"]
+    assert lib.ex.cem_mode2d_conductor_alpha(m, Rs) == g["alpha_c"]
+    # the reference test's own acceptance: discrete-dispersion beta to 1e-8 (test_mode2d.c:22-31)
+    dy = a / NY
+    kcd = 2 / dy * np.sin(np.pi / a * dy / 2)
+    assert abs(g["beta"] - np.sqrt(k0 ** 2 - kcd ** 2)) / g["beta"] < 1e-8
+    lib.ex.cem_mode2d_destroy(m)
+
+
+def test_mode_port_source_and_port_modes(lib, golden):
+    g = golden["modeport_small"]
+    s, meta = scenes.gcpw_line(lib, length=2e-3, hmin=100e-6, hmax=400e-6, dx=200e-6, yair=0.6e-3, zair=0.8e-3,
+                               npml=6, feed=2e-3, mon=0.8e-3, nf=4, modeports=True, steps=300)
+    plan = s.plan()
+    from tests_util import digest
+    assert {k: digest(v) for k, v in plan["modeSource"].items()} == g["mode_source"]
+    w = s.modePortWaves(meta["modeports"][0])   # port modes solved on the host, no stepping needed
+    assert w["z0"].tolist() == g["z0"] and w["beta"].tolist() == g["beta"]
+
+
+def test_s2_renormalize(lib, ref_lib):
+    rng = np.random.default_rng(7)
+    for _ in range(20):
+        S = list(rng.normal(size=4) * 0.4 + 1j * rng.normal(size=4) * 0.4)
+        z1, z2 = rng.uniform(20, 80, size=2)
+        assert lib.renormalize2(S, z1, z2, 50.0) == ref_lib.renormalize2(S, z1, z2, 50.0)
