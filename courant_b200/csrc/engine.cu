@@ -57,7 +57,13 @@ struct PmlAxis {
     const float *bm1_h, *cid_h;          // b-1 and c/d at cells (H auxiliaries)
     const float *bm1_e, *cid_e;          // b-1 and c/dd at nodes (E auxiliaries)
     long long per;                       // points per plane
+    int planes;                          // planes in the CPML slabs of this axis (z-axis layout stride)
 };
+
+// Device layout of the CPML auxiliaries: x and y slabs as in the reference
+// (plane-major, then the in-plane index); z slabs with the plane index
+// fastest, ((i*(ny+1) + j) * planes + plane), so the z-slab cells of one k
+// row sit next to each other. Host copies use the reference layout.
 
 struct StepArgs {
     Geom g;
@@ -118,25 +124,6 @@ struct PostArgs {
 
 // --------------------------------------------------------------- helpers
 
-template <int A>
-__device__ __forceinline__ long long axis_stride(const Geom &g) {
-    return A == 0 ? g.si : (A == 1 ? (long long)g.sj : 1LL);
-}
-
-template <int A>
-__device__ __forceinline__ int axis_index(int i, int j, int k) {
-    return A == 0 ? i : (A == 1 ? j : k);
-}
-
-// compact CPML index for derivative axis A (reference sim.c:655-678 layout)
-template <int A>
-__device__ __forceinline__ long long psi_index(const StepArgs &a, int plane, int i, int j, int k) {
-    const long long in_plane = A == 0 ? (long long)j * (a.g.n[2] + 1) + k
-                             : A == 1 ? (long long)i * (a.g.n[2] + 1) + k
-                                      : (long long)i * (a.g.n[1] + 1) + j;
-    return plane * a.pml[A].per + in_plane;
-}
-
 __device__ __forceinline__ double gauss(double t, double amp, double t0, double tau) {
     const double x = (t - t0) / tau;
     return amp * exp(-x * x);
@@ -149,98 +136,107 @@ __device__ __forceinline__ double dgauss(double t, double t0, double tau) {
 
 // ---------------------------------------------------------------- H update
 
-// H_C -= dt/mu0 [ (dE_{C+2}/dx_{C+1} + psi0) - (dE_{C+1}/dx_{C+2} + psi1) ]
-template <int C>
-__device__ __forceinline__ void h_component(const StepArgs &a, int i, int j, int k, long long q) {
-    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
-    const int idx[3] = {i, j, k};
-    // H_C exists for idx(A) < n(A) on both transverse axes
-    if (idx[A1] >= a.g.n[A1] || idx[A2] >= a.g.n[A2]) return;
-    const float *EA2 = a.E[A2], *EA1 = a.E[A1];
-    const float d1 = EA2[q + axis_stride<A1>(a.g)] - EA2[q];
-    const float d2 = EA1[q + axis_stride<A2>(a.g)] - EA1[q];
-    float t1 = d1 * a.hc[A1][idx[A1]];
-    float t2 = d2 * a.hc[A2][idx[A2]];
-    if (a.has_pml) {
-        const int p1 = a.pml[A1].plane_h[idx[A1]];
-        if (p1 >= 0) {
-            const long long pi = psi_index<A1>(a, p1, i, j, k);
-            float psi = a.psiH[C][0][pi];
-            psi = psi + a.pml[A1].bm1_h[idx[A1]] * psi + a.pml[A1].cid_h[idx[A1]] * d1;
-            a.psiH[C][0][pi] = psi;
-            t1 += a.dth * psi;
-        }
-        const int p2 = a.pml[A2].plane_h[idx[A2]];
-        if (p2 >= 0) {
-            const long long pi = psi_index<A2>(a, p2, i, j, k);
-            float psi = a.psiH[C][1][pi];
-            psi = psi + a.pml[A2].bm1_h[idx[A2]] * psi + a.pml[A2].cid_h[idx[A2]] * d2;
-            a.psiH[C][1][pi] = psi;
-            t2 += a.dth * psi;
-        }
-    }
-    a.H[C][q] -= t1 - t2;
+constexpr int kMarch = 4;   // node planes per thread along x (values of the previous plane stay in registers)
+
+// CPML auxiliary recursion psi += (b-1) psi + (c/d) diff, written back; returns psi
+__device__ __forceinline__ float psi_step(float *__restrict__ arr, long long idx, float bm1, float cid, float diff) {
+    float psi = arr[idx];
+    psi = psi + bm1 * psi + cid * diff;
+    arr[idx] = psi;
+    return psi;
 }
 
-__global__ void __launch_bounds__(kBlock) k_update_h(const StepArgs a, int i0) {
-    const int i = i0 + blockIdx.y;
+// H_c -= dt/mu0 [ (dE_{c+2}/dx_{c+1} + psi_{c,0}) - (dE_{c+1}/dx_{c+2} + psi_{c,1}) ]
+// (reference sim.c:579-606 bulk, :680-754 CPML). A thread owns one (j,k) and
+// marches over kMarch node planes; all loads of a plane are issued before
+// its arithmetic, with neighbour offsets clamped in range where the
+// component does not exist.
+__global__ void __launch_bounds__(kBlock, 4) k_update_h(const StepArgs a, int i0, int i1) {
     const int m = blockIdx.x * kBlock + threadIdx.x;
     if (m >= a.g.plane) return;
     const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
     const int k = m - j * a.g.sj;
-    const long long q = (long long)i * a.g.si + m;
-    h_component<0>(a, i, j, k, q);
-    h_component<1>(a, i, j, k, q);
-    h_component<2>(a, i, j, k, q);
+    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
+    const long long si = a.g.si;
+    const int ib = i0 + blockIdx.y * kMarch, ie = min(ib + kMarch, i1);
+    const float *__restrict__ Ex = a.E[0];
+    const float *__restrict__ Ey = a.E[1];
+    const float *__restrict__ Ez = a.E[2];
+    float *__restrict__ Hx = a.H[0];
+    float *__restrict__ Hy = a.H[1];
+    float *__restrict__ Hz = a.H[2];
+    const bool okx = j < ny && k < nz;   // Hx: all i <= nx
+    const bool oky = k < nz;             // Hy: j <= ny, i < nx
+    const bool okz = j < ny;             // Hz: k <= nz, i < nx
+    const int djp = j < ny ? a.g.sj : 0, dkp = k < nz ? 1 : 0;
+    const float hcy = a.hc[1][min(j, ny - 1)], hcz = a.hc[2][min(k, nz - 1)];
+    int phj = -1, phk = -1;
+    float bj = 0, cj = 0, bk = 0, ck = 0;
+    if (a.has_pml) {
+        if (j < ny) { phj = a.pml[1].plane_h[j]; bj = a.pml[1].bm1_h[j]; cj = a.pml[1].cid_h[j]; }
+        if (k < nz) { phk = a.pml[2].plane_h[k]; bk = a.pml[2].bm1_h[k]; ck = a.pml[2].cid_h[k]; }
+    }
+    long long q = (long long)ib * si + m;
+    float ex = Ex[q], ey = Ey[q], ez = Ez[q];
+    for (int i = ib; i < ie; i++, q += si) {
+        const bool nxt = i < nx;
+        const long long qn = nxt ? q + si : q;
+        const float ex1 = Ex[qn], ey1 = Ey[qn], ez1 = Ez[qn];
+        const float ez_jp = Ez[q + djp], ex_jp = Ex[q + djp];
+        const float ey_kp = Ey[q + dkp], ex_kp = Ex[q + dkp];
+        const float hx = Hx[q], hy = Hy[q], hz = Hz[q];
+        const int ic = min(i, nx - 1);
+        const float hcx = a.hc[0][ic];
+        int phi = -1;
+        float bi = 0, ci = 0;
+        if (a.has_pml && nxt) { phi = a.pml[0].plane_h[i]; bi = a.pml[0].bm1_h[i]; ci = a.pml[0].cid_h[i]; }
+        if (okx) {
+            const float d1 = ez_jp - ez, d2 = ey_kp - ey;
+            float t1 = d1 * hcy, t2 = d2 * hcz;
+            if (phj >= 0) t1 += a.dth * psi_step(a.psiH[0][0], phj * a.pml[1].per + (long long)i * (nz + 1) + k, bj, cj, d1);
+            if (phk >= 0) t2 += a.dth * psi_step(a.psiH[0][1], ((long long)i * (ny + 1) + j) * a.pml[2].planes + phk, bk, ck, d2);
+            Hx[q] = hx - (t1 - t2);
+        }
+        if (oky && nxt) {
+            const float d1 = ex_kp - ex, d2 = ez1 - ez;
+            float t1 = d1 * hcz, t2 = d2 * hcx;
+            if (phk >= 0) t1 += a.dth * psi_step(a.psiH[1][0], ((long long)i * (ny + 1) + j) * a.pml[2].planes + phk, bk, ck, d1);
+            if (phi >= 0) t2 += a.dth * psi_step(a.psiH[1][1], phi * a.pml[0].per + (long long)j * (nz + 1) + k, bi, ci, d2);
+            Hy[q] = hy - (t1 - t2);
+        }
+        if (okz && nxt) {
+            const float d1 = ey1 - ey, d2 = ex_jp - ex;
+            float t1 = d1 * hcx, t2 = d2 * hcy;
+            if (phi >= 0) t1 += a.dth * psi_step(a.psiH[2][0], phi * a.pml[0].per + (long long)j * (nz + 1) + k, bi, ci, d1);
+            if (phj >= 0) t2 += a.dth * psi_step(a.psiH[2][1], phj * a.pml[1].per + (long long)i * (nz + 1) + k, bj, cj, d2);
+            Hz[q] = hz - (t1 - t2);
+        }
+        ex = ex1; ey = ey1; ez = ez1;
+    }
 }
 
 // ---------------------------------------------------------------- E update
 
-// E_C = E + (ca-1) E + cb [ (dH_{C+2}/dx_{C+1} + psi0) - (dH_{C+1}/dx_{C+2} + psi1) - sum_p hk_p J_p ]
-//       + cs Vs(t) + w Vm(t);   J_p += -(1-k_p) J_p + beta_p/dt (E_new - E_old)
+// Per-edge epilogue: material table, Debye correction and update, sources.
+//   E = E + (ca-1) E + cb [curl - sum_p hk_p J_p] + cs Vs(t) + w Vm(t)
+//   J_p += -(1-k_p) J_p + beta_p/dt (E_new - E_old)
+// (reference sim.c:608-637, :894-910; dispersive.c:93-112; modeport.c:130-135)
 template <int C>
-__device__ __forceinline__ void e_component(const StepArgs &a, int i, int j, int k, long long q, long long step) {
-    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
-    const int idx[3] = {i, j, k};
-    if (idx[C] >= a.g.n[C]) return;
-    if (idx[A1] < 1 || idx[A1] >= a.g.n[A1] || idx[A2] < 1 || idx[A2] >= a.g.n[A2]) return;
-    const float *HA2 = a.H[A2], *HA1 = a.H[A1];
-    const float d1 = HA2[q] - HA2[q - axis_stride<A1>(a.g)];
-    const float d2 = HA1[q] - HA1[q - axis_stride<A2>(a.g)];
-    float t1 = d1 * a.ec[A1][idx[A1]];
-    float t2 = d2 * a.ec[A2][idx[A2]];
-    if (a.has_pml) {
-        const int p1 = a.pml[A1].plane_e[idx[A1]];
-        if (p1 >= 0) {
-            const long long pi = psi_index<A1>(a, p1, i, j, k);
-            float psi = a.psiE[C][0][pi];
-            psi = psi + a.pml[A1].bm1_e[idx[A1]] * psi + a.pml[A1].cid_e[idx[A1]] * d1;
-            a.psiE[C][0][pi] = psi;
-            t1 += psi;
-        }
-        const int p2 = a.pml[A2].plane_e[idx[A2]];
-        if (p2 >= 0) {
-            const long long pi = psi_index<A2>(a, p2, i, j, k);
-            float psi = a.psiE[C][1][pi];
-            psi = psi + a.pml[A2].bm1_e[idx[A2]] * psi + a.pml[A2].cid_e[idx[A2]] * d2;
-            a.psiE[C][1][pi] = psi;
-            t2 += psi;
-        }
-    }
-    const int mi = a.mat[C][q];
+__device__ __forceinline__ float e_finish(const StepArgs &a, int mi, float e_old, float curl, int i, int j, int k,
+                                          long long step) {
     const int nt = a.ntab[C];
-    const float *tab = a.tab[C];
+    const float *__restrict__ tab = a.tab[C];
     const float cam1 = __ldg(tab + mi), cb = __ldg(tab + nt + mi);
     const unsigned flag = __ldg(a.tflag[C] + mi);
-    const float e_old = a.E[C][q];
-    float curl = t1 - t2;
+    if (!flag) return fmaf(cam1, e_old, e_old) + cb * curl;
     long long jo = 0, jvol = 0;
+    float *__restrict__ J = a.J[C];
     if (flag & kFlagDisp) {
         const int *bx = a.jbox[C];
         jvol = (long long)bx[3] * bx[4] * bx[5];
         jo = ((long long)(i - bx[0]) * bx[4] + (j - bx[1])) * bx[5] + (k - bx[2]);
         float acc = 0.f;
-        for (int p = 0; p < a.npole; p++) acc += a.hk[p] * a.J[C][p * jvol + jo];
+        for (int p = 0; p < a.npole; p++) acc += a.hk[p] * J[p * jvol + jo];
         curl -= acc;
     }
     float e = fmaf(cam1, e_old, e_old) + cb * curl;
@@ -259,24 +255,84 @@ __device__ __forceinline__ void e_component(const StepArgs &a, int i, int j, int
         const float de = e - e_old;
         for (int p = 0; p < a.npole; p++) {
             const float bidt = __ldg(tab + (3 + p) * nt + mi);
-            const float jp = a.J[C][p * jvol + jo];
-            a.J[C][p * jvol + jo] = jp - a.omk[p] * jp + bidt * de;
+            const float jp = J[p * jvol + jo];
+            J[p * jvol + jo] = jp - a.omk[p] * jp + bidt * de;
         }
     }
-    a.E[C][q] = e;
+    return e;
 }
 
-__global__ void __launch_bounds__(kBlock) k_update_e(const StepArgs a, int i0) {
-    const int i = i0 + blockIdx.y;
+// E_c = ca E + cb [ (dH_{c+2}/dx_{c+1} + psi_{c,0}) - (dH_{c+1}/dx_{c+2} + psi_{c,1}) ] and the
+// epilogue above; same thread layout as k_update_h.
+__global__ void __launch_bounds__(kBlock, 3) k_update_e(const StepArgs a, int i0, int i1) {
     const int m = blockIdx.x * kBlock + threadIdx.x;
     if (m >= a.g.plane) return;
     const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
     const int k = m - j * a.g.sj;
-    const long long q = (long long)i * a.g.si + m;
+    const int ny = a.g.n[1], nz = a.g.n[2];
+    const long long si = a.g.si;
+    const int ib = i0 + blockIdx.y * kMarch, ie = min(ib + kMarch, i1);
+    const float *__restrict__ Hx = a.H[0];
+    const float *__restrict__ Hy = a.H[1];
+    const float *__restrict__ Hz = a.H[2];
+    float *__restrict__ Ex = a.E[0];
+    float *__restrict__ Ey = a.E[1];
+    float *__restrict__ Ez = a.E[2];
+    const unsigned short *__restrict__ M0 = a.mat[0];
+    const unsigned short *__restrict__ M1 = a.mat[1];
+    const unsigned short *__restrict__ M2 = a.mat[2];
+    const bool jin = j >= 1 && j < ny, kin = k >= 1 && k < nz;
+    const bool okx = jin && kin;     // Ex: i < nx
+    const bool oky = j < ny && kin;  // Ey: 1 <= i < nx
+    const bool okz = jin && k < nz;  // Ez: 1 <= i < nx
+    const int djm = j >= 1 ? a.g.sj : 0, dkm = k >= 1 ? 1 : 0;
+    const float ecy = a.ec[1][j], ecz = a.ec[2][k];
+    int pej = -1, pek = -1;
+    float bj = 0, cj = 0, bk = 0, ck = 0;
+    if (a.has_pml) {
+        pej = a.pml[1].plane_e[j]; bj = a.pml[1].bm1_e[j]; cj = a.pml[1].cid_e[j];
+        pek = a.pml[2].plane_e[k]; bk = a.pml[2].bm1_e[k]; ck = a.pml[2].cid_e[k];
+    }
     const long long step = *a.dstep;
-    e_component<0>(a, i, j, k, q, step);
-    e_component<1>(a, i, j, k, q, step);
-    e_component<2>(a, i, j, k, q, step);
+    long long q = (long long)ib * si + m;
+    const long long qp = ib >= 1 ? q - si : q;
+    float hy_p = Hy[qp], hz_p = Hz[qp];
+    for (int i = ib; i < ie; i++, q += si) {
+        const float hx = Hx[q], hy = Hy[q], hz = Hz[q];
+        const float hz_jm = Hz[q - djm], hx_jm = Hx[q - djm];
+        const float hy_km = Hy[q - dkm], hx_km = Hx[q - dkm];
+        const float ex = Ex[q], ey = Ey[q], ez = Ez[q];
+        const int m0 = M0[q], m1 = M1[q], m2 = M2[q];
+        const float ecx = a.ec[0][i];
+        int pei = -1;
+        float bi = 0, ci = 0;
+        if (a.has_pml) { pei = a.pml[0].plane_e[i]; bi = a.pml[0].bm1_e[i]; ci = a.pml[0].cid_e[i]; }
+        if (okx) {
+            const float d1 = hz - hz_jm, d2 = hy - hy_km;
+            float t1 = d1 * ecy, t2 = d2 * ecz;
+            if (pej >= 0) t1 += psi_step(a.psiE[0][0], pej * a.pml[1].per + (long long)i * (nz + 1) + k, bj, cj, d1);
+            if (pek >= 0) t2 += psi_step(a.psiE[0][1], ((long long)i * (ny + 1) + j) * a.pml[2].planes + pek, bk, ck, d2);
+            Ex[q] = e_finish<0>(a, m0, ex, t1 - t2, i, j, k, step);
+        }
+        if (i >= 1) {
+            if (oky) {
+                const float d1 = hx - hx_km, d2 = hz - hz_p;
+                float t1 = d1 * ecz, t2 = d2 * ecx;
+                if (pek >= 0) t1 += psi_step(a.psiE[1][0], ((long long)i * (ny + 1) + j) * a.pml[2].planes + pek, bk, ck, d1);
+                if (pei >= 0) t2 += psi_step(a.psiE[1][1], pei * a.pml[0].per + (long long)j * (nz + 1) + k, bi, ci, d2);
+                Ey[q] = e_finish<1>(a, m1, ey, t1 - t2, i, j, k, step);
+            }
+            if (okz) {
+                const float d1 = hy - hy_p, d2 = hx - hx_jm;
+                float t1 = d1 * ecx, t2 = d2 * ecy;
+                if (pei >= 0) t1 += psi_step(a.psiE[2][0], pei * a.pml[0].per + (long long)j * (nz + 1) + k, bi, ci, d1);
+                if (pej >= 0) t2 += psi_step(a.psiE[2][1], pej * a.pml[1].per + (long long)i * (nz + 1) + k, bj, cj, d2);
+                Ez[q] = e_finish<2>(a, m2, ez, t1 - t2, i, j, k, step);
+            }
+        }
+        hy_p = hy;
+        hz_p = hz;
+    }
 }
 
 // ------------------------------------------------------------------- SIBC
@@ -350,9 +406,11 @@ __global__ void __launch_bounds__(kBlock) k_post(const PostArgs a) {
     if (threadIdx.x == 0) *a.dstep = step + 1;
 }
 
-// acc[slot][f] += sum over the pending rows of (sample * dt) e^{-j w t}, t the
-// slot's sampling time: (n + 1/2) dt for H-time slots, (n + 1) dt for the
-// voltage probes (reference sim.c:840-861,872-933).
+// acc[slot][f] += (sample * dt) e^{-j w t} for each pending row in step order,
+// t the slot's sampling time: (n + 1/2) dt for H-time slots, (n + 1) dt for
+// the voltage probes (reference sim.c:840-861,872-933). Adding row by row
+// into the accumulator, as the reference does, makes the result independent
+// of where the ring was flushed (checkpoint resume stays bit-exact).
 __global__ void k_dft(const double *ring, int nslot, int first_e_slot, long long step0, int count, double dt,
                       const double *omega, int nf, double *acc) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -360,7 +418,8 @@ __global__ void k_dft(const double *ring, int nslot, int first_e_slot, long long
     if (f >= nf) return;
     const double w = omega[f];
     const double toff = s >= first_e_slot ? 1.0 : 0.5;
-    double re = 0, im = 0;
+    double *a = acc + (long long)s * 2 * nf + 2 * f;
+    double re = a[0], im = a[1];
     for (int r = 0; r < count; r++) {
         const long long n = step0 + r;
         const double v = ring[(n % kRing) * nslot + s] * dt;
@@ -369,8 +428,8 @@ __global__ void k_dft(const double *ring, int nslot, int first_e_slot, long long
         re += v * cs;
         im += v * -sn;
     }
-    acc[(long long)s * 2 * nf + 2 * f] += re;
-    acc[(long long)s * 2 * nf + 2 * f + 1] += im;
+    a[0] = re;
+    a[1] = im;
 }
 
 // ----------------------------------------------------------------- energy
@@ -462,6 +521,7 @@ struct Device {
     DevBuf<float> bm1_h[3], cid_h[3], bm1_e[3], cid_e[3];
     DevBuf<float> psiH[3][2], psiE[3][2];
     size_t psi_len_h[3][2] = {}, psi_len_e[3][2] = {};
+    int zplanes = 0;   // planes of the z CPML slabs (same count for cells and nodes)
     DevBuf<unsigned short> mat[3];
     DevBuf<float> tab[3];
     DevBuf<unsigned char> tflag[3];
@@ -712,6 +772,12 @@ bool build_pml(cem_sim *s, Device &D) {
             !dev_upload(s, D.cid_h[a], chh) || !dev_upload(s, D.bm1_e[a], be) || !dev_upload(s, D.cid_e[a], cee))
             return false;
     }
+    {
+        int r[2][2], planes = 0;
+        pml_ranges(s, 2, 0, r);
+        for (int sd = 0; sd < 2; sd++) planes += r[sd][1] >= r[sd][0] ? r[sd][1] - r[sd][0] + 1 : 0;
+        D.zplanes = planes;
+    }
     for (int c = 0; c < 3; c++)
         for (int w = 0; w < 2; w++) {
             D.psi_len_h[c][w] = psi_len(s, 0, c, w);
@@ -805,7 +871,7 @@ void fill_args(cem_sim *s, Device &D) {
         a.hc[c] = D.hc[c].p;
         a.ec[c] = D.ec[c].p;
         a.pml[c] = PmlAxis{D.plane_h[c].p, D.plane_e[c].p, D.bm1_h[c].p, D.cid_h[c].p, D.bm1_e[c].p, D.cid_e[c].p,
-                           (long long)pml_per(s, c)};
+                           (long long)pml_per(s, c), D.zplanes};
         for (int w = 0; w < 2; w++) {
             a.psiH[c][w] = D.psiH[c][w].p;
             a.psiE[c][w] = D.psiE[c][w].p;
@@ -971,6 +1037,27 @@ bool flush_dft(cem_sim *s) {
     return true;
 }
 
+// reference compact layout <-> device layout (z-axis slabs transposed)
+bool psi_is_z(int c, int w) { return (c + w + 1) % 3 == 2; }
+
+std::vector<double> psi_to_device(const cem_sim *s, const Device &D, int c, int w, const std::vector<double> &v) {
+    if (!psi_is_z(c, w) || v.empty()) return v;
+    const size_t per = pml_per(s, 2), P = (size_t)D.zplanes;
+    std::vector<double> o(v.size());
+    for (size_t pl = 0; pl < P; pl++)
+        for (size_t x = 0; x < per; x++) o[x * P + pl] = v[pl * per + x];
+    return o;
+}
+
+void psi_to_host(const cem_sim *s, const Device &D, int c, int w, std::vector<double> &v) {
+    if (!psi_is_z(c, w) || v.empty()) return;
+    const size_t per = pml_per(s, 2), P = (size_t)D.zplanes;
+    std::vector<double> o(v.size());
+    for (size_t pl = 0; pl < P; pl++)
+        for (size_t x = 0; x < per; x++) o[pl * per + x] = v[x * P + pl];
+    v.swap(o);
+}
+
 bool upload_group(cem_sim *s, unsigned g, bool from_host) {
     Device &D = *s->dev;
     const size_t N = s->N;
@@ -989,8 +1076,8 @@ bool upload_group(cem_sim *s, unsigned g, bool from_host) {
         for (int c = 0; c < 3; c++)
             for (int w = 0; w < 2; w++) {
                 if (from_host) {
-                    if (!upload_f32(s, D.psiE[c][w].p, s->psiE[c][w], D.psi_len_e[c][w]) ||
-                        !upload_f32(s, D.psiH[c][w].p, s->psiH[c][w], D.psi_len_h[c][w]))
+                    if (!upload_f32(s, D.psiE[c][w].p, psi_to_device(s, D, c, w, s->psiE[c][w]), D.psi_len_e[c][w]) ||
+                        !upload_f32(s, D.psiH[c][w].p, psi_to_device(s, D, c, w, s->psiH[c][w]), D.psi_len_h[c][w]))
                         return false;
                 } else if (!zero_dev(s, D.psiE[c][w].p, D.psiE[c][w].n * 4) ||
                            !zero_dev(s, D.psiH[c][w].p, D.psiH[c][w].n * 4)) {
@@ -1053,6 +1140,10 @@ bool download_group(cem_sim *s, unsigned g) {
                 if (!download_f32(s, s->psiE[c][w], D.psiE[c][w].p, D.psi_len_e[c][w]) ||
                     !download_f32(s, s->psiH[c][w], D.psiH[c][w].p, D.psi_len_h[c][w]))
                     return false;
+                else {
+                    psi_to_host(s, D, c, w, s->psiE[c][w]);
+                    psi_to_host(s, D, c, w, s->psiH[c][w]);
+                }
     if (g & kGroupDebye) {
         s->d_J.assign((size_t)s->npole * s->ndisp, 0.0);
         if (s->d_Eold.size() != (size_t)s->ndisp) s->d_Eold.assign(s->ndisp, 0.0);
@@ -1132,7 +1223,11 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
     const int gx = (D.g.plane + kBlock - 1) / kBlock;
     if (phase_mask & 1) {   // H over node planes [i0, i1) within [0, nx]
         const int a = std::max(0, i0), b = std::min(nx + 1, i1);
-        if (b > a) { t_begin(0); k_update_h<<<dim3(gx, b - a), blk, 0, D.stream>>>(D.sa, a); t_end(); }
+        if (b > a) {
+            t_begin(0);
+            k_update_h<<<dim3(gx, (b - a + kMarch - 1) / kMarch), blk, 0, D.stream>>>(D.sa, a, b);
+            t_end();
+        }
     }
     if (phase_mask & 2) {   // port voltages before the E update
         D.pa.advance = 0;
@@ -1140,7 +1235,11 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
     }
     if (phase_mask & 4) {   // E over node planes [i0, i1) within [0, nx)
         const int a = std::max(0, i0), b = std::min(nx, i1);
-        if (b > a) { t_begin(1); k_update_e<<<dim3(gx, b - a), blk, 0, D.stream>>>(D.sa, a); t_end(); }
+        if (b > a) {
+            t_begin(1);
+            k_update_e<<<dim3(gx, (b - a + kMarch - 1) / kMarch), blk, 0, D.stream>>>(D.sa, a, b);
+            t_end();
+        }
     }
     if (phase_mask & 8) {   // surface impedance, probes, step count
         if (D.ring_count == kRing && !flush_dft(s)) return false;

