@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <unordered_map>
@@ -56,7 +57,7 @@ struct PmlAxis {
     const int *plane_h, *plane_e;        // CPML plane of a cell / node, -1 outside
     const float *bm1_h, *cid_h;          // b-1 and c/d at cells (H auxiliaries)
     const float *bm1_e, *cid_e;          // b-1 and c/dd at nodes (E auxiliaries)
-    long long per;                       // points per plane
+    int per;                             // points per plane
     int planes;                          // planes in the CPML slabs of this axis (z-axis layout stride)
 };
 
@@ -75,7 +76,8 @@ struct StepArgs {
     PmlAxis pml[3];
     float *psiH[3][2], *psiE[3][2];
     const unsigned short *mat[3];
-    const float *tab[3];
+    const float *tab[3];          // field-major: ca-1, cb, cs, beta_p/dt (p = 0..P-1)
+    const float4 *tab4[3];        // packed per entry: ca-1, cb, cs, flags (bit pattern)
     const unsigned char *tflag[3];
     int ntab[3];
     int npole;
@@ -101,6 +103,14 @@ struct SibcArgs {
     float c[kSibcTerms], ome[kSibcTerms];
     float *E[3];
     const float *H[3];
+};
+
+// buffers of one fused step: read the old, write the new
+struct FusedArgs {
+    const float *Eo[3], *Ho[3];
+    float *En[3], *Hn[3];
+    float *psiHo[3][2];   // read only
+    float *psiHn[3][2];
 };
 
 struct PostArgs {
@@ -134,88 +144,113 @@ __device__ __forceinline__ double dgauss(double t, double t0, double tau) {
     return -2 * x * exp(-x * x);
 }
 
-// ---------------------------------------------------------------- H update
+// ------------------------------------------------- per-point arithmetic
+//
+// The H and E updates of one point are written once, with explicit
+// round-to-nearest intrinsics (no contraction left to the compiler), and
+// shared by the fused step and the separate phase kernels: both give the
+// same bits, as cem_step and the cem_mt_* phases do in the reference
+// (sim.c:863-866).
 
-constexpr int kMarch = 4;   // node planes per thread along x (values of the previous plane stay in registers)
-
-// CPML auxiliary recursion psi += (b-1) psi + (c/d) diff, written back; returns psi
-__device__ __forceinline__ float psi_step(float *__restrict__ arr, long long idx, float bm1, float cid, float diff) {
-    float psi = arr[idx];
-    psi = psi + bm1 * psi + cid * diff;
-    arr[idx] = psi;
-    return psi;
+// CPML recursion psi' = psi + (b-1) psi + (c/d) diff
+__device__ __forceinline__ float psi_next(float psi, float bm1, float cid, float diff) {
+    return __fmaf_rn(bm1, psi, __fmaf_rn(cid, diff, psi));
 }
 
-// H_c -= dt/mu0 [ (dE_{c+2}/dx_{c+1} + psi_{c,0}) - (dE_{c+1}/dx_{c+2} + psi_{c,1}) ]
-// (reference sim.c:579-606 bulk, :680-754 CPML). A thread owns one (j,k) and
-// marches over kMarch node planes; all loads of a plane are issued before
-// its arithmetic, with neighbour offsets clamped in range where the
-// component does not exist.
-__global__ void __launch_bounds__(kBlock, 4) k_update_h(const StepArgs a, int i0, int i1) {
-    const int m = blockIdx.x * kBlock + threadIdx.x;
-    if (m >= a.g.plane) return;
-    const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
-    const int k = m - j * a.g.sj;
-    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
-    const long long si = a.g.si;
-    const int ib = i0 + blockIdx.y * kMarch, ie = min(ib + kMarch, i1);
-    const float *__restrict__ Ex = a.E[0];
-    const float *__restrict__ Ey = a.E[1];
-    const float *__restrict__ Ez = a.E[2];
-    float *__restrict__ Hx = a.H[0];
-    float *__restrict__ Hy = a.H[1];
-    float *__restrict__ Hz = a.H[2];
-    const bool okx = j < ny && k < nz;   // Hx: all i <= nx
-    const bool oky = k < nz;             // Hy: j <= ny, i < nx
-    const bool okz = j < ny;             // Hz: k <= nz, i < nx
-    const int djp = j < ny ? a.g.sj : 0, dkp = k < nz ? 1 : 0;
-    const float hcy = a.hc[1][min(j, ny - 1)], hcz = a.hc[2][min(k, nz - 1)];
-    int phj = -1, phk = -1;
-    float bj = 0, cj = 0, bk = 0, ck = 0;
+// Values of a (j,k) column that stay fixed while a thread marches along x:
+// update coefficients and CPML plane indices (-1 outside the slabs).
+struct Column {
+    float hcy, hcz, ecy, ecz;
+    int phj, phk, pej, pek;
+};
+
+__device__ __forceinline__ Column column_at(const StepArgs &a, int j, int k) {
+    const int ny = a.g.n[1], nz = a.g.n[2];
+    Column c;
+    c.hcy = j < ny ? a.hc[1][j] : 0.f;
+    c.hcz = k < nz ? a.hc[2][k] : 0.f;
+    c.ecy = a.ec[1][j];
+    c.ecz = a.ec[2][k];
+    c.phj = c.phk = c.pej = c.pek = -1;
     if (a.has_pml) {
-        if (j < ny) { phj = a.pml[1].plane_h[j]; bj = a.pml[1].bm1_h[j]; cj = a.pml[1].cid_h[j]; }
-        if (k < nz) { phk = a.pml[2].plane_h[k]; bk = a.pml[2].bm1_h[k]; ck = a.pml[2].cid_h[k]; }
+        if (j < ny) c.phj = a.pml[1].plane_h[j];
+        if (k < nz) c.phk = a.pml[2].plane_h[k];
+        c.pej = a.pml[1].plane_e[j];
+        c.pek = a.pml[2].plane_e[k];
     }
-    long long q = (long long)ib * si + m;
-    float ex = Ex[q], ey = Ey[q], ez = Ez[q];
-    for (int i = ib; i < ie; i++, q += si) {
-        const bool nxt = i < nx;
-        const long long qn = nxt ? q + si : q;
-        const float ex1 = Ex[qn], ey1 = Ey[qn], ez1 = Ez[qn];
-        const float ez_jp = Ez[q + djp], ex_jp = Ex[q + djp];
-        const float ey_kp = Ey[q + dkp], ex_kp = Ex[q + dkp];
-        const float hx = Hx[q], hy = Hy[q], hz = Hz[q];
-        const int ic = min(i, nx - 1);
-        const float hcx = a.hc[0][ic];
-        int phi = -1;
-        float bi = 0, ci = 0;
-        if (a.has_pml && nxt) { phi = a.pml[0].plane_h[i]; bi = a.pml[0].bm1_h[i]; ci = a.pml[0].cid_h[i]; }
-        if (okx) {
-            const float d1 = ez_jp - ez, d2 = ey_kp - ey;
-            float t1 = d1 * hcy, t2 = d2 * hcz;
-            if (phj >= 0) t1 += a.dth * psi_step(a.psiH[0][0], phj * a.pml[1].per + (long long)i * (nz + 1) + k, bj, cj, d1);
-            if (phk >= 0) t2 += a.dth * psi_step(a.psiH[0][1], ((long long)i * (ny + 1) + j) * a.pml[2].planes + phk, bk, ck, d2);
-            Hx[q] = hx - (t1 - t2);
-        }
-        if (oky && nxt) {
-            const float d1 = ex_kp - ex, d2 = ez1 - ez;
-            float t1 = d1 * hcz, t2 = d2 * hcx;
-            if (phk >= 0) t1 += a.dth * psi_step(a.psiH[1][0], ((long long)i * (ny + 1) + j) * a.pml[2].planes + phk, bk, ck, d1);
-            if (phi >= 0) t2 += a.dth * psi_step(a.psiH[1][1], phi * a.pml[0].per + (long long)j * (nz + 1) + k, bi, ci, d2);
-            Hy[q] = hy - (t1 - t2);
-        }
-        if (okz && nxt) {
-            const float d1 = ey1 - ey, d2 = ex_jp - ex;
-            float t1 = d1 * hcx, t2 = d2 * hcy;
-            if (phi >= 0) t1 += a.dth * psi_step(a.psiH[2][0], phi * a.pml[0].per + (long long)j * (nz + 1) + k, bi, ci, d1);
-            if (phj >= 0) t2 += a.dth * psi_step(a.psiH[2][1], phj * a.pml[1].per + (long long)i * (nz + 1) + k, bj, cj, d2);
-            Hz[q] = hz - (t1 - t2);
-        }
-        ex = ex1; ey = ey1; ez = ez1;
-    }
+    return c;
 }
 
-// ---------------------------------------------------------------- E update
+// Values of node plane i, the same for every thread of the plane.
+struct Plane {
+    float hcx, ecx;
+    int phi, pei;
+};
+
+__device__ __forceinline__ Plane plane_at(const StepArgs &a, int i) {
+    const int nx = a.g.n[0];
+    Plane p;
+    p.hcx = i < nx ? a.hc[0][i] : 0.f;
+    p.ecx = a.ec[0][i];
+    p.phi = a.has_pml && i < nx ? a.pml[0].plane_h[i] : -1;
+    p.pei = a.has_pml ? a.pml[0].plane_e[i] : -1;
+    return p;
+}
+
+// compact index of a CPML auxiliary for derivative axis A (device layout, see PmlAxis)
+template <int A>
+__device__ __forceinline__ int psi_at(const StepArgs &a, int plane, int i, int j, int k) {
+    if (A == 0) return plane * a.pml[0].per + j * (a.g.n[2] + 1) + k;
+    if (A == 1) return plane * a.pml[1].per + i * (a.g.n[2] + 1) + k;
+    return (i * (a.g.n[1] + 1) + j) * a.pml[2].planes + plane;
+}
+
+// H component C at (i, j, k) (reference sim.c:579-606, CPML :680-754):
+//   H_C -= dt/mu0 [ (d1 c1 + psi_{C,0}) - (d2 c2 + psi_{C,1}) ]
+// with d1 = dE_{C+2} along axis C+1, d2 = dE_{C+1} along axis C+2, c1, c2 the
+// kappa-scaled inverse cell sizes times dt/mu0, p1, p2 the CPML planes of the
+// two derivative axes (-1 outside). psi read from `pin`, written to `pout`
+// when STORE.
+template <int C, bool STORE>
+__device__ __forceinline__ float h_comp(const StepArgs &a, float *const (&pin)[3][2], float *const (&pout)[3][2],
+                                        int i, int j, int k, float h, float d1, float d2, float c1, float c2, int p1,
+                                        int p2) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    const int idx[3] = {i, j, k};
+    float t1 = __fmul_rn(d1, c1), t2 = __fmul_rn(d2, c2);
+    if (p1 >= 0) {
+        const int x = psi_at<A1>(a, p1, i, j, k);
+        const float psi = psi_next(pin[C][0][x], a.pml[A1].bm1_h[idx[A1]], a.pml[A1].cid_h[idx[A1]], d1);
+        if (STORE) pout[C][0][x] = psi;
+        t1 = __fmaf_rn(a.dth, psi, t1);
+    }
+    if (p2 >= 0) {
+        const int x = psi_at<A2>(a, p2, i, j, k);
+        const float psi = psi_next(pin[C][1][x], a.pml[A2].bm1_h[idx[A2]], a.pml[A2].cid_h[idx[A2]], d2);
+        if (STORE) pout[C][1][x] = psi;
+        t2 = __fmaf_rn(a.dth, psi, t2);
+    }
+    return __fsub_rn(h, __fsub_rn(t1, t2));
+}
+
+// All three H components at (i, j, k) for the fused step. e*: E at the point;
+// *_jp, *_kp: at j+1, k+1; ey1, ez1: at i+1. h* in: old, out: new.
+template <bool STORE>
+__device__ __forceinline__ void h_point(const StepArgs &a, const Column &col, const Plane &pl,
+                                        float *const (&pin)[3][2], float *const (&pout)[3][2], int i, int j, int k,
+                                        float ex, float ey, float ez, float ez_jp, float ex_jp, float ey_kp,
+                                        float ex_kp, float ey1, float ez1, float &hx, float &hy, float &hz) {
+    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
+    if (j < ny && k < nz)
+        hx = h_comp<0, STORE>(a, pin, pout, i, j, k, hx, __fsub_rn(ez_jp, ez), __fsub_rn(ey_kp, ey), col.hcy, col.hcz,
+                              col.phj, col.phk);
+    if (k < nz && i < nx)
+        hy = h_comp<1, STORE>(a, pin, pout, i, j, k, hy, __fsub_rn(ex_kp, ex), __fsub_rn(ez1, ez), col.hcz, pl.hcx,
+                              col.phk, pl.phi);
+    if (j < ny && i < nx)
+        hz = h_comp<2, STORE>(a, pin, pout, i, j, k, hz, __fsub_rn(ey1, ey), __fsub_rn(ex_jp, ex), pl.hcx, col.hcy,
+                              pl.phi, col.phj);
+}
 
 // Per-edge epilogue: material table, Debye correction and update, sources.
 //   E = E + (ca-1) E + cb [curl - sum_p hk_p J_p] + cs Vs(t) + w Vm(t)
@@ -224,114 +259,316 @@ __global__ void __launch_bounds__(kBlock, 4) k_update_h(const StepArgs a, int i0
 template <int C>
 __device__ __forceinline__ float e_finish(const StepArgs &a, int mi, float e_old, float curl, int i, int j, int k,
                                           long long step) {
+    const float4 t = __ldg(a.tab4[C] + mi);   // ca-1, cb, cs, flags
+    const unsigned flag = __float_as_uint(t.w);
+    const float base = __fmaf_rn(t.x, e_old, e_old);
+    if (!flag) return __fmaf_rn(t.y, curl, base);
     const int nt = a.ntab[C];
     const float *__restrict__ tab = a.tab[C];
-    const float cam1 = __ldg(tab + mi), cb = __ldg(tab + nt + mi);
-    const unsigned flag = __ldg(a.tflag[C] + mi);
-    if (!flag) return fmaf(cam1, e_old, e_old) + cb * curl;
-    long long jo = 0, jvol = 0;
+    int jo = 0, jvol = 0;
     float *__restrict__ J = a.J[C];
     if (flag & kFlagDisp) {
         const int *bx = a.jbox[C];
-        jvol = (long long)bx[3] * bx[4] * bx[5];
-        jo = ((long long)(i - bx[0]) * bx[4] + (j - bx[1])) * bx[5] + (k - bx[2]);
+        jvol = bx[3] * bx[4] * bx[5];
+        jo = ((i - bx[0]) * bx[4] + (j - bx[1])) * bx[5] + (k - bx[2]);
         float acc = 0.f;
-        for (int p = 0; p < a.npole; p++) acc += a.hk[p] * J[p * jvol + jo];
-        curl -= acc;
+        for (int p = 0; p < a.npole; p++) acc = __fmaf_rn(a.hk[p], J[p * jvol + jo], acc);
+        curl = __fsub_rn(curl, acc);
     }
-    float e = fmaf(cam1, e_old, e_old) + cb * curl;
+    float e = __fmaf_rn(t.y, curl, base);
     if (flag & kFlagSrc) {
         const double tH = ((double)step + 0.5) * a.dt;
-        e += __ldg(tab + 2 * nt + mi) * (float)gauss(tH, a.src_amp, a.src_t0, a.src_tau);
+        e = __fmaf_rn(t.z, (float)gauss(tH, a.src_amp, a.src_t0, a.src_tau), e);
     }
     if (C > 0 && a.msrc_on && i == a.i_src) {
-        const float w = a.wsrc[C - 1][(long long)j * (a.g.n[2] + 1) + k];
+        const float w = a.wsrc[C - 1][j * (a.g.n[2] + 1) + k];
         if (w != 0.f) {
             const double tH = ((double)step + 0.5) * a.dt;
-            e += w * (float)dgauss(tH, a.m_t0, a.m_tau);
+            e = __fmaf_rn(w, (float)dgauss(tH, a.m_t0, a.m_tau), e);
         }
     }
     if (flag & kFlagDisp) {
-        const float de = e - e_old;
+        const float de = __fsub_rn(e, e_old);
         for (int p = 0; p < a.npole; p++) {
             const float bidt = __ldg(tab + (3 + p) * nt + mi);
             const float jp = J[p * jvol + jo];
-            J[p * jvol + jo] = jp - a.omk[p] * jp + bidt * de;
+            J[p * jvol + jo] = __fmaf_rn(bidt, de, __fmaf_rn(-a.omk[p], jp, jp));
         }
     }
     return e;
 }
 
-// E_c = ca E + cb [ (dH_{c+2}/dx_{c+1} + psi_{c,0}) - (dH_{c+1}/dx_{c+2} + psi_{c,1}) ] and the
-// epilogue above; same thread layout as k_update_h.
-__global__ void __launch_bounds__(kBlock, 3) k_update_e(const StepArgs a, int i0, int i1) {
-    const int m = blockIdx.x * kBlock + threadIdx.x;
+// E component C at (i, j, k) (reference sim.c:608-637, CPML :756-832):
+//   E_C = ca E + cb [ (d1 c1 + psi_{C,0}) - (d2 c2 + psi_{C,1}) ] + epilogue
+// with d1 = dH_{C+2} along axis C+1, d2 = dH_{C+1} along axis C+2.
+template <int C>
+__device__ __forceinline__ float e_comp(const StepArgs &a, int i, int j, int k, long long step, float e, float d1,
+                                        float d2, float c1, float c2, int p1, int p2, int mi) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    const int idx[3] = {i, j, k};
+    float t1 = __fmul_rn(d1, c1), t2 = __fmul_rn(d2, c2);
+    if (p1 >= 0) {
+        float *arr = a.psiE[C][0];
+        const int x = psi_at<A1>(a, p1, i, j, k);
+        const float psi = psi_next(arr[x], a.pml[A1].bm1_e[idx[A1]], a.pml[A1].cid_e[idx[A1]], d1);
+        arr[x] = psi;
+        t1 = __fadd_rn(t1, psi);
+    }
+    if (p2 >= 0) {
+        float *arr = a.psiE[C][1];
+        const int x = psi_at<A2>(a, p2, i, j, k);
+        const float psi = psi_next(arr[x], a.pml[A2].bm1_e[idx[A2]], a.pml[A2].cid_e[idx[A2]], d2);
+        arr[x] = psi;
+        t2 = __fadd_rn(t2, psi);
+    }
+    return e_finish<C>(a, mi, e, __fsub_rn(t1, t2), i, j, k, step);
+}
+
+// All three E components at (i, j, k) for the fused step. h*: H at the point;
+// *_jm, *_km: at j-1, k-1; hy_p, hz_p: at i-1. e* in: old, out: new.
+__device__ __forceinline__ void e_point(const StepArgs &a, const Column &col, const Plane &pl, int i, int j, int k,
+                                        long long step, float hx, float hy, float hz, float hz_jm, float hx_jm,
+                                        float hy_km, float hx_km, float hy_p, float hz_p, int m0, int m1, int m2,
+                                        float &ex, float &ey, float &ez) {
+    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
+    if (i >= nx) return;
+    const bool jin = j >= 1 && j < ny, kin = k >= 1 && k < nz;
+    if (jin && kin)
+        ex = e_comp<0>(a, i, j, k, step, ex, __fsub_rn(hz, hz_jm), __fsub_rn(hy, hy_km), col.ecy, col.ecz, col.pej,
+                       col.pek, m0);
+    if (i < 1) return;
+    if (j < ny && kin)
+        ey = e_comp<1>(a, i, j, k, step, ey, __fsub_rn(hx, hx_km), __fsub_rn(hz, hz_p), col.ecz, pl.ecx, col.pek,
+                       pl.pei, m1);
+    if (jin && k < nz)
+        ez = e_comp<2>(a, i, j, k, step, ez, __fsub_rn(hy, hy_p), __fsub_rn(hx, hx_jm), pl.ecx, col.ecy, pl.pei,
+                       col.pej, m2);
+}
+
+// ------------------------------------------------ separate phase kernels
+//
+// One thread per component of one point; the three components of a chunk of
+// a (j,k) plane sit in adjacent blocks, so the neighbour values they share
+// come from L2. Each thread issues its handful of loads before any
+// arithmetic; few registers leave room for many warps per SM.
+
+template <int A>
+__device__ __forceinline__ int stride_of(const StepArgs &a) {
+    return A == 0 ? (int)a.g.si : (A == 1 ? a.g.sj : 1);
+}
+
+template <int C>
+__device__ __forceinline__ void h_one(const StepArgs &a, int i, int j, int k, int q) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    const int idx[3] = {i, j, k};
+    if (idx[A1] >= a.g.n[A1] || idx[A2] >= a.g.n[A2]) return;
+    const float *__restrict__ E2 = a.E[A2];
+    const float *__restrict__ E1 = a.E[A1];
+    float *__restrict__ H = a.H[C];
+    const float e2 = E2[q], e2n = E2[q + stride_of<A1>(a)], e1 = E1[q], e1n = E1[q + stride_of<A2>(a)];
+    const float h = H[q];
+    const float c1 = a.hc[A1][idx[A1]], c2 = a.hc[A2][idx[A2]];
+    const int p1 = a.has_pml ? a.pml[A1].plane_h[idx[A1]] : -1, p2 = a.has_pml ? a.pml[A2].plane_h[idx[A2]] : -1;
+    H[q] = h_comp<C, true>(a, a.psiH, a.psiH, i, j, k, h, __fsub_rn(e2n, e2), __fsub_rn(e1n, e1), c1, c2, p1, p2);
+}
+
+template <int C>
+__device__ __forceinline__ void e_one(const StepArgs &a, int i, int j, int k, int q, long long step) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    const int idx[3] = {i, j, k};
+    if (idx[C] >= a.g.n[C]) return;
+    if (idx[A1] < 1 || idx[A1] >= a.g.n[A1] || idx[A2] < 1 || idx[A2] >= a.g.n[A2]) return;
+    const float *__restrict__ H2 = a.H[A2];
+    const float *__restrict__ H1 = a.H[A1];
+    float *__restrict__ E = a.E[C];
+    const float h2 = H2[q], h2m = H2[q - stride_of<A1>(a)], h1 = H1[q], h1m = H1[q - stride_of<A2>(a)];
+    const float e = E[q];
+    const int mi = a.mat[C][q];
+    const float c1 = a.ec[A1][idx[A1]], c2 = a.ec[A2][idx[A2]];
+    const int p1 = a.has_pml ? a.pml[A1].plane_e[idx[A1]] : -1, p2 = a.has_pml ? a.pml[A2].plane_e[idx[A2]] : -1;
+    E[q] = e_comp<C>(a, i, j, k, step, e, __fsub_rn(h2, h2m), __fsub_rn(h1, h1m), c1, c2, p1, p2, mi);
+}
+
+// H over node planes [i0, i0 + gridDim.y) (cem_mt_H and the unfused step)
+__global__ void __launch_bounds__(kBlock, 8) k_update_h(const StepArgs a, int i0) {
+    const int comp = blockIdx.x % 3;
+    const int m = (blockIdx.x / 3) * kBlock + threadIdx.x;
     if (m >= a.g.plane) return;
+    const int i = i0 + blockIdx.y;
     const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
     const int k = m - j * a.g.sj;
-    const int ny = a.g.n[1], nz = a.g.n[2];
-    const long long si = a.g.si;
-    const int ib = i0 + blockIdx.y * kMarch, ie = min(ib + kMarch, i1);
-    const float *__restrict__ Hx = a.H[0];
-    const float *__restrict__ Hy = a.H[1];
-    const float *__restrict__ Hz = a.H[2];
-    float *__restrict__ Ex = a.E[0];
-    float *__restrict__ Ey = a.E[1];
-    float *__restrict__ Ez = a.E[2];
-    const unsigned short *__restrict__ M0 = a.mat[0];
-    const unsigned short *__restrict__ M1 = a.mat[1];
-    const unsigned short *__restrict__ M2 = a.mat[2];
-    const bool jin = j >= 1 && j < ny, kin = k >= 1 && k < nz;
-    const bool okx = jin && kin;     // Ex: i < nx
-    const bool oky = j < ny && kin;  // Ey: 1 <= i < nx
-    const bool okz = jin && k < nz;  // Ez: 1 <= i < nx
-    const int djm = j >= 1 ? a.g.sj : 0, dkm = k >= 1 ? 1 : 0;
-    const float ecy = a.ec[1][j], ecz = a.ec[2][k];
-    int pej = -1, pek = -1;
-    float bj = 0, cj = 0, bk = 0, ck = 0;
-    if (a.has_pml) {
-        pej = a.pml[1].plane_e[j]; bj = a.pml[1].bm1_e[j]; cj = a.pml[1].cid_e[j];
-        pek = a.pml[2].plane_e[k]; bk = a.pml[2].bm1_e[k]; ck = a.pml[2].cid_e[k];
-    }
+    const int q = i * (int)a.g.si + m;
+    if (comp == 0) h_one<0>(a, i, j, k, q);
+    else if (comp == 1) h_one<1>(a, i, j, k, q);
+    else h_one<2>(a, i, j, k, q);
+}
+
+// E over node planes [i0, i0 + gridDim.y) (cem_mt_E and the unfused step)
+__global__ void __launch_bounds__(kBlock, 6) k_update_e(const StepArgs a, int i0) {
+    const int comp = blockIdx.x % 3;
+    const int m = (blockIdx.x / 3) * kBlock + threadIdx.x;
+    if (m >= a.g.plane) return;
+    const int i = i0 + blockIdx.y;
+    const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
+    const int k = m - j * a.g.sj;
+    const int q = i * (int)a.g.si + m;
     const long long step = *a.dstep;
-    long long q = (long long)ib * si + m;
-    const long long qp = ib >= 1 ? q - si : q;
-    float hy_p = Hy[qp], hz_p = Hz[qp];
-    for (int i = ib; i < ie; i++, q += si) {
-        const float hx = Hx[q], hy = Hy[q], hz = Hz[q];
-        const float hz_jm = Hz[q - djm], hx_jm = Hx[q - djm];
-        const float hy_km = Hy[q - dkm], hx_km = Hx[q - dkm];
-        const float ex = Ex[q], ey = Ey[q], ez = Ez[q];
-        const int m0 = M0[q], m1 = M1[q], m2 = M2[q];
-        const float ecx = a.ec[0][i];
-        int pei = -1;
-        float bi = 0, ci = 0;
-        if (a.has_pml) { pei = a.pml[0].plane_e[i]; bi = a.pml[0].bm1_e[i]; ci = a.pml[0].cid_e[i]; }
-        if (okx) {
-            const float d1 = hz - hz_jm, d2 = hy - hy_km;
-            float t1 = d1 * ecy, t2 = d2 * ecz;
-            if (pej >= 0) t1 += psi_step(a.psiE[0][0], pej * a.pml[1].per + (long long)i * (nz + 1) + k, bj, cj, d1);
-            if (pek >= 0) t2 += psi_step(a.psiE[0][1], ((long long)i * (ny + 1) + j) * a.pml[2].planes + pek, bk, ck, d2);
-            Ex[q] = e_finish<0>(a, m0, ex, t1 - t2, i, j, k, step);
+    if (comp == 0) e_one<0>(a, i, j, k, q, step);
+    else if (comp == 1) e_one<1>(a, i, j, k, q, step);
+    else e_one<2>(a, i, j, k, q, step);
+}
+
+// ------------------------------------------------------- fused H + E step
+
+// One time step in a single pass over the fields. A block owns a (j,k) tile
+// of kFK x kFJ points and marches over kFX node planes along x. E planes
+// (tile plus a one-point halo) and H_old planes (tile plus the low halo)
+// stream into shared memory with cp.async two planes ahead of the
+// arithmetic (a ring of three E and two H_old planes). At plane i the block
+// computes H_new(i) on the tile and, redundantly, on its low halo, then
+// E_new(i) on the tile from those values and H_new(i-1) kept in registers.
+// Fields and H auxiliaries are read from the old buffers and written to the
+// new ones, so the redundant halo work never sees a neighbour's updated
+// values. Per step the fields are read once and written once: 48 bytes per
+// cell instead of 72 for separate H and E passes.
+constexpr int kFK = 32, kFJ = 8, kFX = 16, kFT = kFK * kFJ;
+constexpr int kRK = kFK + 2, kRJ = kFJ + 2, kRN = kRJ * kRK;   // E region: tile + halo on both sides
+constexpr int kHK = kFK + 1, kHJ = kFJ + 1, kHN = kHJ * kHK;   // H region: tile + the low halo
+constexpr int kHalo = kHK + kFJ;                               // halo H points per plane
+
+struct FusedShared {
+    float E[3][3][kRJ][kRK];    // ring of three E_old planes
+    float Ho[2][3][kHJ][kHK];   // ring of two H_old planes
+    float H[3][kHJ][kHK];       // H_new of the current plane
+};
+
+__device__ __forceinline__ void cp_async4(float *dst, const float *src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+__global__ void __launch_bounds__(kFT, 3) k_step_fused(const StepArgs a, const FusedArgs f) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FusedShared &sm = *reinterpret_cast<FusedShared *>(smem_raw);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kFK + tx;
+    const int k0 = blockIdx.x * kFK, j0 = blockIdx.y * kFJ;
+    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
+    const int sj = a.g.sj;
+    const long long si = a.g.si;
+    const int ib = blockIdx.z * kFX, ie = min(ib + kFX, nx + 1);
+    const int j = j0 + ty, k = k0 + tx;
+    const bool inside = j <= ny && k <= nz;
+
+    // this thread's staging slots in the E and H regions (element t = tid and tid + kFT)
+    int eoff[2], ereg[2], hoff[2], hreg[2];
+    bool eok[2], hok[2];
+    for (int s2 = 0; s2 < 2; s2++) {
+        const int t = tid + s2 * kFT;
+        int rj = t / kRK, rk = t - rj * kRK;
+        int jj = j0 - 1 + rj, kk = k0 - 1 + rk;
+        ereg[s2] = t < kRN ? t : -1;
+        eok[s2] = t < kRN && jj >= 0 && jj <= ny && kk >= 0 && kk <= nz;
+        eoff[s2] = eok[s2] ? jj * sj + kk : 0;
+        rj = t / kHK; rk = t - rj * kHK;
+        jj = j0 - 1 + rj; kk = k0 - 1 + rk;
+        hreg[s2] = t < kHN ? t : -1;
+        hok[s2] = t < kHN && jj >= 0 && jj <= ny && kk >= 0 && kk <= nz;
+        hoff[s2] = hok[s2] ? jj * sj + kk : 0;
+    }
+    auto issue_e = [&](int p) {
+        if (p > nx) return;
+        const long long base = (long long)p * si;
+        float *dst = &sm.E[p % 3][0][0][0];
+        for (int s2 = 0; s2 < 2; s2++)
+            if (ereg[s2] >= 0)
+                for (int c = 0; c < 3; c++) cp_async4(dst + c * kRN + ereg[s2], f.Eo[c] + base + eoff[s2], eok[s2]);
+    };
+    auto issue_h = [&](int p) {
+        if (p > nx) return;
+        const long long base = (long long)p * si;
+        float *dst = &sm.Ho[p % 2][0][0][0];
+        for (int s2 = 0; s2 < 2; s2++)
+            if (hreg[s2] >= 0)
+                for (int c = 0; c < 3; c++) cp_async4(dst + c * kHN + hreg[s2], f.Ho[c] + base + hoff[s2], hok[s2]);
+    };
+    // H_new at (p, jj, kk) from the staged planes; rj, rk: E-region coordinates
+    auto h_at = [&](const Column &col, const Plane &pl, int p, int jj, int kk, int rj, int rk, bool own, float &hx,
+                    float &hy, float &hz) {
+        const float (*Ec)[kRJ][kRK] = sm.E[p % 3];
+        const float (*En)[kRJ][kRK] = sm.E[(p + 1) % 3];
+        const float (*Hb)[kHJ][kHK] = sm.Ho[p % 2];
+        hx = Hb[0][rj][rk]; hy = Hb[1][rj][rk]; hz = Hb[2][rj][rk];
+        if (own)
+            h_point<true>(a, col, pl, f.psiHo, f.psiHn, p, jj, kk, Ec[0][rj][rk], Ec[1][rj][rk], Ec[2][rj][rk],
+                          Ec[2][rj + 1][rk], Ec[0][rj + 1][rk], Ec[1][rj][rk + 1], Ec[0][rj][rk + 1], En[1][rj][rk],
+                          En[2][rj][rk], hx, hy, hz);
+        else
+            h_point<false>(a, col, pl, f.psiHo, f.psiHn, p, jj, kk, Ec[0][rj][rk], Ec[1][rj][rk], Ec[2][rj][rk],
+                           Ec[2][rj + 1][rk], Ec[0][rj + 1][rk], Ec[1][rj][rk + 1], Ec[0][rj][rk + 1], En[1][rj][rk],
+                           En[2][rj][rk], hx, hy, hz);
+    };
+    // the halo H point of this thread (threads 0 .. kHalo-1): row j0-1, then column k0-1
+    int hj = -1, hk = -1;
+    if (tid < kHK) { hj = j0 - 1; hk = k0 - 1 + tid; }
+    else if (tid < kHalo) { hj = j0 + (tid - kHK); hk = k0 - 1; }
+    const bool halo = tid < kHalo && hj >= 0 && hk >= 0 && hj <= ny && hk <= nz;
+    const Column col = column_at(a, min(j, ny), min(k, nz));
+    const Column hcol = column_at(a, halo ? hj : 0, halo ? hk : 0);
+
+    const long long step = *a.dstep;
+    float hy_prev = 0.f, hz_prev = 0.f;
+    if (ib >= 1) { issue_e(ib - 1); issue_h(ib - 1); }
+    issue_e(ib);
+    issue_h(ib);
+    issue_e(ib + 1);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+    if (ib >= 1) {
+        if (inside) {   // H_new(ib-1) at the own point, for the x-derivative of E at ib
+            float hx, hy, hz;
+            h_at(col, plane_at(a, ib - 1), ib - 1, j, k, ty + 1, tx + 1, false, hx, hy, hz);
+            hy_prev = hy;
+            hz_prev = hz;
         }
-        if (i >= 1) {
-            if (oky) {
-                const float d1 = hx - hx_km, d2 = hz - hz_p;
-                float t1 = d1 * ecz, t2 = d2 * ecx;
-                if (pek >= 0) t1 += psi_step(a.psiE[1][0], ((long long)i * (ny + 1) + j) * a.pml[2].planes + pek, bk, ck, d1);
-                if (pei >= 0) t2 += psi_step(a.psiE[1][1], pei * a.pml[0].per + (long long)j * (nz + 1) + k, bi, ci, d2);
-                Ey[q] = e_finish<1>(a, m1, ey, t1 - t2, i, j, k, step);
-            }
-            if (okz) {
-                const float d1 = hy - hy_p, d2 = hx - hx_jm;
-                float t1 = d1 * ecx, t2 = d2 * ecy;
-                if (pei >= 0) t1 += psi_step(a.psiE[2][0], pei * a.pml[0].per + (long long)j * (nz + 1) + k, bi, ci, d1);
-                if (pej >= 0) t2 += psi_step(a.psiE[2][1], pej * a.pml[1].per + (long long)i * (nz + 1) + k, bj, cj, d2);
-                Ez[q] = e_finish<2>(a, m2, ez, t1 - t2, i, j, k, step);
-            }
+        __syncthreads();   // the loop's first copies reuse the slots of plane ib-1
+    }
+    for (int i = ib; i < ie; i++) {
+        issue_e(i + 2);
+        issue_h(i + 1);
+        cp_async_commit();
+        const int q = i * (int)si + j * sj + k;
+        int m0 = 0, m1 = 0, m2 = 0;
+        if (inside && i < nx) { m0 = a.mat[0][q]; m1 = a.mat[1][q]; m2 = a.mat[2][q]; }
+        cp_async_wait<1>();
+        __syncthreads();
+        const Plane pl = plane_at(a, i);
+        float hx = 0.f, hy = 0.f, hz = 0.f;
+        if (inside) {
+            h_at(col, pl, i, j, k, ty + 1, tx + 1, true, hx, hy, hz);
+            sm.H[0][ty + 1][tx + 1] = hx; sm.H[1][ty + 1][tx + 1] = hy; sm.H[2][ty + 1][tx + 1] = hz;
+            f.Hn[0][q] = hx; f.Hn[1][q] = hy; f.Hn[2][q] = hz;
         }
-        hy_p = hy;
-        hz_p = hz;
+        if (halo) {
+            const int rj = hj - j0 + 1, rk = hk - k0 + 1;
+            float gx, gy, gz;
+            h_at(hcol, pl, i, hj, hk, rj, rk, false, gx, gy, gz);
+            sm.H[0][rj][rk] = gx; sm.H[1][rj][rk] = gy; sm.H[2][rj][rk] = gz;
+        }
+        __syncthreads();
+        if (inside) {
+            const float (*Ec)[kRJ][kRK] = sm.E[i % 3];
+            float ex = Ec[0][ty + 1][tx + 1], ey = Ec[1][ty + 1][tx + 1], ez = Ec[2][ty + 1][tx + 1];
+            e_point(a, col, pl, i, j, k, step, hx, hy, hz, sm.H[2][ty][tx + 1], sm.H[0][ty][tx + 1], sm.H[1][ty + 1][tx],
+                    sm.H[0][ty + 1][tx], hy_prev, hz_prev, m0, m1, m2, ex, ey, ez);
+            f.En[0][q] = ex; f.En[1][q] = ey; f.En[2][q] = ez;
+        }
+        hy_prev = hy;
+        hz_prev = hz;
+        __syncthreads();
     }
 }
 
@@ -515,15 +752,20 @@ struct Device {
     std::string error;
 
     Geom g{};
-    DevBuf<float> E[3], H[3];
+    // fields and H auxiliaries are double-buffered: the fused step reads
+    // buffer `cur` and writes buffer cur^1 (the other kernels work in place on cur)
+    DevBuf<float> E[2][3], H[2][3];
+    int cur = 0;
+    bool use_fused = false;  // CEM_B200_FUSED=1 selects the single-pass H+E kernel
     DevBuf<float> hc[3], ec[3];
     DevBuf<int> plane_h[3], plane_e[3];
     DevBuf<float> bm1_h[3], cid_h[3], bm1_e[3], cid_e[3];
-    DevBuf<float> psiH[3][2], psiE[3][2];
+    DevBuf<float> psiH[2][3][2], psiE[3][2];
     size_t psi_len_h[3][2] = {}, psi_len_e[3][2] = {};
     int zplanes = 0;   // planes of the z CPML slabs (same count for cells and nodes)
     DevBuf<unsigned short> mat[3];
     DevBuf<float> tab[3];
+    DevBuf<float4> tab4[3];
     DevBuf<unsigned char> tflag[3];
     DevBuf<double> cb64[3];
     int ntab[3] = {0, 0, 0};
@@ -548,10 +790,11 @@ struct Device {
     int ring_count = 0;
     bool vold_valid = false;
 
-    StepArgs sa{};
-    SibcArgs sb{};
-    PostArgs pa{};
-    EnergyArgs ea{};
+    StepArgs sa[2]{};
+    SibcArgs sb[2]{};
+    PostArgs pa[2]{};
+    EnergyArgs ea[2]{};
+    FusedArgs fa[2]{};
 
     ~Device() {
         if (stream) cudaStreamDestroy(stream);
@@ -619,6 +862,12 @@ bool d2h(cem_sim *s, void *dst, const void *src, size_t bytes) {
     if (!bytes) return true;
     CB2_CHECK(s, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->dev->stream));
     CB2_CHECK(s, cudaStreamSynchronize(s->dev->stream));
+    return true;
+}
+
+bool zero_dev(cem_sim *s, void *p, size_t bytes) {
+    if (!bytes || !p) return true;
+    CB2_CHECK(s, cudaMemsetAsync(p, 0, bytes, s->dev->stream));
     return true;
 }
 
@@ -729,6 +978,17 @@ bool build_tables(cem_sim *s, Device &D) {
         if (!dev_upload(s, D.mat[c], mat)) return false;
         if (!dev_upload(s, D.tab[c], tb.field_major())) return false;
         if (!dev_upload(s, D.tflag[c], tb.flags)) return false;
+        {
+            const size_t ne = tb.flags.size();
+            std::vector<float4> packed(ne);
+            for (size_t e = 0; e < ne; e++) {
+                unsigned fl = tb.flags[e];
+                float fbits;
+                std::memcpy(&fbits, &fl, 4);
+                packed[e] = make_float4(tb.rows[e * nfields], tb.rows[e * nfields + 1], tb.rows[e * nfields + 2], fbits);
+            }
+            if (!dev_upload(s, D.tab4[c], packed)) return false;
+        }
         if (!dev_upload(s, D.cb64[c], tb.cb64)) return false;
         if (box_hi[0] >= 0) {
             for (int a = 0; a < 3; a++) {
@@ -782,8 +1042,11 @@ bool build_pml(cem_sim *s, Device &D) {
         for (int w = 0; w < 2; w++) {
             D.psi_len_h[c][w] = psi_len(s, 0, c, w);
             D.psi_len_e[c][w] = psi_len(s, 1, c, w);
-            if (!dev_alloc(s, D.psiH[c][w], D.psi_len_h[c][w] + 1) || !dev_alloc(s, D.psiE[c][w], D.psi_len_e[c][w] + 1))
+            if (!dev_alloc(s, D.psiH[0][c][w], D.psi_len_h[c][w] + 1) ||
+                !dev_alloc(s, D.psiH[1][c][w], D.psi_len_h[c][w] + 1) || !dev_alloc(s, D.psiE[c][w], D.psi_len_e[c][w] + 1))
                 return false;
+            // unused slots of the compact layout are read by nobody but must stay finite
+            if (!zero_dev(s, D.psiH[1][c][w].p, D.psiH[1][c][w].n * 4)) return false;
         }
     return true;
 }
@@ -861,24 +1124,25 @@ bool build_sources(cem_sim *s, Device &D) {
     return true;
 }
 
-void fill_args(cem_sim *s, Device &D) {
-    StepArgs &a = D.sa;
+void fill_args_for(cem_sim *s, Device &D, int cur) {
+    StepArgs &a = D.sa[cur];
     a = StepArgs{};
     a.g = D.g;
     for (int c = 0; c < 3; c++) {
-        a.E[c] = D.E[c].p;
-        a.H[c] = D.H[c].p;
+        a.E[c] = D.E[cur][c].p;
+        a.H[c] = D.H[cur][c].p;
         a.hc[c] = D.hc[c].p;
         a.ec[c] = D.ec[c].p;
         a.pml[c] = PmlAxis{D.plane_h[c].p, D.plane_e[c].p, D.bm1_h[c].p, D.cid_h[c].p, D.bm1_e[c].p, D.cid_e[c].p,
-                           (long long)pml_per(s, c), D.zplanes};
+                           (int)pml_per(s, c), D.zplanes};
         for (int w = 0; w < 2; w++) {
-            a.psiH[c][w] = D.psiH[c][w].p;
+            a.psiH[c][w] = D.psiH[cur][c][w].p;
             a.psiE[c][w] = D.psiE[c][w].p;
         }
         a.mat[c] = D.mat[c].p;
         a.tab[c] = D.tab[c].p;
         a.tflag[c] = D.tflag[c].p;
+        a.tab4[c] = D.tab4[c].p;
         a.ntab[c] = D.ntab[c];
         a.J[c] = D.J[c].p;
         for (int q = 0; q < 6; q++) a.jbox[c][q] = D.jbox[c][q];
@@ -906,7 +1170,17 @@ void fill_args(cem_sim *s, Device &D) {
     }
     a.dstep = D.dstep.p;
 
-    SibcArgs &b = D.sb;
+    FusedArgs &f = D.fa[cur];
+    for (int c = 0; c < 3; c++) {
+        f.Eo[c] = D.E[cur][c].p; f.Ho[c] = D.H[cur][c].p;
+        f.En[c] = D.E[cur ^ 1][c].p; f.Hn[c] = D.H[cur ^ 1][c].p;
+        for (int w = 0; w < 2; w++) {
+            f.psiHo[c][w] = D.psiH[cur][c][w].p;
+            f.psiHn[c][w] = D.psiH[cur ^ 1][c][w].p;
+        }
+    }
+
+    SibcArgs &b = D.sb[cur];
     b = SibcArgs{};
     b.ns = s->nsb;
     b.K = s->sibc_npole;
@@ -916,9 +1190,9 @@ void fill_args(cem_sim *s, Device &D) {
         b.c[k] = (float)s->sibc_c[k];
         b.ome[k] = (float)(-std::expm1(-s->sibc_a[k] * s->dt));   // 1 - e_k without cancellation
     }
-    for (int c = 0; c < 3; c++) { b.E[c] = D.E[c].p; b.H[c] = D.H[c].p; }
+    for (int c = 0; c < 3; c++) { b.E[c] = D.E[cur][c].p; b.H[c] = D.H[cur][c].p; }
 
-    PostArgs &p = D.pa;
+    PostArgs &p = D.pa[cur];
     p = PostArgs{};
     p.nin = D.nin; p.nip = D.nip; p.nport = D.nport; p.nvp = D.nvp; p.nslot = D.nslot;
     p.off = D.off.p; p.ecomp = D.ecomp.p; p.eidx = D.eidx.p; p.ew = D.ew.p; p.R = D.R.p; p.vold = D.vold.p;
@@ -926,18 +1200,23 @@ void fill_args(cem_sim *s, Device &D) {
     p.src_amp = s->src_amp; p.src_t0 = s->src_t0; p.src_tau = s->src_tau; p.dt = s->dt;
     p.msrc_on = s->msrc >= 0; p.m_t0 = s->msrc_t0; p.m_tau = s->msrc_tau;
     p.ring = D.ring.p;
-    for (int c = 0; c < 3; c++) { p.F[c] = D.E[c].p; p.F[3 + c] = D.H[c].p; }
+    for (int c = 0; c < 3; c++) { p.F[c] = D.E[cur][c].p; p.F[3 + c] = D.H[cur][c].p; }
     p.dstep = D.dstep.p;
 
-    EnergyArgs &e = D.ea;
+    EnergyArgs &e = D.ea[cur];
     e.g = D.g;
     for (int c = 0; c < 3; c++) {
-        e.F[c] = D.E[c].p; e.F[3 + c] = D.H[c].p;
+        e.F[c] = D.E[cur][c].p; e.F[3 + c] = D.H[cur][c].p;
         e.mat[c] = D.mat[c].p; e.cb64[c] = D.cb64[c].p;
         e.d[c] = D.d64[c].p; e.dd[c] = D.dd64[c].p;
     }
     e.dt = s->dt;
     e.partial = D.partial.p;
+}
+
+void fill_args(cem_sim *s, Device &D) {
+    fill_args_for(s, D, 0);
+    fill_args_for(s, D, 1);
 }
 
 bool create_device_impl(cem_sim *s);
@@ -963,6 +1242,7 @@ bool create_device_impl(cem_sim *s) {
     Device &D = *s->dev;
     if (g_selected_device >= 0) CB2_CHECK(s, cudaSetDevice(g_selected_device));
     CB2_CHECK(s, cudaGetDevice(&D.device));
+    if (const char *e = std::getenv("CEM_B200_FUSED")) D.use_fused = e[0] == '1';
     CB2_CHECK(s, cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking));
     Geom &g = D.g;
     for (int a = 0; a < 3; a++) g.n[a] = s->n[a];
@@ -970,12 +1250,13 @@ bool create_device_impl(cem_sim *s) {
     g.sj = (int)s->sj;
     g.plane = (int)s->si;
     g.sj_magic = ((1ull << 40) + s->sj - 1) / s->sj;
-    if ((double)g.plane * (double)g.sj >= 1099511627776.0) {
-        set_error("grid plane too large");
+    if ((double)g.plane * (double)g.sj >= 1099511627776.0 || s->N >= (1ull << 31)) {
+        set_error("grid too large: more than 2^31 points");
         return false;
     }
     for (int c = 0; c < 3; c++) {
-        if (!dev_alloc(s, D.E[c], s->N) || !dev_alloc(s, D.H[c], s->N)) return false;
+        for (int b = 0; b < 2; b++)
+            if (!dev_alloc(s, D.E[b][c], s->N) || !dev_alloc(s, D.H[b][c], s->N)) return false;
         std::vector<double> hc(s->n[c]);
         for (int i = 0; i < s->n[c]; i++) hc[i] = s->dt / CEM_MU0 * s->idh[c][i];
         if (!dev_upload(s, D.hc[c], to_f32(hc)) || !dev_upload(s, D.ec[c], to_f32(s->ide[c]))) return false;
@@ -1007,11 +1288,6 @@ bool download_f32(cem_sim *s, std::vector<double> &dst, const float *src, size_t
     return true;
 }
 
-bool zero_dev(cem_sim *s, void *p, size_t bytes) {
-    if (!bytes || !p) return true;
-    CB2_CHECK(s, cudaMemsetAsync(p, 0, bytes, s->dev->stream));
-    return true;
-}
 
 // pack the host DFT accumulators in slot order: I probes, port V/I, source, V probes
 std::vector<double *> dft_slots(cem_sim *s) {
@@ -1063,13 +1339,13 @@ bool upload_group(cem_sim *s, unsigned g, bool from_host) {
     const size_t N = s->N;
     for (int c = 0; c < 3; c++) {
         if (g & (kGroupE0 << c)) {
-            if (from_host) { if (!upload_f32(s, D.E[c].p, s->E[c], N)) return false; }
-            else if (!zero_dev(s, D.E[c].p, N * sizeof(float))) return false;
+            if (from_host) { if (!upload_f32(s, D.E[D.cur][c].p, s->E[c], N)) return false; }
+            else if (!zero_dev(s, D.E[D.cur][c].p, N * sizeof(float))) return false;
             D.vold_valid = false;
         }
         if (g & (kGroupH0 << c)) {
-            if (from_host) { if (!upload_f32(s, D.H[c].p, s->H[c], N)) return false; }
-            else if (!zero_dev(s, D.H[c].p, N * sizeof(float))) return false;
+            if (from_host) { if (!upload_f32(s, D.H[D.cur][c].p, s->H[c], N)) return false; }
+            else if (!zero_dev(s, D.H[D.cur][c].p, N * sizeof(float))) return false;
         }
     }
     if (g & kGroupPsi)
@@ -1077,10 +1353,10 @@ bool upload_group(cem_sim *s, unsigned g, bool from_host) {
             for (int w = 0; w < 2; w++) {
                 if (from_host) {
                     if (!upload_f32(s, D.psiE[c][w].p, psi_to_device(s, D, c, w, s->psiE[c][w]), D.psi_len_e[c][w]) ||
-                        !upload_f32(s, D.psiH[c][w].p, psi_to_device(s, D, c, w, s->psiH[c][w]), D.psi_len_h[c][w]))
+                        !upload_f32(s, D.psiH[D.cur][c][w].p, psi_to_device(s, D, c, w, s->psiH[c][w]), D.psi_len_h[c][w]))
                         return false;
                 } else if (!zero_dev(s, D.psiE[c][w].p, D.psiE[c][w].n * 4) ||
-                           !zero_dev(s, D.psiH[c][w].p, D.psiH[c][w].n * 4)) {
+                           !zero_dev(s, D.psiH[D.cur][c][w].p, D.psiH[D.cur][c][w].n * 4)) {
                     return false;
                 }
             }
@@ -1131,14 +1407,14 @@ bool download_group(cem_sim *s, unsigned g) {
     if ((g & kGroupDft) && !flush_dft(s)) return false;
     CB2_CHECK(s, cudaStreamSynchronize(D.stream));
     for (int c = 0; c < 3; c++) {
-        if ((g & (kGroupE0 << c)) && !download_f32(s, s->E[c], D.E[c].p, N)) return false;
-        if ((g & (kGroupH0 << c)) && !download_f32(s, s->H[c], D.H[c].p, N)) return false;
+        if ((g & (kGroupE0 << c)) && !download_f32(s, s->E[c], D.E[D.cur][c].p, N)) return false;
+        if ((g & (kGroupH0 << c)) && !download_f32(s, s->H[c], D.H[D.cur][c].p, N)) return false;
     }
     if (g & kGroupPsi)
         for (int c = 0; c < 3; c++)
             for (int w = 0; w < 2; w++)
                 if (!download_f32(s, s->psiE[c][w], D.psiE[c][w].p, D.psi_len_e[c][w]) ||
-                    !download_f32(s, s->psiH[c][w], D.psiH[c][w].p, D.psi_len_h[c][w]))
+                    !download_f32(s, s->psiH[c][w], D.psiH[D.cur][c][w].p, D.psi_len_h[c][w]))
                     return false;
                 else {
                     psi_to_host(s, D, c, w, s->psiE[c][w]);
@@ -1198,8 +1474,9 @@ bool begin_device_op(cem_sim *s) {
     CB2_CHECK(s, cudaMemcpyAsync(D.dstep.p, &st, sizeof st, cudaMemcpyHostToDevice, D.stream));
     CB2_CHECK(s, cudaStreamSynchronize(D.stream));
     if (!D.vold_valid && D.nport) {
-        D.pa.advance = 0;
-        k_post<<<1, kBlock, 0, D.stream>>>(D.pa);
+        PostArgs pa = D.pa[D.cur];
+        pa.advance = 0;
+        k_post<<<1, kBlock, 0, D.stream>>>(pa);
         CB2_CHECK(s, cudaGetLastError());
         D.vold_valid = true;
     }
@@ -1216,8 +1493,30 @@ bool end_device_op(cem_sim *s) {
     return true;
 }
 
+// one whole step: the fused H+E pass, then SIBC, probes and the step count
+bool launch_fused_step(cem_sim *s) {
+    Device &D = *s->dev;
+    if (D.ring_count == kRing && !flush_dft(s)) return false;
+    const dim3 grid((s->n[2] + 1 + kFK - 1) / kFK, (s->n[1] + 1 + kFJ - 1) / kFJ, (s->n[0] + 1 + kFX - 1) / kFX);
+    t_begin(1);
+    k_step_fused<<<grid, dim3(kFK, kFJ), sizeof(FusedShared), D.stream>>>(D.sa[D.cur], D.fa[D.cur]);
+    t_end();
+    D.cur ^= 1;
+    if (s->nsb) { t_begin(2); k_sibc<<<(s->nsb + kBlock - 1) / kBlock, kBlock, 0, D.stream>>>(D.sb[D.cur]); t_end(); }
+    PostArgs pa = D.pa[D.cur];
+    pa.advance = 1;
+    t_begin(3);
+    k_post<<<1, kBlock, 0, D.stream>>>(pa);
+    t_end();
+    D.ring_count++;
+    s->step++;
+    CB2_CHECK(s, cudaGetLastError());
+    return true;
+}
+
 bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
     Device &D = *s->dev;
+    if (phase_mask == (1 | 4 | 8) && i0 <= 0 && i1 > s->n[0] && D.use_fused) return launch_fused_step(s);
     const int nx = s->n[0];
     const dim3 blk(kBlock);
     const int gx = (D.g.plane + kBlock - 1) / kBlock;
@@ -1225,28 +1524,30 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
         const int a = std::max(0, i0), b = std::min(nx + 1, i1);
         if (b > a) {
             t_begin(0);
-            k_update_h<<<dim3(gx, (b - a + kMarch - 1) / kMarch), blk, 0, D.stream>>>(D.sa, a, b);
+            k_update_h<<<dim3(3 * gx, b - a), blk, 0, D.stream>>>(D.sa[D.cur], a);
             t_end();
         }
     }
     if (phase_mask & 2) {   // port voltages before the E update
-        D.pa.advance = 0;
-        if (D.nport) k_post<<<1, kBlock, 0, D.stream>>>(D.pa);
+        PostArgs pa = D.pa[D.cur];
+        pa.advance = 0;
+        if (D.nport) k_post<<<1, kBlock, 0, D.stream>>>(pa);
     }
     if (phase_mask & 4) {   // E over node planes [i0, i1) within [0, nx)
         const int a = std::max(0, i0), b = std::min(nx, i1);
         if (b > a) {
             t_begin(1);
-            k_update_e<<<dim3(gx, (b - a + kMarch - 1) / kMarch), blk, 0, D.stream>>>(D.sa, a, b);
+            k_update_e<<<dim3(3 * gx, b - a), blk, 0, D.stream>>>(D.sa[D.cur], a);
             t_end();
         }
     }
     if (phase_mask & 8) {   // surface impedance, probes, step count
         if (D.ring_count == kRing && !flush_dft(s)) return false;
-        if (s->nsb) { t_begin(2); k_sibc<<<(s->nsb + kBlock - 1) / kBlock, blk, 0, D.stream>>>(D.sb); t_end(); }
-        D.pa.advance = 1;
+        if (s->nsb) { t_begin(2); k_sibc<<<(s->nsb + kBlock - 1) / kBlock, blk, 0, D.stream>>>(D.sb[D.cur]); t_end(); }
+        PostArgs pa = D.pa[D.cur];
+        pa.advance = 1;
         t_begin(3);
-        k_post<<<1, kBlock, 0, D.stream>>>(D.pa);
+        k_post<<<1, kBlock, 0, D.stream>>>(pa);
         t_end();
         D.ring_count++;
         s->step++;
@@ -1329,7 +1630,7 @@ bool energy_on_device(cem_sim *s, double *out) {
     if (!begin_device_op(s)) return false;
     Device &D = *s->dev;
     const int gx = (D.g.plane + kBlock - 1) / kBlock;
-    k_energy<<<dim3(gx, s->n[0] + 1), kBlock, 0, D.stream>>>(D.ea);
+    k_energy<<<dim3(gx, s->n[0] + 1), kBlock, 0, D.stream>>>(D.ea[D.cur]);
     k_sum<<<1, 1024, 0, D.stream>>>(D.partial.p, (long long)gx * (s->n[0] + 1), D.scalar.p);
     CB2_CHECK(s, cudaGetLastError());
     CB2_CHECK(s, cudaMemcpyAsync(out, D.scalar.p, sizeof(double), cudaMemcpyDeviceToHost, D.stream));
@@ -1423,9 +1724,9 @@ int cemx_sizes(const cem_sim *s, long long *out, int n) {
         long long bytes = 0;
         const Device &D = *s->dev;
         for (int c = 0; c < 3; c++) {
-            bytes += (long long)(D.E[c].n + D.H[c].n + D.hc[c].n + D.ec[c].n) * 4 + (long long)D.mat[c].n * 2 +
-                     (long long)D.tab[c].n * 4 + (long long)D.J[c].n * 4;
-            for (int w = 0; w < 2; w++) bytes += (long long)(D.psiE[c][w].n + D.psiH[c][w].n) * 4;
+            bytes += (long long)(2 * D.E[0][c].n + 2 * D.H[0][c].n + D.hc[c].n + D.ec[c].n) * 4 +
+                     (long long)D.mat[c].n * 2 + (long long)D.tab[c].n * 4 + (long long)D.J[c].n * 4;
+            for (int w = 0; w < 2; w++) bytes += (long long)(D.psiE[c][w].n + 2 * D.psiH[0][c][w].n) * 4;
         }
         bytes += (long long)(D.sb_y.n + D.sb_hw.n) * 4 + (long long)(D.sb_eidx.n + D.sb_hidx.n) * 8 +
                  (long long)(D.ring.n + D.acc.n) * 8;
