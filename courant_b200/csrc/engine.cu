@@ -46,6 +46,10 @@ constexpr unsigned kFlagDisp = 1, kFlagSrc = 2;
 
 // ---------------------------------------------------------------- arguments
 
+// Device index space: rows padded to 16 bytes, q = i*si + j*sj + k with
+// sj = round_up(nz+1, 4) and si = (ny+1)*sj; padding elements (k > nz) stay
+// zero and belong to no field component. Host copies use the reference index
+// space (sj = nz+1) and are converted row by row at transfer.
 struct Geom {
     int n[3];
     long long si;
@@ -361,7 +365,7 @@ template <int C>
 __device__ __forceinline__ void h_one(const StepArgs &a, int i, int j, int k, int q) {
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
     const int idx[3] = {i, j, k};
-    if (idx[A1] >= a.g.n[A1] || idx[A2] >= a.g.n[A2]) return;
+    if (idx[A1] >= a.g.n[A1] || idx[A2] >= a.g.n[A2] || k > a.g.n[2]) return;
     const float *__restrict__ E2 = a.E[A2];
     const float *__restrict__ E1 = a.E[A1];
     float *__restrict__ H = a.H[C];
@@ -687,9 +691,9 @@ __global__ void __launch_bounds__(kBlock) k_energy(const EnergyArgs a) {
     const int i = blockIdx.y;
     const int m = blockIdx.x * kBlock + threadIdx.x;
     double acc = 0;
-    if (m < a.g.plane) {
-        const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
-        const int k = m - j * a.g.sj;
+    const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
+    const int k = m - j * a.g.sj;
+    if (m < a.g.plane && k <= a.g.n[2]) {
         const long long q = (long long)i * a.g.si + m;
         const int idx[3] = {i, j, k};
         for (int c = 0; c < 3; c++) {
@@ -752,6 +756,7 @@ struct Device {
     std::string error;
 
     Geom g{};
+    size_t Np = 0;   // points in the padded device index space
     // fields and H auxiliaries are double-buffered: the fused step reads
     // buffer `cur` and writes buffer cur^1 (the other kernels work in place on cur)
     DevBuf<float> E[2][3], H[2][3];
@@ -885,6 +890,12 @@ bool dev_upload(cem_sim *s, DevBuf<T> &b, const std::vector<T> &v) {
     return h2d(s, b.p, v.data(), v.size() * sizeof(T));
 }
 
+// reference index q -> padded device index
+long long dev_index(const cem_sim *s, const Device &D, size_t q) {
+    const size_t i = q / s->si, r = q % s->si, j = r / s->sj, k = r % s->sj;
+    return (long long)(i * D.g.si + j * D.g.sj + k);
+}
+
 std::vector<float> to_f32(const std::vector<double> &v) {
     std::vector<float> o(v.size());
     for (size_t i = 0; i < v.size(); i++) o[i] = (float)v[i];
@@ -939,7 +950,7 @@ bool build_tables(cem_sim *s, Device &D) {
     const int *n = s->n;
     for (int c = 0; c < 3; c++) {
         TableBuilder tb(nfields);
-        std::vector<unsigned short> mat(s->N, 0);
+        std::vector<unsigned short> mat(D.Np, 0);
         std::vector<float> row(nfields);
         int box_lo[3] = {n[0], n[1], n[2]}, box_hi[3] = {-1, -1, -1};
         std::string last_key;
@@ -972,7 +983,7 @@ bool build_tables(cem_sim *s, Device &D) {
                         set_error("more than 65535 distinct update coefficients on one component");
                         return false;
                     }
-                    mat[q] = (unsigned short)id;
+                    mat[(size_t)i * D.g.si + (size_t)j * D.g.sj + k] = (unsigned short)id;
                 }
         D.ntab[c] = (int)tb.flags.size();
         if (!dev_upload(s, D.mat[c], mat)) return false;
@@ -1063,19 +1074,19 @@ bool build_probes(cem_sim *s, Device &D) {
     std::vector<double> w;
     for (const CurrentProbe &p : s->ip) {
         for (size_t e = 0; e < p.idx.size(); e++) {
-            comp.push_back((unsigned char)p.comp[e]); idx.push_back((long long)p.idx[e]); w.push_back(p.w[e]);
+            comp.push_back((unsigned char)p.comp[e]); idx.push_back(dev_index(s, D, p.idx[e])); w.push_back(p.w[e]);
         }
         off.push_back((int)idx.size());
     }
     for (const LumpedPort &p : s->port) {
         for (size_t e = 0; e < p.edge.size(); e++) {
-            comp.push_back((unsigned char)p.axis); idx.push_back((long long)p.edge[e]); w.push_back(p.dl[e] * p.dir);
+            comp.push_back((unsigned char)p.axis); idx.push_back(dev_index(s, D, p.edge[e])); w.push_back(p.dl[e] * p.dir);
         }
         off.push_back((int)idx.size());
     }
     for (const VoltageProbe &p : s->vp) {
         for (size_t e = 0; e < p.edge.size(); e++) {
-            comp.push_back((unsigned char)p.axis); idx.push_back((long long)p.edge[e]); w.push_back(p.dl[e]);
+            comp.push_back((unsigned char)p.axis); idx.push_back(dev_index(s, D, p.edge[e])); w.push_back(p.dl[e]);
         }
         off.push_back((int)idx.size());
     }
@@ -1098,9 +1109,9 @@ bool build_sibc(cem_sim *s, Device &D) {
     std::vector<long long> eidx(s->nsb), hidx(4 * (size_t)s->nsb);
     std::vector<float> hw(4 * (size_t)s->nsb);
     for (int e = 0; e < s->nsb; e++) {
-        eidx[e] = (long long)s->sb_idx[e];
+        eidx[e] = dev_index(s, D, s->sb_idx[e]);
         for (int f = 0; f < 4; f++) {
-            hidx[4 * e + f] = (long long)s->sb_hi[4 * e + f];
+            hidx[4 * e + f] = f < s->sb_nf[e] ? dev_index(s, D, s->sb_hi[4 * e + f]) : 0;
             hw[4 * e + f] = f < s->sb_nf[e] ? (float)s->sb_sg[4 * e + f] : 0.f;
         }
     }
@@ -1246,17 +1257,20 @@ bool create_device_impl(cem_sim *s) {
     CB2_CHECK(s, cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking));
     Geom &g = D.g;
     for (int a = 0; a < 3; a++) g.n[a] = s->n[a];
-    g.si = (long long)s->si;
-    g.sj = (int)s->sj;
-    g.plane = (int)s->si;
-    g.sj_magic = ((1ull << 40) + s->sj - 1) / s->sj;
-    if ((double)g.plane * (double)g.sj >= 1099511627776.0 || s->N >= (1ull << 31)) {
+    g.sj = (s->n[2] + 1 + 3) / 4 * 4;
+    g.si = (long long)(s->n[1] + 1) * g.sj;
+    g.plane = (int)g.si;
+    g.sj_magic = ((1ull << 40) + g.sj - 1) / g.sj;
+    D.Np = (size_t)g.si * (s->n[0] + 1);
+    if ((double)g.plane * (double)g.sj >= 1099511627776.0 || D.Np >= (1ull << 31)) {
         set_error("grid too large: more than 2^31 points");
         return false;
     }
     for (int c = 0; c < 3; c++) {
         for (int b = 0; b < 2; b++)
-            if (!dev_alloc(s, D.E[b][c], s->N) || !dev_alloc(s, D.H[b][c], s->N)) return false;
+            if (!dev_alloc(s, D.E[b][c], D.Np) || !dev_alloc(s, D.H[b][c], D.Np) ||
+                !zero_dev(s, D.E[b][c].p, D.Np * 4) || !zero_dev(s, D.H[b][c].p, D.Np * 4))
+                return false;
         std::vector<double> hc(s->n[c]);
         for (int i = 0; i < s->n[c]; i++) hc[i] = s->dt / CEM_MU0 * s->idh[c][i];
         if (!dev_upload(s, D.hc[c], to_f32(hc)) || !dev_upload(s, D.ec[c], to_f32(s->ide[c]))) return false;
@@ -1271,6 +1285,35 @@ bool create_device_impl(cem_sim *s) {
 }
 
 // ----------------------------------------------------- host <-> device moves
+
+// a field in the reference layout -> the padded device layout, and back
+bool upload_field(cem_sim *s, float *dst, const std::vector<double> &src) {
+    const Device &D = *s->dev;
+    std::vector<float> tmp(D.Np, 0.f);
+    const int nx = s->n[0], ny = s->n[1], nz = s->n[2];
+    for (int i = 0; i <= nx; i++)
+        for (int j = 0; j <= ny; j++) {
+            const double *r = &src[(size_t)i * s->si + (size_t)j * s->sj];
+            float *o = &tmp[(size_t)i * D.g.si + (size_t)j * D.g.sj];
+            for (int k = 0; k <= nz; k++) o[k] = (float)r[k];
+        }
+    return h2d(s, dst, tmp.data(), tmp.size() * 4);
+}
+
+bool download_field(cem_sim *s, std::vector<double> &dst, const float *src) {
+    const Device &D = *s->dev;
+    std::vector<float> tmp(D.Np);
+    if (!d2h(s, tmp.data(), src, tmp.size() * 4)) return false;
+    dst.resize(s->N);
+    const int nx = s->n[0], ny = s->n[1], nz = s->n[2];
+    for (int i = 0; i <= nx; i++)
+        for (int j = 0; j <= ny; j++) {
+            const float *r = &tmp[(size_t)i * D.g.si + (size_t)j * D.g.sj];
+            double *o = &dst[(size_t)i * s->si + (size_t)j * s->sj];
+            for (int k = 0; k <= nz; k++) o[k] = r[k];
+        }
+    return true;
+}
 
 bool upload_f32(cem_sim *s, float *dst, const std::vector<double> &src, size_t n) {
     if (!n) return true;
@@ -1336,16 +1379,15 @@ void psi_to_host(const cem_sim *s, const Device &D, int c, int w, std::vector<do
 
 bool upload_group(cem_sim *s, unsigned g, bool from_host) {
     Device &D = *s->dev;
-    const size_t N = s->N;
     for (int c = 0; c < 3; c++) {
         if (g & (kGroupE0 << c)) {
-            if (from_host) { if (!upload_f32(s, D.E[D.cur][c].p, s->E[c], N)) return false; }
-            else if (!zero_dev(s, D.E[D.cur][c].p, N * sizeof(float))) return false;
+            if (from_host) { if (!upload_field(s, D.E[D.cur][c].p, s->E[c])) return false; }
+            else if (!zero_dev(s, D.E[D.cur][c].p, D.Np * sizeof(float))) return false;
             D.vold_valid = false;
         }
         if (g & (kGroupH0 << c)) {
-            if (from_host) { if (!upload_f32(s, D.H[D.cur][c].p, s->H[c], N)) return false; }
-            else if (!zero_dev(s, D.H[D.cur][c].p, N * sizeof(float))) return false;
+            if (from_host) { if (!upload_field(s, D.H[D.cur][c].p, s->H[c])) return false; }
+            else if (!zero_dev(s, D.H[D.cur][c].p, D.Np * sizeof(float))) return false;
         }
     }
     if (g & kGroupPsi)
@@ -1403,12 +1445,11 @@ bool upload_group(cem_sim *s, unsigned g, bool from_host) {
 
 bool download_group(cem_sim *s, unsigned g) {
     Device &D = *s->dev;
-    const size_t N = s->N;
     if ((g & kGroupDft) && !flush_dft(s)) return false;
     CB2_CHECK(s, cudaStreamSynchronize(D.stream));
     for (int c = 0; c < 3; c++) {
-        if ((g & (kGroupE0 << c)) && !download_f32(s, s->E[c], D.E[D.cur][c].p, N)) return false;
-        if ((g & (kGroupH0 << c)) && !download_f32(s, s->H[c], D.H[D.cur][c].p, N)) return false;
+        if ((g & (kGroupE0 << c)) && !download_field(s, s->E[c], D.E[D.cur][c].p)) return false;
+        if ((g & (kGroupH0 << c)) && !download_field(s, s->H[c], D.H[D.cur][c].p)) return false;
     }
     if (g & kGroupPsi)
         for (int c = 0; c < 3; c++)
@@ -1719,8 +1760,6 @@ int cemx_sizes(const cem_sim *s, long long *out, int n) {
     v[7] = s->sibc_npole;
     if (s->dev) {
         for (int c = 0; c < 3; c++) v[8 + c] = s->dev->ntab[c];
-        size_t free_b = 0, total_b = 0;
-        (void)free_b; (void)total_b;
         long long bytes = 0;
         const Device &D = *s->dev;
         for (int c = 0; c < 3; c++) {
