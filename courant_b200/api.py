@@ -142,6 +142,7 @@ _EXT_PROTOS = [
     ("cemx_synchronize", _i, [_p]),
     ("cemx_select_device", _i, [_i]),
     ("cemx_release_device", _i, [_p]),
+    ("cemx_use_fused", _i, [_p, _i]),
 ]
 
 
@@ -471,6 +472,10 @@ class Sim:
         keys = ["cells", "points", "psiE", "psiH", "ndisp", "npole", "nsibc", "sibc_terms", "tab_x", "tab_y", "tab_z",
                 "device_bytes", "launches_per_step"]
         return dict(zip(keys, [int(v) for v in out]))
+
+    def useFused(self, on: bool = True) -> bool:
+        """Select the single-pass fused H+E kernel (True) or the separate kernels."""
+        return bool(self.c.ex.cemx_use_fused(self.h, int(on)))
 
     def releaseDevice(self):
         self._check(self.c.ex.cemx_release_device(self.h), "release_device")

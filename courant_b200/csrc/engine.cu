@@ -22,6 +22,8 @@
 #include "sim.hpp"
 #include "../../include/courant_b200.h"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -115,6 +117,12 @@ struct FusedArgs {
     float *En[3], *Hn[3];
     float *psiHo[3][2];   // read only
     float *psiHn[3][2];
+    int *error;           // set when a bounded wait gives up
+};
+
+// TMA descriptors of the old E and H buffers of one parity (3D tiled: k, j, i)
+struct TmaMaps {
+    CUtensorMap e[3], h[3];
 };
 
 struct PostArgs {
@@ -259,24 +267,28 @@ __device__ __forceinline__ void h_point(const StepArgs &a, const Column &col, co
 // Per-edge epilogue: material table, Debye correction and update, sources.
 //   E = E + (ca-1) E + cb [curl - sum_p hk_p J_p] + cs Vs(t) + w Vm(t)
 //   J_p += -(1-k_p) J_p + beta_p/dt (E_new - E_old)
+// P (the number of Debye poles) is a template parameter so the pole loops
+// unroll and the currents stay in registers.
 // (reference sim.c:608-637, :894-910; dispersive.c:93-112; modeport.c:130-135)
-template <int C>
+template <int C, int P>
 __device__ __forceinline__ float e_finish(const StepArgs &a, int mi, float e_old, float curl, int i, int j, int k,
                                           long long step) {
     const float4 t = __ldg(a.tab4[C] + mi);   // ca-1, cb, cs, flags
     const unsigned flag = __float_as_uint(t.w);
     const float base = __fmaf_rn(t.x, e_old, e_old);
     if (!flag) return __fmaf_rn(t.y, curl, base);
-    const int nt = a.ntab[C];
-    const float *__restrict__ tab = a.tab[C];
     int jo = 0, jvol = 0;
-    float *__restrict__ J = a.J[C];
-    if (flag & kFlagDisp) {
+    float jv[P > 0 ? P : 1];
+    if (P > 0 && (flag & kFlagDisp)) {
         const int *bx = a.jbox[C];
         jvol = bx[3] * bx[4] * bx[5];
         jo = ((i - bx[0]) * bx[4] + (j - bx[1])) * bx[5] + (k - bx[2]);
         float acc = 0.f;
-        for (int p = 0; p < a.npole; p++) acc = __fmaf_rn(a.hk[p], J[p * jvol + jo], acc);
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            jv[p] = a.J[C][p * jvol + jo];
+            acc = __fmaf_rn(a.hk[p], jv[p], acc);
+        }
         curl = __fsub_rn(curl, acc);
     }
     float e = __fmaf_rn(t.y, curl, base);
@@ -291,12 +303,13 @@ __device__ __forceinline__ float e_finish(const StepArgs &a, int mi, float e_old
             e = __fmaf_rn(w, (float)dgauss(tH, a.m_t0, a.m_tau), e);
         }
     }
-    if (flag & kFlagDisp) {
+    if (P > 0 && (flag & kFlagDisp)) {
         const float de = __fsub_rn(e, e_old);
-        for (int p = 0; p < a.npole; p++) {
-            const float bidt = __ldg(tab + (3 + p) * nt + mi);
-            const float jp = J[p * jvol + jo];
-            J[p * jvol + jo] = __fmaf_rn(bidt, de, __fmaf_rn(-a.omk[p], jp, jp));
+        const int nt = a.ntab[C];
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            const float bidt = __ldg(a.tab[C] + (3 + p) * nt + mi);
+            a.J[C][p * jvol + jo] = __fmaf_rn(bidt, de, __fmaf_rn(-a.omk[p], jv[p], jv[p]));
         }
     }
     return e;
@@ -305,7 +318,7 @@ __device__ __forceinline__ float e_finish(const StepArgs &a, int mi, float e_old
 // E component C at (i, j, k) (reference sim.c:608-637, CPML :756-832):
 //   E_C = ca E + cb [ (d1 c1 + psi_{C,0}) - (d2 c2 + psi_{C,1}) ] + epilogue
 // with d1 = dH_{C+2} along axis C+1, d2 = dH_{C+1} along axis C+2.
-template <int C>
+template <int C, int P>
 __device__ __forceinline__ float e_comp(const StepArgs &a, int i, int j, int k, long long step, float e, float d1,
                                         float d2, float c1, float c2, int p1, int p2, int mi) {
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
@@ -325,11 +338,12 @@ __device__ __forceinline__ float e_comp(const StepArgs &a, int i, int j, int k, 
         arr[x] = psi;
         t2 = __fadd_rn(t2, psi);
     }
-    return e_finish<C>(a, mi, e, __fsub_rn(t1, t2), i, j, k, step);
+    return e_finish<C, P>(a, mi, e, __fsub_rn(t1, t2), i, j, k, step);
 }
 
 // All three E components at (i, j, k) for the fused step. h*: H at the point;
 // *_jm, *_km: at j-1, k-1; hy_p, hz_p: at i-1. e* in: old, out: new.
+template <int P>
 __device__ __forceinline__ void e_point(const StepArgs &a, const Column &col, const Plane &pl, int i, int j, int k,
                                         long long step, float hx, float hy, float hz, float hz_jm, float hx_jm,
                                         float hy_km, float hx_km, float hy_p, float hz_p, int m0, int m1, int m2,
@@ -338,23 +352,25 @@ __device__ __forceinline__ void e_point(const StepArgs &a, const Column &col, co
     if (i >= nx) return;
     const bool jin = j >= 1 && j < ny, kin = k >= 1 && k < nz;
     if (jin && kin)
-        ex = e_comp<0>(a, i, j, k, step, ex, __fsub_rn(hz, hz_jm), __fsub_rn(hy, hy_km), col.ecy, col.ecz, col.pej,
+        ex = e_comp<0, P>(a, i, j, k, step, ex, __fsub_rn(hz, hz_jm), __fsub_rn(hy, hy_km), col.ecy, col.ecz, col.pej,
                        col.pek, m0);
     if (i < 1) return;
     if (j < ny && kin)
-        ey = e_comp<1>(a, i, j, k, step, ey, __fsub_rn(hx, hx_km), __fsub_rn(hz, hz_p), col.ecz, pl.ecx, col.pek,
+        ey = e_comp<1, P>(a, i, j, k, step, ey, __fsub_rn(hx, hx_km), __fsub_rn(hz, hz_p), col.ecz, pl.ecx, col.pek,
                        pl.pei, m1);
     if (jin && k < nz)
-        ez = e_comp<2>(a, i, j, k, step, ez, __fsub_rn(hy, hy_p), __fsub_rn(hx, hx_jm), pl.ecx, col.ecy, pl.pei,
+        ez = e_comp<2, P>(a, i, j, k, step, ez, __fsub_rn(hy, hy_p), __fsub_rn(hx, hx_jm), pl.ecx, col.ecy, pl.pei,
                        col.pej, m2);
 }
 
 // ------------------------------------------------ separate phase kernels
 //
-// One thread per component of one point; the three components of a chunk of
-// a (j,k) plane sit in adjacent blocks, so the neighbour values they share
-// come from L2. Each thread issues its handful of loads before any
-// arithmetic; few registers leave room for many warps per SM.
+// One thread per field component of a (j,k) column, marching over kU node
+// planes along x with the loads of all kU planes issued before any
+// arithmetic. The three components of a chunk of the plane sit in adjacent
+// blocks, so the neighbour values they share come from L2.
+
+constexpr int kU = 4;
 
 template <int A>
 __device__ __forceinline__ int stride_of(const StepArgs &a) {
@@ -362,159 +378,238 @@ __device__ __forceinline__ int stride_of(const StepArgs &a) {
 }
 
 template <int C>
-__device__ __forceinline__ void h_one(const StepArgs &a, int i, int j, int k, int q) {
+__device__ __forceinline__ void h_march(const StepArgs &a, int ib, int ie, int j, int k, int m) {
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
-    const int idx[3] = {i, j, k};
-    if (idx[A1] >= a.g.n[A1] || idx[A2] >= a.g.n[A2] || k > a.g.n[2]) return;
+    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
+    const int jk[3] = {0, j, k};
+    if ((A1 != 0 && jk[A1] >= a.g.n[A1]) || (A2 != 0 && jk[A2] >= a.g.n[A2]) || k > nz) return;
+    const int last = (A1 == 0 || A2 == 0) ? min(ie, nx) : ie;   // an x-derivative needs plane i+1
+    const int si = (int)a.g.si, s1 = stride_of<A1>(a), s2 = stride_of<A2>(a);
     const float *__restrict__ E2 = a.E[A2];
     const float *__restrict__ E1 = a.E[A1];
     float *__restrict__ H = a.H[C];
-    const float e2 = E2[q], e2n = E2[q + stride_of<A1>(a)], e1 = E1[q], e1n = E1[q + stride_of<A2>(a)];
-    const float h = H[q];
-    const float c1 = a.hc[A1][idx[A1]], c2 = a.hc[A2][idx[A2]];
-    const int p1 = a.has_pml ? a.pml[A1].plane_h[idx[A1]] : -1, p2 = a.has_pml ? a.pml[A2].plane_h[idx[A2]] : -1;
-    H[q] = h_comp<C, true>(a, a.psiH, a.psiH, i, j, k, h, __fsub_rn(e2n, e2), __fsub_rn(e1n, e1), c1, c2, p1, p2);
+    float e2[kU], e2n[kU], e1[kU], e1n[kU], h[kU];
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+        const int q = (ib + u) * si + m;
+        if (ib + u < last) {
+            e2[u] = E2[q]; e2n[u] = E2[q + s1]; e1[u] = E1[q]; e1n[u] = E1[q + s2]; h[u] = H[q];
+        }
+    }
+    const float cj = a.hc[1][min(j, ny - 1)], ck = a.hc[2][min(k, nz - 1)];
+    const int pj = a.has_pml && j < ny ? a.pml[1].plane_h[j] : -1, pk = a.has_pml && k < nz ? a.pml[2].plane_h[k] : -1;
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+        const int i = ib + u;
+        if (i >= last) break;
+        const float ci = a.hc[0][min(i, nx - 1)];
+        const int pi = a.has_pml && i < nx ? a.pml[0].plane_h[i] : -1;
+        const float c[3] = {ci, cj, ck};
+        const int pp[3] = {pi, pj, pk};
+        H[i * si + m] = h_comp<C, true>(a, a.psiH, a.psiH, i, j, k, h[u], __fsub_rn(e2n[u], e2[u]),
+                                        __fsub_rn(e1n[u], e1[u]), c[A1], c[A2], pp[A1], pp[A2]);
+    }
 }
 
-template <int C>
-__device__ __forceinline__ void e_one(const StepArgs &a, int i, int j, int k, int q, long long step) {
+template <int C, int P>
+__device__ __forceinline__ void e_march(const StepArgs &a, int ib, int ie, int j, int k, int m, long long step) {
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
-    const int idx[3] = {i, j, k};
-    if (idx[C] >= a.g.n[C]) return;
-    if (idx[A1] < 1 || idx[A1] >= a.g.n[A1] || idx[A2] < 1 || idx[A2] >= a.g.n[A2]) return;
+    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
+    const int jk[3] = {0, j, k};
+    // own axis: index < n; transverse axes: 1 <= index < n
+    if (C != 0 && jk[C] >= a.g.n[C]) return;
+    if (A1 != 0 && (jk[A1] < 1 || jk[A1] >= a.g.n[A1])) return;
+    if (A2 != 0 && (jk[A2] < 1 || jk[A2] >= a.g.n[A2])) return;
+    const int first = C == 0 ? ib : max(ib, 1), last = min(ie, nx);
+    const int si = (int)a.g.si, s1 = stride_of<A1>(a), s2 = stride_of<A2>(a);
     const float *__restrict__ H2 = a.H[A2];
     const float *__restrict__ H1 = a.H[A1];
     float *__restrict__ E = a.E[C];
-    const float h2 = H2[q], h2m = H2[q - stride_of<A1>(a)], h1 = H1[q], h1m = H1[q - stride_of<A2>(a)];
-    const float e = E[q];
-    const int mi = a.mat[C][q];
-    const float c1 = a.ec[A1][idx[A1]], c2 = a.ec[A2][idx[A2]];
-    const int p1 = a.has_pml ? a.pml[A1].plane_e[idx[A1]] : -1, p2 = a.has_pml ? a.pml[A2].plane_e[idx[A2]] : -1;
-    E[q] = e_comp<C>(a, i, j, k, step, e, __fsub_rn(h2, h2m), __fsub_rn(h1, h1m), c1, c2, p1, p2, mi);
+    const unsigned short *__restrict__ M = a.mat[C];
+    float h2[kU], h2m[kU], h1[kU], h1m[kU], e[kU];
+    int mi[kU];
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+        const int i = ib + u, q = i * si + m;
+        if (i >= first && i < last) {
+            h2[u] = H2[q]; h2m[u] = H2[q - s1]; h1[u] = H1[q]; h1m[u] = H1[q - s2]; e[u] = E[q]; mi[u] = M[q];
+        }
+    }
+    const float cj = a.ec[1][j], ck = a.ec[2][k];
+    const int pj = a.has_pml ? a.pml[1].plane_e[j] : -1, pk = a.has_pml ? a.pml[2].plane_e[k] : -1;
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+        const int i = ib + u;
+        if (i < first || i >= last) continue;
+        const float c[3] = {a.ec[0][i], cj, ck};
+        const int pp[3] = {a.has_pml ? a.pml[0].plane_e[i] : -1, pj, pk};
+        E[i * si + m] = e_comp<C, P>(a, i, j, k, step, e[u], __fsub_rn(h2[u], h2m[u]), __fsub_rn(h1[u], h1m[u]),
+                                     c[A1], c[A2], pp[A1], pp[A2], mi[u]);
+    }
 }
 
-// H over node planes [i0, i0 + gridDim.y) (cem_mt_H and the unfused step)
-__global__ void __launch_bounds__(kBlock, 8) k_update_h(const StepArgs a, int i0) {
+// H over node planes [i0, i1) (cem_mt_H and the unfused step)
+__global__ void __launch_bounds__(kBlock, 6) k_update_h(const StepArgs a, int i0, int i1) {
     const int comp = blockIdx.x % 3;
     const int m = (blockIdx.x / 3) * kBlock + threadIdx.x;
     if (m >= a.g.plane) return;
-    const int i = i0 + blockIdx.y;
+    const int ib = i0 + blockIdx.y * kU, ie = min(ib + kU, i1);
     const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
     const int k = m - j * a.g.sj;
-    const int q = i * (int)a.g.si + m;
-    if (comp == 0) h_one<0>(a, i, j, k, q);
-    else if (comp == 1) h_one<1>(a, i, j, k, q);
-    else h_one<2>(a, i, j, k, q);
+    if (comp == 0) h_march<0>(a, ib, ie, j, k, m);
+    else if (comp == 1) h_march<1>(a, ib, ie, j, k, m);
+    else h_march<2>(a, ib, ie, j, k, m);
 }
 
-// E over node planes [i0, i0 + gridDim.y) (cem_mt_E and the unfused step)
-__global__ void __launch_bounds__(kBlock, 6) k_update_e(const StepArgs a, int i0) {
+// E over node planes [i0, i1) (cem_mt_E and the unfused step)
+template <int P>
+__global__ void __launch_bounds__(kBlock, 3) k_update_e(const StepArgs a, int i0, int i1) {
     const int comp = blockIdx.x % 3;
     const int m = (blockIdx.x / 3) * kBlock + threadIdx.x;
     if (m >= a.g.plane) return;
-    const int i = i0 + blockIdx.y;
+    const int ib = i0 + blockIdx.y * kU, ie = min(ib + kU, i1);
     const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
     const int k = m - j * a.g.sj;
-    const int q = i * (int)a.g.si + m;
     const long long step = *a.dstep;
-    if (comp == 0) e_one<0>(a, i, j, k, q, step);
-    else if (comp == 1) e_one<1>(a, i, j, k, q, step);
-    else e_one<2>(a, i, j, k, q, step);
+    if (comp == 0) e_march<0, P>(a, ib, ie, j, k, m, step);
+    else if (comp == 1) e_march<1, P>(a, ib, ie, j, k, m, step);
+    else e_march<2, P>(a, ib, ie, j, k, m, step);
 }
 
 // ------------------------------------------------------- fused H + E step
 
 // One time step in a single pass over the fields. A block owns a (j,k) tile
-// of kFK x kFJ points and marches over kFX node planes along x. E planes
-// (tile plus a one-point halo) and H_old planes (tile plus the low halo)
-// stream into shared memory with cp.async two planes ahead of the
-// arithmetic (a ring of three E and two H_old planes). At plane i the block
-// computes H_new(i) on the tile and, redundantly, on its low halo, then
-// E_new(i) on the tile from those values and H_new(i-1) kept in registers.
-// Fields and H auxiliaries are read from the old buffers and written to the
-// new ones, so the redundant halo work never sees a neighbour's updated
-// values. Per step the fields are read once and written once: 48 bytes per
-// cell instead of 72 for separate H and E passes.
+// of kFK x kFJ points and marches over kFX node planes along x. Per plane,
+// one thread arms an mbarrier and issues TMA bulk tensor copies of E_old (the
+// tile plus a one-point halo: box 40 x 10) and H_old (the tile plus the low
+// halo: box 40 x 9) into shared-memory rings of three and two planes, two
+// planes ahead of the arithmetic. At plane i the block computes H_new(i) on
+// the tile and, redundantly, on its low halo, then E_new(i) on the tile from
+// those values and H_new(i-1) kept in registers. Fields and H auxiliaries
+// are read from the old buffers and written to the new ones, so the
+// redundant halo work never sees a neighbour's updated values. Per step the
+// fields are read once and written once: 48 bytes per cell instead of 72 for
+// separate H and E passes. The x coordinate of every box starts 4 elements
+// before the tile (16-byte aligned); out-of-grid elements read as zero.
 constexpr int kFK = 32, kFJ = 8, kFX = 16, kFT = kFK * kFJ;
-constexpr int kRK = kFK + 2, kRJ = kFJ + 2, kRN = kRJ * kRK;   // E region: tile + halo on both sides
-constexpr int kHK = kFK + 1, kHJ = kFJ + 1, kHN = kHJ * kHK;   // H region: tile + the low halo
+constexpr int kBX = kFK + 8;                                   // box width: k0-4 .. k0+35
+constexpr int kRJ = kFJ + 2, kHJ = kFJ + 1;                    // E rows j0-1..j0+8, H rows j0-1..j0+7
+constexpr int kHK = kFK + 1;                                   // H region width: k0-1 .. k0+31
 constexpr int kHalo = kHK + kFJ;                               // halo H points per plane
+constexpr int kEBox = kRJ * kBX * 4, kHBox = kHJ * kBX * 4;    // bytes per component box
+constexpr int kEStride = (kEBox + 127) / 128 * 128, kHStride = (kHBox + 127) / 128 * 128;
+constexpr int kOffE = 0;                                       // 3 slots x 3 components
+constexpr int kOffH = kOffE + 9 * kEStride;                    // 2 slots x 3 components
+constexpr int kOffHn = kOffH + 6 * kHStride;                   // H_new of the current plane [3][kHJ][kHK]
+constexpr int kOffBar = (kOffHn + 3 * kHJ * kHK * 4 + 15) / 16 * 16;
+constexpr int kFusedSmem = kOffBar + 5 * 8;
+constexpr unsigned kWaitLimit = 1u << 24;
 
-struct FusedShared {
-    float E[3][3][kRJ][kRK];    // ring of three E_old planes
-    float Ho[2][3][kHJ][kHK];   // ring of two H_old planes
-    float H[3][kHJ][kHK];       // H_new of the current plane
-};
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ void cp_async4(float *dst, const float *src, bool valid) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+__device__ __forceinline__ void mbar_init(unsigned long long *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void mbar_expect(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// bounded wait; on timeout the error flag is set and the copies in flight
+// get a second bounded wait, so the block never leaves with TMA writes pending
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int *err) {
+    for (unsigned it = 0; it < kWaitLimit; it++)
+        if (mbar_try(bar, parity)) return true;
+    atomicExch(err, 1);
+    for (unsigned it = 0; it < kWaitLimit; it++)
+        if (mbar_try(bar, parity)) break;
+    return false;
+}
+__device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, int x, int y, int z, unsigned long long *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+            "r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
 
-__global__ void __launch_bounds__(kFT, 3) k_step_fused(const StepArgs a, const FusedArgs f) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    FusedShared &sm = *reinterpret_cast<FusedShared *>(smem_raw);
+template <int P>
+__global__ void __launch_bounds__(kFT, 3) k_step_fused(const StepArgs a, const FusedArgs f,
+                                                       const __grid_constant__ TmaMaps maps) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned long long *bar = reinterpret_cast<unsigned long long *>(smem + kOffBar);   // E slots 0-2, H slots 3-4
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kFK + tx;
     const int k0 = blockIdx.x * kFK, j0 = blockIdx.y * kFJ;
     const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
-    const int sj = a.g.sj;
-    const long long si = a.g.si;
+    const int sj = a.g.sj, si = (int)a.g.si;
     const int ib = blockIdx.z * kFX, ie = min(ib + kFX, nx + 1);
     const int j = j0 + ty, k = k0 + tx;
     const bool inside = j <= ny && k <= nz;
 
-    // this thread's staging slots in the E and H regions (element t = tid and tid + kFT)
-    int eoff[2], ereg[2], hoff[2], hreg[2];
-    bool eok[2], hok[2];
-    for (int s2 = 0; s2 < 2; s2++) {
-        const int t = tid + s2 * kFT;
-        int rj = t / kRK, rk = t - rj * kRK;
-        int jj = j0 - 1 + rj, kk = k0 - 1 + rk;
-        ereg[s2] = t < kRN ? t : -1;
-        eok[s2] = t < kRN && jj >= 0 && jj <= ny && kk >= 0 && kk <= nz;
-        eoff[s2] = eok[s2] ? jj * sj + kk : 0;
-        rj = t / kHK; rk = t - rj * kHK;
-        jj = j0 - 1 + rj; kk = k0 - 1 + rk;
-        hreg[s2] = t < kHN ? t : -1;
-        hok[s2] = t < kHN && jj >= 0 && jj <= ny && kk >= 0 && kk <= nz;
-        hoff[s2] = hok[s2] ? jj * sj + kk : 0;
-    }
+    auto Eb = [&](int slot, int c) { return reinterpret_cast<float *>(smem + kOffE + (slot * 3 + c) * kEStride); };
+    auto Hb = [&](int slot, int c) { return reinterpret_cast<float *>(smem + kOffH + (slot * 3 + c) * kHStride); };
+    float *Hn = reinterpret_cast<float *>(smem + kOffHn);   // [3][kHJ][kHK]
+    // Every copy issued is waited for: E planes up to e_last (E(ie) feeds H(ie-1)),
+    // H planes up to ie-1. Every thread tracks the same pending and parity bits;
+    // thread 0 alone issues.
+    const int e_last = min(ie, nx), h_last = ie - 1;
+    unsigned eph = 0, hph = 0, epend = 0, hpend = 0;   // per slot: phase parity, copy in flight
+    bool ok = true;
     auto issue_e = [&](int p) {
-        if (p > nx) return;
-        const long long base = (long long)p * si;
-        float *dst = &sm.E[p % 3][0][0][0];
-        for (int s2 = 0; s2 < 2; s2++)
-            if (ereg[s2] >= 0)
-                for (int c = 0; c < 3; c++) cp_async4(dst + c * kRN + ereg[s2], f.Eo[c] + base + eoff[s2], eok[s2]);
+        if (p > e_last) return;
+        const int sl = p % 3;
+        epend |= 1u << sl;
+        if (tid != 0) return;
+        unsigned long long *b = bar + sl;
+        mbar_expect(b, 3 * kEBox);
+        for (int c = 0; c < 3; c++) tma_load(Eb(sl, c), &maps.e[c], k0 - 4, j0 - 1, p, b);
     };
     auto issue_h = [&](int p) {
-        if (p > nx) return;
-        const long long base = (long long)p * si;
-        float *dst = &sm.Ho[p % 2][0][0][0];
-        for (int s2 = 0; s2 < 2; s2++)
-            if (hreg[s2] >= 0)
-                for (int c = 0; c < 3; c++) cp_async4(dst + c * kHN + hreg[s2], f.Ho[c] + base + hoff[s2], hok[s2]);
+        if (p > h_last) return;
+        const int sl = p % 2;
+        hpend |= 1u << sl;
+        if (tid != 0) return;
+        unsigned long long *b = bar + 3 + sl;
+        mbar_expect(b, 3 * kHBox);
+        for (int c = 0; c < 3; c++) tma_load(Hb(sl, c), &maps.h[c], k0 - 4, j0 - 1, p, b);
     };
-    // H_new at (p, jj, kk) from the staged planes; rj, rk: E-region coordinates
-    auto h_at = [&](const Column &col, const Plane &pl, int p, int jj, int kk, int rj, int rk, bool own, float &hx,
-                    float &hy, float &hz) {
-        const float (*Ec)[kRJ][kRK] = sm.E[p % 3];
-        const float (*En)[kRJ][kRK] = sm.E[(p + 1) % 3];
-        const float (*Hb)[kHJ][kHK] = sm.Ho[p % 2];
-        hx = Hb[0][rj][rk]; hy = Hb[1][rj][rk]; hz = Hb[2][rj][rk];
+    auto wait_e = [&](int p) {
+        const int sl = p % 3;
+        ok &= mbar_wait(bar + sl, (eph >> sl) & 1u, f.error);
+        eph ^= 1u << sl;
+        epend &= ~(1u << sl);
+    };
+    auto wait_h = [&](int p) {
+        const int sl = p % 2;
+        ok &= mbar_wait(bar + 3 + sl, (hph >> sl) & 1u, f.error);
+        hph ^= 1u << sl;
+        hpend &= ~(1u << sl);
+    };
+    // after a timed-out wait: give every copy still in flight a bounded wait, then leave
+    auto drain = [&]() {
+        for (int sl = 0; sl < 3; sl++)
+            if (epend & (1u << sl)) mbar_wait(bar + sl, (eph >> sl) & 1u, f.error);
+        for (int sl = 0; sl < 2; sl++)
+            if (hpend & (1u << sl)) mbar_wait(bar + 3 + sl, (hph >> sl) & 1u, f.error);
+    };
+    // H_new at (p, jj, kk); the E region column of kk is x = kk - k0 + 4, its row rj = jj - j0 + 1
+    auto h_at = [&](const Column &col, const Plane &pl, int p, int jj, int kk, bool own, float &hx, float &hy,
+                    float &hz) {
+        const int rj = jj - j0 + 1, x = kk - k0 + 4;
+        const float *e0 = Eb(p % 3, 0), *e1 = Eb(p % 3, 1), *e2 = Eb(p % 3, 2);
+        const float *n1 = Eb((p + 1) % 3, 1), *n2 = Eb((p + 1) % 3, 2);
+        const int o = rj * kBX + x;
+        hx = Hb(p % 2, 0)[o]; hy = Hb(p % 2, 1)[o]; hz = Hb(p % 2, 2)[o];
         if (own)
-            h_point<true>(a, col, pl, f.psiHo, f.psiHn, p, jj, kk, Ec[0][rj][rk], Ec[1][rj][rk], Ec[2][rj][rk],
-                          Ec[2][rj + 1][rk], Ec[0][rj + 1][rk], Ec[1][rj][rk + 1], Ec[0][rj][rk + 1], En[1][rj][rk],
-                          En[2][rj][rk], hx, hy, hz);
+            h_point<true>(a, col, pl, f.psiHo, f.psiHn, p, jj, kk, e0[o], e1[o], e2[o], e2[o + kBX], e0[o + kBX],
+                          e1[o + 1], e0[o + 1], n1[o], n2[o], hx, hy, hz);
         else
-            h_point<false>(a, col, pl, f.psiHo, f.psiHn, p, jj, kk, Ec[0][rj][rk], Ec[1][rj][rk], Ec[2][rj][rk],
-                           Ec[2][rj + 1][rk], Ec[0][rj + 1][rk], Ec[1][rj][rk + 1], Ec[0][rj][rk + 1], En[1][rj][rk],
-                           En[2][rj][rk], hx, hy, hz);
+            h_point<false>(a, col, pl, f.psiHo, f.psiHn, p, jj, kk, e0[o], e1[o], e2[o], e2[o + kBX], e0[o + kBX],
+                           e1[o + 1], e0[o + 1], n1[o], n2[o], hx, hy, hz);
     };
-    // the halo H point of this thread (threads 0 .. kHalo-1): row j0-1, then column k0-1
     int hj = -1, hk = -1;
     if (tid < kHK) { hj = j0 - 1; hk = k0 - 1 + tid; }
     else if (tid < kHalo) { hj = j0 + (tid - kHK); hk = k0 - 1; }
@@ -522,52 +617,60 @@ __global__ void __launch_bounds__(kFT, 3) k_step_fused(const StepArgs a, const F
     const Column col = column_at(a, min(j, ny), min(k, nz));
     const Column hcol = column_at(a, halo ? hj : 0, halo ? hk : 0);
 
-    const long long step = *a.dstep;
-    float hy_prev = 0.f, hz_prev = 0.f;
+    if (tid == 0) {
+        for (int q = 0; q < 5; q++) mbar_init(bar + q);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
     if (ib >= 1) { issue_e(ib - 1); issue_h(ib - 1); }
     issue_e(ib);
     issue_h(ib);
     issue_e(ib + 1);
-    cp_async_commit();
-    cp_async_wait<0>();
-    __syncthreads();
+    const long long step = *a.dstep;
+    float hy_prev = 0.f, hz_prev = 0.f;
+    if (ib >= 1) { wait_e(ib - 1); wait_h(ib - 1); }
+    wait_e(ib);
+    if (__syncthreads_or(!ok)) { drain(); return; }
     if (ib >= 1) {
-        if (inside) {   // H_new(ib-1) at the own point, for the x-derivative of E at ib
+        if (inside) {   // H_new(ib-1) at the own point, for the x-derivatives of E at ib
             float hx, hy, hz;
-            h_at(col, plane_at(a, ib - 1), ib - 1, j, k, ty + 1, tx + 1, false, hx, hy, hz);
+            h_at(col, plane_at(a, ib - 1), ib - 1, j, k, false, hx, hy, hz);
             hy_prev = hy;
             hz_prev = hz;
         }
-        __syncthreads();   // the loop's first copies reuse the slots of plane ib-1
+        __syncthreads();   // the first copies of the loop reuse the slots of plane ib-1
     }
     for (int i = ib; i < ie; i++) {
+        if (tid == 0) asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");   // generic reads before async writes
         issue_e(i + 2);
         issue_h(i + 1);
-        cp_async_commit();
-        const int q = i * (int)si + j * sj + k;
+        const int q = i * si + j * sj + k;
         int m0 = 0, m1 = 0, m2 = 0;
         if (inside && i < nx) { m0 = a.mat[0][q]; m1 = a.mat[1][q]; m2 = a.mat[2][q]; }
-        cp_async_wait<1>();
-        __syncthreads();
+        if (i < nx) wait_e(i + 1);
+        wait_h(i);
+        if (__syncthreads_or(!ok)) { drain(); return; }
         const Plane pl = plane_at(a, i);
         float hx = 0.f, hy = 0.f, hz = 0.f;
         if (inside) {
-            h_at(col, pl, i, j, k, ty + 1, tx + 1, true, hx, hy, hz);
-            sm.H[0][ty + 1][tx + 1] = hx; sm.H[1][ty + 1][tx + 1] = hy; sm.H[2][ty + 1][tx + 1] = hz;
+            h_at(col, pl, i, j, k, true, hx, hy, hz);
+            const int o = (ty + 1) * kHK + tx + 1;
+            Hn[o] = hx; Hn[kHJ * kHK + o] = hy; Hn[2 * kHJ * kHK + o] = hz;
             f.Hn[0][q] = hx; f.Hn[1][q] = hy; f.Hn[2][q] = hz;
         }
         if (halo) {
-            const int rj = hj - j0 + 1, rk = hk - k0 + 1;
             float gx, gy, gz;
-            h_at(hcol, pl, i, hj, hk, rj, rk, false, gx, gy, gz);
-            sm.H[0][rj][rk] = gx; sm.H[1][rj][rk] = gy; sm.H[2][rj][rk] = gz;
+            h_at(hcol, pl, i, hj, hk, false, gx, gy, gz);
+            const int o = (hj - j0 + 1) * kHK + (hk - k0 + 1);
+            Hn[o] = gx; Hn[kHJ * kHK + o] = gy; Hn[2 * kHJ * kHK + o] = gz;
         }
         __syncthreads();
         if (inside) {
-            const float (*Ec)[kRJ][kRK] = sm.E[i % 3];
-            float ex = Ec[0][ty + 1][tx + 1], ey = Ec[1][ty + 1][tx + 1], ez = Ec[2][ty + 1][tx + 1];
-            e_point(a, col, pl, i, j, k, step, hx, hy, hz, sm.H[2][ty][tx + 1], sm.H[0][ty][tx + 1], sm.H[1][ty + 1][tx],
-                    sm.H[0][ty + 1][tx], hy_prev, hz_prev, m0, m1, m2, ex, ey, ez);
+            const int x = tx + 4, o = (ty + 1) * kBX + x;
+            float ex = Eb(i % 3, 0)[o], ey = Eb(i % 3, 1)[o], ez = Eb(i % 3, 2)[o];
+            const int h = (ty + 1) * kHK + tx + 1;
+            e_point<P>(a, col, pl, i, j, k, step, hx, hy, hz, Hn[2 * kHJ * kHK + h - kHK], Hn[h - kHK],
+                    Hn[kHJ * kHK + h - 1], Hn[h - 1], hy_prev, hz_prev, m0, m1, m2, ex, ey, ez);
             f.En[0][q] = ex; f.En[1][q] = ey; f.En[2][q] = ez;
         }
         hy_prev = hy;
@@ -575,6 +678,18 @@ __global__ void __launch_bounds__(kFT, 3) k_step_fused(const StepArgs a, const F
         __syncthreads();
     }
 }
+
+// launchers of the pole-count instantiations
+using EKernel = void (*)(StepArgs, int, int);
+using FKernel = void (*)(StepArgs, FusedArgs, TmaMaps);
+#define CB2_POLES(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
+#define CB2_EK(p) k_update_e<p>,
+#define CB2_FK(p) k_step_fused<p>,
+const EKernel kEKernels[] = {CB2_POLES(CB2_EK)};
+const FKernel kFKernels[] = {CB2_POLES(CB2_FK)};
+#undef CB2_EK
+#undef CB2_FK
+#undef CB2_POLES
 
 // ------------------------------------------------------------------- SIBC
 
@@ -753,7 +868,7 @@ struct Device {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool failed = false;
-    std::string error;
+    std::string error_msg;
 
     Geom g{};
     size_t Np = 0;   // points in the padded device index space
@@ -795,6 +910,8 @@ struct Device {
     int ring_count = 0;
     bool vold_valid = false;
 
+    TmaMaps maps[2]{};
+    DevBuf<int> error;
     StepArgs sa[2]{};
     SibcArgs sb[2]{};
     PostArgs pa[2]{};
@@ -843,7 +960,7 @@ bool fail(cem_sim *s, const char *what, cudaError_t e) {
     std::fprintf(stderr, "courant-b200: %s\n", msg);
     if (s->dev) {
         s->dev->failed = true;
-        s->dev->error = msg;
+        s->dev->error_msg = msg;
     }
     return false;
 }
@@ -1182,6 +1299,7 @@ void fill_args_for(cem_sim *s, Device &D, int cur) {
     a.dstep = D.dstep.p;
 
     FusedArgs &f = D.fa[cur];
+    f.error = D.error.p;
     for (int c = 0; c < 3; c++) {
         f.Eo[c] = D.E[cur][c].p; f.Ho[c] = D.H[cur][c].p;
         f.En[c] = D.E[cur ^ 1][c].p; f.Hn[c] = D.H[cur ^ 1][c].p;
@@ -1240,6 +1358,34 @@ bool create_device(cem_sim *s) {
     return false;
 }
 
+// 3D tiled TMA descriptor of one field buffer (padded layout), box kBX x rows x 1
+bool make_tmap(cem_sim *s, CUtensorMap *map, const float *base, unsigned rows) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void *fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            set_error("cuTensorMapEncodeTiled unavailable");
+            return false;
+        }
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const Device &D = *s->dev;
+    const cuuint64_t dims[3] = {(cuuint64_t)s->n[2] + 1, (cuuint64_t)s->n[1] + 1, (cuuint64_t)s->n[0] + 1};
+    const cuuint64_t strides[2] = {(cuuint64_t)D.g.sj * 4, (cuuint64_t)D.g.si * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)kBX, rows, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed");
+        return false;
+    }
+    return true;
+}
+
 bool create_device_impl(cem_sim *s) {
     if (!s->finalized) { set_error("not finalized"); return false; }
     int ndev = 0;
@@ -1254,6 +1400,7 @@ bool create_device_impl(cem_sim *s) {
     if (g_selected_device >= 0) CB2_CHECK(s, cudaSetDevice(g_selected_device));
     CB2_CHECK(s, cudaGetDevice(&D.device));
     if (const char *e = std::getenv("CEM_B200_FUSED")) D.use_fused = e[0] == '1';
+    if (s->kernel_choice >= 0) D.use_fused = s->kernel_choice == 1;
     CB2_CHECK(s, cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking));
     Geom &g = D.g;
     for (int a = 0; a < 3; a++) g.n[a] = s->n[a];
@@ -1278,6 +1425,12 @@ bool create_device_impl(cem_sim *s) {
     }
     if (!build_pml(s, D) || !build_tables(s, D) || !build_probes(s, D) || !build_sibc(s, D) || !build_sources(s, D))
         return false;
+    for (int b = 0; b < 2; b++)
+        for (int c = 0; c < 3; c++)
+            if (!make_tmap(s, &D.maps[b].e[c], D.E[b][c].p, kRJ) || !make_tmap(s, &D.maps[b].h[c], D.H[b][c].p, kHJ))
+                return false;
+    if (!dev_alloc(s, D.error, 1) || !zero_dev(s, D.error.p, 4)) return false;
+    CB2_CHECK(s, cudaFuncSetAttribute(kFKernels[s->npole], cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem));
     const long long nblk = (long long)((g.plane + kBlock - 1) / kBlock) * (s->n[0] + 1);
     if (!dev_alloc(s, D.partial, (size_t)nblk) || !dev_alloc(s, D.scalar, 1)) return false;
     fill_args(s, D);
@@ -1501,7 +1654,7 @@ bool download_group(cem_sim *s, unsigned g) {
 bool begin_device_op(cem_sim *s) {
     if (!create_device(s)) return false;
     Device &D = *s->dev;
-    if (D.failed) { set_error(D.error.c_str()); return false; }
+    if (D.failed) { set_error(D.error_msg.c_str()); return false; }
     CB2_CHECK(s, cudaSetDevice(D.device));
     CB2_CHECK(s, cudaStreamSynchronize(D.stream));
     const unsigned need = (~s->dev_valid | s->exposed) & kGroupAll;
@@ -1527,6 +1680,18 @@ bool begin_device_op(cem_sim *s) {
 
 // After a device operation: refresh what callers hold pointers to.
 bool end_device_op(cem_sim *s) {
+    Device &D = *s->dev;
+    if (D.use_fused) {
+        int err = 0;
+        if (!d2h(s, &err, D.error.p, sizeof err)) return false;
+        if (err) {
+            D.failed = true;
+            D.error_msg = "device: a TMA wait in the fused step timed out";
+            set_error(D.error_msg.c_str());
+            std::fprintf(stderr, "courant-b200: %s\n", D.error_msg.c_str());
+            return false;
+        }
+    }
     if (s->exposed) {
         if (!download_group(s, s->exposed)) return false;
         s->host_valid |= s->exposed;
@@ -1540,7 +1705,7 @@ bool launch_fused_step(cem_sim *s) {
     if (D.ring_count == kRing && !flush_dft(s)) return false;
     const dim3 grid((s->n[2] + 1 + kFK - 1) / kFK, (s->n[1] + 1 + kFJ - 1) / kFJ, (s->n[0] + 1 + kFX - 1) / kFX);
     t_begin(1);
-    k_step_fused<<<grid, dim3(kFK, kFJ), sizeof(FusedShared), D.stream>>>(D.sa[D.cur], D.fa[D.cur]);
+    kFKernels[s->npole]<<<grid, dim3(kFK, kFJ), kFusedSmem, D.stream>>>(D.sa[D.cur], D.fa[D.cur], D.maps[D.cur]);
     t_end();
     D.cur ^= 1;
     if (s->nsb) { t_begin(2); k_sibc<<<(s->nsb + kBlock - 1) / kBlock, kBlock, 0, D.stream>>>(D.sb[D.cur]); t_end(); }
@@ -1565,7 +1730,7 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
         const int a = std::max(0, i0), b = std::min(nx + 1, i1);
         if (b > a) {
             t_begin(0);
-            k_update_h<<<dim3(3 * gx, b - a), blk, 0, D.stream>>>(D.sa[D.cur], a);
+            k_update_h<<<dim3(3 * gx, (b - a + kU - 1) / kU), blk, 0, D.stream>>>(D.sa[D.cur], a, b);
             t_end();
         }
     }
@@ -1578,7 +1743,7 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
         const int a = std::max(0, i0), b = std::min(nx, i1);
         if (b > a) {
             t_begin(1);
-            k_update_e<<<dim3(3 * gx, b - a), blk, 0, D.stream>>>(D.sa[D.cur], a);
+            kEKernels[s->npole]<<<dim3(3 * gx, (b - a + kU - 1) / kU), blk, 0, D.stream>>>(D.sa[D.cur], a, b);
             t_end();
         }
     }
@@ -1792,6 +1957,13 @@ int cemx_release_device(cem_sim *s) {
     s->dev.reset();
     s->dev_valid = 0;
     return 0;
+}
+
+int cemx_use_fused(cem_sim *s, int on) {
+    const int prev = s->dev ? (s->dev->use_fused ? 1 : 0) : (s->kernel_choice >= 0 ? s->kernel_choice : 0);
+    s->kernel_choice = on ? 1 : 0;
+    if (s->dev) s->dev->use_fused = on != 0;
+    return prev;
 }
 
 int cemx_synchronize(cem_sim *s) {

@@ -142,6 +142,7 @@ struct cem_sim {
     // pointer into the host copy and may read or write it between calls.
     // With neither bit set the state is all zeros (freshly finalized).
     unsigned host_valid = 0, dev_valid = 0, exposed = 0;
+    int kernel_choice = -1;   // -1: environment default, 0: separate H/E kernels, 1: fused
 
     std::unique_ptr<cb2::Device, void (*)(cb2::Device *)> dev{nullptr, cb2::device_release};
 };

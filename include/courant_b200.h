@@ -43,6 +43,12 @@ CEM_API int cemx_select_device(int device);
  * or -1. */
 CEM_API int cemx_release_device(cem_sim *s);
 
+/* Time-step kernel of s: 1 = the single-pass fused H+E kernel (TMA-staged),
+ * 0 = separate H and E kernels (the ones the cem_mt_* phases use). Both give
+ * bit-identical fields. The default is 0, or CEM_B200_FUSED=1 from the
+ * environment. Returns the previous setting, or -1. */
+CEM_API int cemx_use_fused(cem_sim *s, int on);
+
 /* Wait for all device work of s. Returns 0 or -1. */
 CEM_API int cemx_synchronize(cem_sim *s);
 

@@ -52,8 +52,9 @@ def spectrum_errors(gpu, orc, meta):
     return {k: float(np.max(np.abs(sg[k] - so[k])) / max(np.max(np.abs(so[k])), 1e-300)) for k in sg}
 
 
+@pytest.mark.parametrize("fused", [False, True], ids=["separate", "fused"])
 @pytest.mark.parametrize("fn", [scenes.parity_scene, scenes.lossy_scene], ids=["parity", "lossy"])
-def test_scene_against_oracle(lib, oracle_lib, fn):
+def test_scene_against_oracle(lib, oracle_lib, fn, fused):
     """At step 600 (fields near their peak, the step of the reference's own
     GPU-vs-CPU check) every component is within relative L2 1e-5 of the f64
     oracle, and max|diff|/max|field| per E/H family as the reference measures
@@ -61,6 +62,7 @@ def test_scene_against_oracle(lib, oracle_lib, fn):
     of their peak, errors are measured against each component's peak norm
     over the run; spectra and energy against their own magnitude."""
     s, meta = fn(lib)
+    s.useFused(fused)
     n = meta["steps"]
     o = oracle_lib.OracleSim.from_sim(s, meta["freqs"], n)
     peak = np.zeros(6)
@@ -101,10 +103,13 @@ def test_parity_scene_against_reference_printout(lib):
         assert np.max(np.abs(a - r)) / np.max(np.abs(r)) < SPEC_TOL, name
 
 
-def test_checkpoint_resume_bit_exact(lib):
+@pytest.mark.parametrize("fused", [False, True], ids=["separate", "fused"])
+def test_checkpoint_resume_bit_exact(lib, fused):
     A, _ = scenes.lossy_scene(lib)
     B, _ = scenes.lossy_scene(lib)
     C, meta = scenes.lossy_scene(lib)
+    for x in (A, B, C):
+        x.useFused(fused)
     A.step(900)
     B.step(400)
     buf = B.checkpoint()
@@ -134,9 +139,12 @@ def test_checkpoint_from_reference_resumes(lib, ref_lib):
         assert np.max(np.abs(G.portV(p) - R.portV(p))) / np.max(np.abs(R.portV(p))) < SPEC_TOL
 
 
-def test_phased_stepping_matches_cem_step(lib):
+@pytest.mark.parametrize("fused", [False, True], ids=["separate", "fused"])
+def test_phased_stepping_matches_cem_step(lib, fused):
+    """The cem_mt_* phases (separate kernels, any slab split) give the same bits as cem_step."""
     A, _ = scenes.parity_scene(lib)
     B, _ = scenes.parity_scene(lib)
+    A.useFused(fused)
     A.step(50)
     nx = B.nx
     for _ in range(50):
@@ -179,10 +187,12 @@ def test_run_stops_on_energy_decay(lib, oracle_lib):
     assert abs(s.energy() - o.energy()) / o.energy() < 1e-4
 
 
-def test_gcpw_lumped_sparams(lib, oracle_lib):
+@pytest.mark.parametrize("fused", [False, True], ids=["separate", "fused"])
+def test_gcpw_lumped_sparams(lib, oracle_lib, fused):
     """S11/S21 of a short lumped-port GCPW within 1e-3 dB / 0.01 degree of the f64 oracle."""
     kw = dict(length=3e-3, hmin=50e-6, hmax=200e-6, dx=100e-6, yair=0.6e-3, zair=0.8e-3, npml=6, df=1e9, steps=3000)
     s, meta = scenes.gcpw_line(lib, **kw)
+    s.useFused(fused)
     n = meta["steps"]
     o = oracle_lib.OracleSim.from_sim(s, meta["freqs"], n)
     s.step(n)
