@@ -143,6 +143,7 @@ _EXT_PROTOS = [
     ("cemx_select_device", _i, [_i]),
     ("cemx_release_device", _i, [_p]),
     ("cemx_use_fused", _i, [_p, _i]),
+    ("cemx_energy_noalloc", _i, [_p, _dp]),
 ]
 
 
@@ -482,6 +483,12 @@ class Sim:
 
     def synchronize(self):
         self._check(self.c.ex.cemx_synchronize(self.h), "synchronize")
+
+    def energyNoAlloc(self) -> float:
+        """cem_energy without device allocation (static scratch; see courant_b200.h)."""
+        w = C.c_double()
+        self._check(self.c.ex.cemx_energy_noalloc(self.h, C.byref(w)), "energy_noalloc")
+        return w.value
 
     def destroy(self):
         if getattr(self, "h", None):

@@ -31,6 +31,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -1849,6 +1850,76 @@ int engine_energy(const cem_sim *cs, double *out) {
     return energy_on_device(const_cast<cem_sim *>(cs), out) ? 0 : -1;
 }
 
+// ------------------------------------------- energy without device allocation
+//
+// cemx_energy_noalloc runs k_energy and k_sum exactly as energy_on_device
+// does, but its block partials and its result live in this file-scope array
+// instead of the simulation's own buffers. Every slot is written before it is
+// read, so nothing has to start at zero. One array per device and process:
+// calls for different simulations on one device must not overlap in time.
+constexpr long long kNoAllocPartials = 65536;   // 512 KiB of block partials
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocPartials + 1];   // + the result
+
+constexpr int kMaxScratchDevices = 64;
+std::mutex g_scratch_mu;
+double *g_scratch_addr[kMaxScratchDevices] = {};
+
+// Address of g_noalloc_scratch on `device`, which must be current. Looked up
+// once per device; later calls only read the cached pointer.
+double *noalloc_scratch(int device) {
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (device < 0 || device >= kMaxScratchDevices) {
+        set_error("cemx_energy_noalloc: device ordinal beyond the 64 this library tracks");
+        return nullptr;
+    }
+    if (!g_scratch_addr[device]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            char msg[256];
+            std::snprintf(msg, sizeof msg, "cemx_energy_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            set_error(msg);
+            return nullptr;
+        }
+        g_scratch_addr[device] = static_cast<double *>(p);
+    }
+    return g_scratch_addr[device];
+}
+
+bool energy_noalloc(cem_sim *s, double *out) {
+    if (!s->dev) {
+        set_error("cemx_energy_noalloc: no device state (step the simulation first; this call never creates it)");
+        return false;
+    }
+    Device &D = *s->dev;
+    if (D.failed) { set_error(D.error_msg.c_str()); return false; }
+    if ((s->dev_valid & kGroupFields) != kGroupFields || (s->exposed & kGroupFields)) {
+        set_error("cemx_energy_noalloc: fields are held or modified on the host; use cem_energy");
+        return false;
+    }
+    const int gx = (D.g.plane + kBlock - 1) / kBlock;
+    const long long nblk = (long long)gx * (s->n[0] + 1);
+    if (nblk > kNoAllocPartials) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg,
+                      "cemx_energy_noalloc: grid needs %lld block partials, above the static scratch of %lld; "
+                      "use cem_energy", nblk, kNoAllocPartials);
+        set_error(msg);
+        return false;
+    }
+    CB2_CHECK(s, cudaSetDevice(D.device));
+    double *scratch = noalloc_scratch(D.device);
+    if (!scratch) return false;
+    EnergyArgs ea = D.ea[D.cur];
+    ea.partial = scratch;
+    k_energy<<<dim3(gx, s->n[0] + 1), kBlock, 0, D.stream>>>(ea);
+    k_sum<<<1, 1024, 0, D.stream>>>(scratch, nblk, scratch + kNoAllocPartials);
+    CB2_CHECK(s, cudaGetLastError());
+    CB2_CHECK(s, cudaMemcpyAsync(out, scratch + kNoAllocPartials, sizeof(double), cudaMemcpyDeviceToHost, D.stream));
+    CB2_CHECK(s, cudaStreamSynchronize(D.stream));
+    return true;
+}
+
 }  // namespace cb2
 
 using namespace cb2;
@@ -1964,6 +2035,12 @@ int cemx_use_fused(cem_sim *s, int on) {
     s->kernel_choice = on ? 1 : 0;
     if (s->dev) s->dev->use_fused = on != 0;
     return prev;
+}
+
+int cemx_energy_noalloc(cem_sim *s, double *out) {
+    if (!s || !out) { set_error("cemx_energy_noalloc: null argument"); return -1; }
+    if (!s->finalized) { set_error("not finalized"); return -1; }
+    return energy_noalloc(s, out) ? 0 : -1;
 }
 
 int cemx_synchronize(cem_sim *s) {

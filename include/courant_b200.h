@@ -49,6 +49,25 @@ CEM_API int cemx_release_device(cem_sim *s);
  * environment. Returns the previous setting, or -1. */
 CEM_API int cemx_use_fused(cem_sim *s, int on);
 
+/* Stored electromagnetic energy of s, like cem_energy (no counterpart in the
+ * reference core: it replaces nothing there), computed without allocating
+ * device memory. For callers that must not allocate while stepping: a
+ * serving process that has handed all free HBM to simulation instances (any
+ * cudaMalloc may fail there), or one that cannot accept the device-wide
+ * synchronisation a cudaFree implies. cem_energy may allocate: it creates
+ * the device state of a simulation that has none yet. This call uses the
+ * same kernels, so it returns the same value bit for bit, but keeps its
+ * block partials in one static device array per process and device (512 KiB,
+ * 65536 partials, about 16.7 million grid points); nothing in it has to
+ * start at zero. The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress) and should come before any stream capture on that
+ * device. Calls for simulations on the same device share the array and must
+ * not overlap in time (serialise them across threads).
+ * Fails (-1, cem_last_error() set) when s has no device state yet (step it
+ * first), when field pointers handed out by cem_field are live, or when the
+ * grid needs more than 65536 partials (use cem_energy). Returns 0 or -1. */
+CEM_API int cemx_energy_noalloc(cem_sim *s, double *energy);
+
 /* Wait for all device work of s. Returns 0 or -1. */
 CEM_API int cemx_synchronize(cem_sim *s);
 
