@@ -122,6 +122,15 @@ def algorithmic_bytes(z: dict) -> dict:
     }
 
 
+def _oracle():
+    """The oracle package's ctypes module (oracle/oracle.py): the reference core's location for the CPU legs."""
+    p = str(ROOT / "oracle")
+    if p not in sys.path:
+        sys.path.insert(1, p)
+    import oracle
+    return oracle
+
+
 def build_sim(lib, workload: str):
     from courant_b200 import scenes
     t = time.time()
@@ -132,7 +141,7 @@ def build_sim(lib, workload: str):
 
 def cpu_baseline(workload: str, steps_per_sample: int, samples: int) -> dict:
     """The reference core on the host cores, a bounded sample of the workload."""
-    import oracle
+    oracle = _oracle()
     from courant_b200.api import Courant
     ref = Courant(oracle.REF_LIB)
     s, meta = build_sim(ref, workload)
@@ -153,7 +162,7 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import oracle
+    oracle = _oracle()
     if not oracle.REF_LIB.exists():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcourant_ref.so was not built"}))
         return
@@ -260,7 +269,8 @@ def run_b200(args) -> None:
             specs = [s.vprobe(p) for p in range(nvp)] + [s.iprobe(p) for p in range(nip)]
             specs += [s.portV(p) for p in range(nport)] + [s.portI(p) for p in range(nport)]
             specs.append(s.sourceSpectrum())
-            d2h += sum(a.size * 16 for a in specs)
+            s.energy()   # run control, as the reference's board runner checks after every chunk
+            d2h += sum(a.size * 16 for a in specs) + 8
         torch.cuda.synchronize()
         wall = max_over_ranks(time.perf_counter() - t0)
         barrier()
@@ -268,11 +278,11 @@ def run_b200(args) -> None:
         e2e = {"value": world * cells * chunk * n_chunks / wall, "unit": "cell-updates/s",
                "h2d_bytes_per_step": int(z2["device_bytes"] / n_chunks), "d2h_bytes_per_step": int(d2h / n_chunks),
                "steps": n_chunks, "time_steps": n_chunks * chunk,
-               "note": "first step uploads plan and state (device_bytes); spectra read after every step"}
+               "note": "first step uploads plan and state (device_bytes); spectra and energy read after every step"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        import oracle
+        oracle = _oracle()
         if oracle.REF_LIB.exists():
             cpu = cpu_baseline(args.workload, args.ref_chunk, args.ref_samples)
 
