@@ -45,12 +45,15 @@ namespace cb2 {
 constexpr int kRing = 1024;          // sample rows kept on the device between DFT flushes
 constexpr int kBlock = 256;
 constexpr int kMaxSlots = 2 * kMaxProbes + kMaxPorts;
-constexpr unsigned kFlagDisp = 1, kFlagSrc = 2;
+constexpr int kPostThreads = 1024;   // k_post: one block
+constexpr int kMaxGridY = 65535;     // launches over node planes are split into chunks of this many
+constexpr int kPostStage = 4096;     // probe edge products staged in shared memory
+constexpr unsigned kFlagDisp = 1, kFlagSrc = 2, kFlagMode = 4;   // table entry flags: Debye, lumped source, mode source
 
 // ---------------------------------------------------------------- arguments
 
-// Device index space: rows padded to 16 bytes, q = i*si + j*sj + k with
-// sj = round_up(nz+1, 4) and si = (ny+1)*sj; padding elements (k > nz) stay
+// Device index space: rows padded to 32 bytes, q = i*si + j*sj + k with
+// sj = round_up(nz+1, 8) and si = (ny+1)*sj; padding elements (k > nz) stay
 // zero and belong to no field component. Host copies use the reference index
 // space (sj = nz+1) and are converted row by row at transfer.
 struct Geom {
@@ -64,17 +67,35 @@ struct PmlAxis {
     const int *plane_h, *plane_e;        // CPML plane of a cell / node, -1 outside
     const float *bm1_h, *cid_h;          // b-1 and c/d at cells (H auxiliaries)
     const float *bm1_e, *cid_e;          // b-1 and c/dd at nodes (E auxiliaries)
-    int per;                             // points per plane
-    int planes;                          // planes in the CPML slabs of this axis (z-axis layout stride)
+    int planes;                          // planes in the CPML slabs of this axis (cells and nodes alike)
+    const int *zoff_h, *zoff_e;          // z axis: position of k in its column window, -1 outside
+    int zw_h, zw_e;                      // z axis: window points per (i, j) column
 };
 
-// Device layout of the CPML auxiliaries: x and y slabs as in the reference
-// (plane-major, then the in-plane index); z slabs with the plane index
-// fastest, ((i*(ny+1) + j) * planes + plane), so the z-slab cells of one k
-// row sit next to each other. Host copies use the reference layout.
+// Device layout of the CPML auxiliaries, in the padded index space so that
+// four consecutive k move as one aligned float4:
+//   x slabs  plane * si + j * sj + k
+//   y slabs  (i * planes + plane) * sj + k
+//   z slabs  (i * (ny+1) + j) * zw + zoff[k], where each (i, j) column keeps
+//            a window of whole 4-point groups covering its z slabs.
+// Host copies use the reference's compact layout (sim.c:655-678) and are
+// converted at transfer.
+
+// The update kernels cover each node plane in k segments: the k axis is cut
+// at the CPML slab and Debye box boundaries (rounded down to multiples of 4),
+// and threads are laid out row by row within one segment, so the threads of
+// a warp share their k pattern and mostly take the same branch.
+constexpr int kMaxSegs = 12;
+struct KSegs {
+    int n;                                // segments
+    int k[kMaxSegs + 1];                  // boundaries: k[0] = 0, k[n] = sj, all multiples of 4
+    int blk[kMaxSegs + 1];                // first block of each segment; blk[n]: blocks per plane and component
+    unsigned long long magic[kMaxSegs];   // row of segment thread t: (t * magic) >> 40
+};
 
 struct StepArgs {
     Geom g;
+    KSegs seg_h, seg_e;
     float *E[3], *H[3];
     const float *hc[3];      // dt/mu0 * idh per axis (cells)
     const float *ec[3];      // ide per axis (nodes)
@@ -97,15 +118,16 @@ struct StepArgs {
     double m_t0, m_tau;
     const float *wsrc[2];    // mode-source weights of Ey and Ez on plane i_src
     const long long *dstep;
+    const float *srcv;       // lumped Vs and modal Vm at this step's H time, FP32 (source_values)
 };
 
 struct SibcArgs {
     int ns, K;
-    const int *ecomp;
-    const long long *eidx;
-    const int *hcomp;        // 4 per edge
-    const long long *hidx;   // 4 per edge
-    const float *hw;         // 4 per edge (0 beyond the face count)
+    const unsigned char *ecomp;
+    const unsigned *eidx;
+    const uchar4 *hcomp;     // H component of each face (0..2)
+    const uint4 *hidx;       // H index of each face
+    const float4 *hw;        // face weights (0 beyond the face count)
     float *y;                // K * ns, term-major
     float c[kSibcTerms], ome[kSibcTerms];
     float *E[3];
@@ -131,7 +153,7 @@ struct PostArgs {
     int nip, nport, nvp, nslot;
     const int *off;          // nin + 1 entry offsets
     const unsigned char *ecomp;   // 0..5
-    const long long *eidx;
+    const unsigned *eidx;
     const double *ew;
     const double *R;
     double *vold;
@@ -142,6 +164,7 @@ struct PostArgs {
     double *ring;            // kRing * nslot
     const float *F[6];
     long long *dstep;
+    float *srcv;             // source values of the step the E update runs next
     int advance;             // 1: count this step
 };
 
@@ -210,40 +233,56 @@ __device__ __forceinline__ Plane plane_at(const StepArgs &a, int i) {
     return p;
 }
 
-// compact index of a CPML auxiliary for derivative axis A (device layout, see PmlAxis)
-template <int A>
+// device index of the CPML auxiliary at (i, j, k) for derivative axis A,
+// E (nodes) or H (cells); plane: the point's slab plane on axis A (x, y)
+template <int A, bool E>
 __device__ __forceinline__ int psi_at(const StepArgs &a, int plane, int i, int j, int k) {
-    if (A == 0) return plane * a.pml[0].per + j * (a.g.n[2] + 1) + k;
-    if (A == 1) return plane * a.pml[1].per + i * (a.g.n[2] + 1) + k;
-    return (i * (a.g.n[1] + 1) + j) * a.pml[2].planes + plane;
+    if (A == 0) return plane * (int)a.g.si + j * a.g.sj + k;
+    if (A == 1) return (i * a.pml[1].planes + plane) * a.g.sj + k;
+    return (i * (a.g.n[1] + 1) + j) * (E ? a.pml[2].zw_e : a.pml[2].zw_h) +
+           (E ? a.pml[2].zoff_e : a.pml[2].zoff_h)[k];
 }
 
 // H component C at (i, j, k) (reference sim.c:579-606, CPML :680-754):
 //   H_C -= dt/mu0 [ (d1 c1 + psi_{C,0}) - (d2 c2 + psi_{C,1}) ]
 // with d1 = dE_{C+2} along axis C+1, d2 = dE_{C+1} along axis C+2, c1, c2 the
-// kappa-scaled inverse cell sizes times dt/mu0, p1, p2 the CPML planes of the
-// two derivative axes (-1 outside). psi read from `pin`, written to `pout`
-// when STORE.
+// kappa-scaled inverse cell sizes times dt/mu0. in1, in2: the point lies in
+// the CPML slab of that derivative axis; s1, s2 then hold the old auxiliary
+// on entry and the new one on exit.
+template <int C>
+__device__ __forceinline__ float h_value(const StepArgs &a, int i, int j, int k, float h, float d1, float d2,
+                                         float c1, float c2, bool in1, bool in2, float &s1, float &s2) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    const int idx[3] = {i, j, k};
+    float t1 = __fmul_rn(d1, c1), t2 = __fmul_rn(d2, c2);
+    if (in1) {
+        s1 = psi_next(s1, a.pml[A1].bm1_h[idx[A1]], a.pml[A1].cid_h[idx[A1]], d1);
+        t1 = __fmaf_rn(a.dth, s1, t1);
+    }
+    if (in2) {
+        s2 = psi_next(s2, a.pml[A2].bm1_h[idx[A2]], a.pml[A2].cid_h[idx[A2]], d2);
+        t2 = __fmaf_rn(a.dth, s2, t2);
+    }
+    return __fsub_rn(h, __fsub_rn(t1, t2));
+}
+
+// h_value with the auxiliaries read from `pin` and, when STORE, written to
+// `pout`; p1, p2 are the CPML planes of the two derivative axes (-1 outside).
 template <int C, bool STORE>
 __device__ __forceinline__ float h_comp(const StepArgs &a, float *const (&pin)[3][2], float *const (&pout)[3][2],
                                         int i, int j, int k, float h, float d1, float d2, float c1, float c2, int p1,
                                         int p2) {
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
-    const int idx[3] = {i, j, k};
-    float t1 = __fmul_rn(d1, c1), t2 = __fmul_rn(d2, c2);
-    if (p1 >= 0) {
-        const int x = psi_at<A1>(a, p1, i, j, k);
-        const float psi = psi_next(pin[C][0][x], a.pml[A1].bm1_h[idx[A1]], a.pml[A1].cid_h[idx[A1]], d1);
-        if (STORE) pout[C][0][x] = psi;
-        t1 = __fmaf_rn(a.dth, psi, t1);
+    int x1 = 0, x2 = 0;
+    float s1 = 0.f, s2 = 0.f;
+    if (p1 >= 0) { x1 = psi_at<A1, false>(a, p1, i, j, k); s1 = pin[C][0][x1]; }
+    if (p2 >= 0) { x2 = psi_at<A2, false>(a, p2, i, j, k); s2 = pin[C][1][x2]; }
+    const float r = h_value<C>(a, i, j, k, h, d1, d2, c1, c2, p1 >= 0, p2 >= 0, s1, s2);
+    if (STORE) {
+        if (p1 >= 0) pout[C][0][x1] = s1;
+        if (p2 >= 0) pout[C][1][x2] = s2;
     }
-    if (p2 >= 0) {
-        const int x = psi_at<A2>(a, p2, i, j, k);
-        const float psi = psi_next(pin[C][1][x], a.pml[A2].bm1_h[idx[A2]], a.pml[A2].cid_h[idx[A2]], d2);
-        if (STORE) pout[C][1][x] = psi;
-        t2 = __fmaf_rn(a.dth, psi, t2);
-    }
-    return __fsub_rn(h, __fsub_rn(t1, t2));
+    return r;
 }
 
 // All three H components at (i, j, k) for the fused step. e*: E at the point;
@@ -265,216 +304,530 @@ __device__ __forceinline__ void h_point(const StepArgs &a, const Column &col, co
                               pl.phi, col.phj);
 }
 
-// Per-edge epilogue: material table, Debye correction and update, sources.
+// Per-edge epilogue: material table, Debye correction, sources.
 //   E = E + (ca-1) E + cb [curl - sum_p hk_p J_p] + cs Vs(t) + w Vm(t)
-//   J_p += -(1-k_p) J_p + beta_p/dt (E_new - E_old)
-// P (the number of Debye poles) is a template parameter so the pole loops
-// unroll and the currents stay in registers.
-// (reference sim.c:608-637, :894-910; dispersive.c:93-112; modeport.c:130-135)
-template <int C, int P>
-__device__ __forceinline__ float e_finish(const StepArgs &a, int mi, float e_old, float curl, int i, int j, int k,
-                                          long long step) {
-    const float4 t = __ldg(a.tab4[C] + mi);   // ca-1, cb, cs, flags
+// t: the edge's packed table entry (ca-1, cb, cs, flags); jsum: sum_p hk_p J_p
+// of the edge's Debye currents (debye_sum), used when t flags the edge
+// dispersive; sv: this step's source values (source_values).
+// (reference sim.c:608-637, :894-910; dispersive.c:93-104; modeport.c:130-135)
+template <int C>
+__device__ __forceinline__ float e_finish(const StepArgs &a, const float4 t, float e_old, float curl, int j, int k,
+                                          const float2 sv, float jsum) {
     const unsigned flag = __float_as_uint(t.w);
     const float base = __fmaf_rn(t.x, e_old, e_old);
     if (!flag) return __fmaf_rn(t.y, curl, base);
-    int jo = 0, jvol = 0;
-    float jv[P > 0 ? P : 1];
-    if (P > 0 && (flag & kFlagDisp)) {
-        const int *bx = a.jbox[C];
-        jvol = bx[3] * bx[4] * bx[5];
-        jo = ((i - bx[0]) * bx[4] + (j - bx[1])) * bx[5] + (k - bx[2]);
-        float acc = 0.f;
-#pragma unroll
-        for (int p = 0; p < P; p++) {
-            jv[p] = a.J[C][p * jvol + jo];
-            acc = __fmaf_rn(a.hk[p], jv[p], acc);
-        }
-        curl = __fsub_rn(curl, acc);
-    }
+    if (flag & kFlagDisp) curl = __fsub_rn(curl, jsum);
     float e = __fmaf_rn(t.y, curl, base);
-    if (flag & kFlagSrc) {
-        const double tH = ((double)step + 0.5) * a.dt;
-        e = __fmaf_rn(t.z, (float)gauss(tH, a.src_amp, a.src_t0, a.src_tau), e);
-    }
-    if (C > 0 && a.msrc_on && i == a.i_src) {
+    if (flag & kFlagSrc) e = __fmaf_rn(t.z, sv.x, e);
+    if (C > 0 && (flag & kFlagMode)) {
         const float w = a.wsrc[C - 1][j * (a.g.n[2] + 1) + k];
-        if (w != 0.f) {
-            const double tH = ((double)step + 0.5) * a.dt;
-            e = __fmaf_rn(w, (float)dgauss(tH, a.m_t0, a.m_tau), e);
-        }
-    }
-    if (P > 0 && (flag & kFlagDisp)) {
-        const float de = __fsub_rn(e, e_old);
-        const int nt = a.ntab[C];
-#pragma unroll
-        for (int p = 0; p < P; p++) {
-            const float bidt = __ldg(a.tab[C] + (3 + p) * nt + mi);
-            a.J[C][p * jvol + jo] = __fmaf_rn(bidt, de, __fmaf_rn(-a.omk[p], jv[p], jv[p]));
-        }
+        if (w != 0.f) e = __fmaf_rn(w, sv.y, e);
     }
     return e;
 }
 
+// sum_p hk_p J_p accumulated in pole order, one term at a time
+__device__ __forceinline__ float debye_term(const StepArgs &a, int p, float jp, float acc) {
+    return __fmaf_rn(a.hk[p], jp, acc);
+}
+
+// Debye current update of pole p of a dispersive edge with table index mi
+// (reference dispersive.c:105-112): J_p += -(1-k_p) J_p + beta_p/dt (E_new - E_old)
+template <int C>
+__device__ __forceinline__ float debye_next(const StepArgs &a, int p, int mi, float de, float jp) {
+    const float bidt = __ldg(a.tab[C] + (3 + p) * a.ntab[C] + mi);
+    return __fmaf_rn(bidt, de, __fmaf_rn(-a.omk[p], jp, jp));
+}
+
 // E component C at (i, j, k) (reference sim.c:608-637, CPML :756-832):
 //   E_C = ca E + cb [ (d1 c1 + psi_{C,0}) - (d2 c2 + psi_{C,1}) ] + epilogue
-// with d1 = dH_{C+2} along axis C+1, d2 = dH_{C+1} along axis C+2.
-template <int C, int P>
-__device__ __forceinline__ float e_comp(const StepArgs &a, int i, int j, int k, long long step, float e, float d1,
-                                        float d2, float c1, float c2, int p1, int p2, int mi) {
+// with d1 = dH_{C+2} along axis C+1, d2 = dH_{C+1} along axis C+2; in1, in2,
+// s1, s2 as for h_value.
+template <int C>
+__device__ __forceinline__ float e_value(const StepArgs &a, const float4 t, int i, int j, int k, const float2 sv,
+                                         float e, float d1, float d2, float c1, float c2, bool in1, bool in2,
+                                         float &s1, float &s2, float jsum) {
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
     const int idx[3] = {i, j, k};
     float t1 = __fmul_rn(d1, c1), t2 = __fmul_rn(d2, c2);
-    if (p1 >= 0) {
-        float *arr = a.psiE[C][0];
-        const int x = psi_at<A1>(a, p1, i, j, k);
-        const float psi = psi_next(arr[x], a.pml[A1].bm1_e[idx[A1]], a.pml[A1].cid_e[idx[A1]], d1);
-        arr[x] = psi;
-        t1 = __fadd_rn(t1, psi);
+    if (in1) {
+        s1 = psi_next(s1, a.pml[A1].bm1_e[idx[A1]], a.pml[A1].cid_e[idx[A1]], d1);
+        t1 = __fadd_rn(t1, s1);
     }
-    if (p2 >= 0) {
-        float *arr = a.psiE[C][1];
-        const int x = psi_at<A2>(a, p2, i, j, k);
-        const float psi = psi_next(arr[x], a.pml[A2].bm1_e[idx[A2]], a.pml[A2].cid_e[idx[A2]], d2);
-        arr[x] = psi;
-        t2 = __fadd_rn(t2, psi);
+    if (in2) {
+        s2 = psi_next(s2, a.pml[A2].bm1_e[idx[A2]], a.pml[A2].cid_e[idx[A2]], d2);
+        t2 = __fadd_rn(t2, s2);
     }
-    return e_finish<C, P>(a, mi, e, __fsub_rn(t1, t2), i, j, k, step);
+    return e_finish<C>(a, t, e, __fsub_rn(t1, t2), j, k, sv, jsum);
+}
+
+// offset of (i, j, k) in component C's dense Debye box, -1 outside
+template <int C>
+__device__ __forceinline__ int jbox_at(const StepArgs &a, int i, int j, int k) {
+    const int *bx = a.jbox[C];
+    const int di = i - bx[0], dj = j - bx[1], dk = k - bx[2];
+    if ((unsigned)di >= (unsigned)bx[3] || (unsigned)dj >= (unsigned)bx[4] || (unsigned)dk >= (unsigned)bx[5]) return -1;
+    return (di * bx[4] + dj) * bx[5] + dk;
+}
+
+template <int C>
+__device__ __forceinline__ int jbox_volume(const StepArgs &a) {
+    return a.jbox[C][3] * a.jbox[C][4] * a.jbox[C][5];
+}
+
+// E value with auxiliaries and Debye currents read and written in place
+// (fused step; p1, p2: CPML planes as for h_comp; mi: table index)
+template <int C, int P>
+__device__ __forceinline__ float e_comp(const StepArgs &a, int i, int j, int k, const float2 sv, float e, float d1,
+                                        float d2, float c1, float c2, int p1, int p2, int mi) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    int x1 = 0, x2 = 0;
+    float s1 = 0.f, s2 = 0.f;
+    if (p1 >= 0) { x1 = psi_at<A1, true>(a, p1, i, j, k); s1 = a.psiE[C][0][x1]; }
+    if (p2 >= 0) { x2 = psi_at<A2, true>(a, p2, i, j, k); s2 = a.psiE[C][1][x2]; }
+    const float4 t = __ldg(a.tab4[C] + mi);
+    const bool disp = P > 0 && (__float_as_uint(t.w) & kFlagDisp);
+    float jsum = 0.f;
+    int jo = 0;
+    const int jvol = P > 0 ? jbox_volume<C>(a) : 0;
+    if (disp) {
+        jo = jbox_at<C>(a, i, j, k);
+#pragma unroll
+        for (int p = 0; p < P; p++) jsum = debye_term(a, p, a.J[C][p * jvol + jo], jsum);
+    }
+    const float r = e_value<C>(a, t, i, j, k, sv, e, d1, d2, c1, c2, p1 >= 0, p2 >= 0, s1, s2, jsum);
+    if (p1 >= 0) a.psiE[C][0][x1] = s1;
+    if (p2 >= 0) a.psiE[C][1][x2] = s2;
+    if (disp) {
+        const float de = __fsub_rn(r, e);
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            float *jp = a.J[C] + p * jvol + jo;
+            *jp = debye_next<C>(a, p, mi, de, *jp);
+        }
+    }
+    return r;
 }
 
 // All three E components at (i, j, k) for the fused step. h*: H at the point;
 // *_jm, *_km: at j-1, k-1; hy_p, hz_p: at i-1. e* in: old, out: new.
 template <int P>
 __device__ __forceinline__ void e_point(const StepArgs &a, const Column &col, const Plane &pl, int i, int j, int k,
-                                        long long step, float hx, float hy, float hz, float hz_jm, float hx_jm,
+                                        const float2 sv, float hx, float hy, float hz, float hz_jm, float hx_jm,
                                         float hy_km, float hx_km, float hy_p, float hz_p, int m0, int m1, int m2,
                                         float &ex, float &ey, float &ez) {
     const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
     if (i >= nx) return;
     const bool jin = j >= 1 && j < ny, kin = k >= 1 && k < nz;
     if (jin && kin)
-        ex = e_comp<0, P>(a, i, j, k, step, ex, __fsub_rn(hz, hz_jm), __fsub_rn(hy, hy_km), col.ecy, col.ecz, col.pej,
-                       col.pek, m0);
+        ex = e_comp<0, P>(a, i, j, k, sv, ex, __fsub_rn(hz, hz_jm), __fsub_rn(hy, hy_km), col.ecy, col.ecz, col.pej,
+                          col.pek, m0);
     if (i < 1) return;
     if (j < ny && kin)
-        ey = e_comp<1, P>(a, i, j, k, step, ey, __fsub_rn(hx, hx_km), __fsub_rn(hz, hz_p), col.ecz, pl.ecx, col.pek,
-                       pl.pei, m1);
+        ey = e_comp<1, P>(a, i, j, k, sv, ey, __fsub_rn(hx, hx_km), __fsub_rn(hz, hz_p), col.ecz, pl.ecx, col.pek,
+                          pl.pei, m1);
     if (jin && k < nz)
-        ez = e_comp<2, P>(a, i, j, k, step, ez, __fsub_rn(hy, hy_p), __fsub_rn(hx, hx_jm), pl.ecx, col.ecy, pl.pei,
-                       col.pej, m2);
+        ez = e_comp<2, P>(a, i, j, k, sv, ez, __fsub_rn(hy, hy_p), __fsub_rn(hx, hx_jm), pl.ecx, col.ecy, pl.pei,
+                          col.pej, m2);
 }
 
 // ------------------------------------------------ separate phase kernels
 //
-// One thread per field component of a (j,k) column, marching over kU node
-// planes along x with the loads of all kU planes issued before any
-// arithmetic. The three components of a chunk of the plane sit in adjacent
-// blocks, so the neighbour values they share come from L2.
+// One thread per field component and per four consecutive k points of one
+// padded row (one aligned float4) of one node plane. Fields move as 16-byte
+// loads and stores, material indices as 8-byte loads; the k+1 / k-1
+// neighbour of the four points comes from the adjacent lane by a warp
+// shuffle (the lane at the warp's edge loads it). The CPML auxiliaries and
+// Debye currents of all four points are loaded before any arithmetic, so
+// their latencies overlap. Points a component does not own (boundary
+// tangential E, row padding) are written back unchanged.
 
-constexpr int kU = 4;
+__device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+__device__ __forceinline__ void st4(float *p, const float4 &v) { *reinterpret_cast<float4 *>(p) = v; }
+
+// values at q+1 .. q+4 from v = values at q .. q+3: the next lane's first
+// element, unless this lane ends a run of consecutive points (`edge`: last
+// lane of the warp or of its segment row), which loads p[4] when `need`.
+// Every lane of the warp must call it.
+__device__ __forceinline__ float4 next_k(const float4 &v, const float *p, bool need, bool edge) {
+    float w = __shfl_down_sync(0xffffffffu, v.x, 1);
+    if (edge && need) w = __ldg(p + 4);
+    return make_float4(v.y, v.z, v.w, w);
+}
+
+// values at q-1 .. q+2 (a lane that starts a run loads p[-1] when `need`)
+__device__ __forceinline__ float4 prev_k(const float4 &v, const float *p, bool need, bool edge) {
+    float w = __shfl_up_sync(0xffffffffu, v.w, 1);
+    if (edge && need) w = __ldg(p - 1);
+    return make_float4(w, v.x, v.y, v.z);
+}
+
+// Position of this thread: row j and first point k4 of its four, inside the
+// k segment [ks, ke) that block b (per component) belongs to.
+struct RowPos {
+    int j, k4, ks, ke;
+    bool act;
+};
+
+__device__ __forceinline__ RowPos row_pos(const KSegs &sg, int rows, int b) {
+    int s = 0;
+    while (s + 1 < sg.n && b >= sg.blk[s + 1]) s++;
+    RowPos r;
+    r.ks = sg.k[s];
+    r.ke = sg.k[s + 1];
+    const int nk4 = (r.ke - r.ks) >> 2;
+    const int t = (b - sg.blk[s]) * kBlock + threadIdx.x;
+    r.act = t < rows * nk4;
+    r.j = r.act ? (int)(((unsigned long long)t * sg.magic[s]) >> 40) : 0;
+    r.k4 = r.ks + 4 * (t - r.j * nk4);
+    return r;
+}
 
 template <int A>
 __device__ __forceinline__ int stride_of(const StepArgs &a) {
     return A == 0 ? (int)a.g.si : (A == 1 ? a.g.sj : 1);
 }
 
+__device__ __forceinline__ float lane4(const float4 &v, int e) {
+    return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+
+__device__ __forceinline__ void set4(float4 &v, int e, float x) {
+    if (e == 0) v.x = x;
+    else if (e == 1) v.y = x;
+    else if (e == 2) v.z = x;
+    else v.w = x;
+}
+
+__device__ __forceinline__ int lane4i(const int4 &v, int e) {
+    return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+
+// Where four points k4 .. k4+3 of row (i, j) stand for component C: the
+// CPML planes of the derivative axes (x, y: the row's; z: per point), and
+// whether any of them needs the general path (CPML; for E also the Debye box,
+// jo4 >= 0 the points' offset in it).
+struct Where {
+    int pi, pj;
+    int4 pk;
+    int jo4;
+    bool gen;
+};
+
 template <int C>
-__device__ __forceinline__ void h_march(const StepArgs &a, int ib, int ie, int j, int k, int m) {
+__device__ __forceinline__ Where h_where(const StepArgs &a, int i, int j, int k4) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    Where w{-1, -1, make_int4(-1, -1, -1, -1), -1, false};
+    if (a.has_pml) {
+        if ((A1 == 0 || A2 == 0) && i < a.g.n[0]) w.pi = a.pml[0].plane_h[i];
+        if ((A1 == 1 || A2 == 1) && j < a.g.n[1]) w.pj = a.pml[1].plane_h[j];
+        if (A1 == 2 || A2 == 2) w.pk = __ldg(reinterpret_cast<const int4 *>(a.pml[2].plane_h + k4));
+    }
+    w.gen = w.pi >= 0 || w.pj >= 0 || max(max(w.pk.x, w.pk.y), max(w.pk.z, w.pk.w)) >= 0;
+    return w;
+}
+
+// H component C at points k4 .. k4+3 of row (i, j) from the E values there
+// (e2 = E_{C+2}, e1 = E_{C+1}) and one step along the derivative axes (e2n
+// along C+1, e1n along C+2), h the old H, w from h_where; the new H goes to
+// hq.
+template <int C>
+__device__ __forceinline__ void h_points(const StepArgs &a, int i, int j, int k4, float *hq, const Where &w,
+                                         const float4 &e2, const float4 &e2n, const float4 &e1, const float4 &e1n,
+                                         float4 h) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    constexpr bool kz = A1 == 2 || A2 == 2;
+    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    // coefficients and CPML planes of the derivative axes
+    const float ci = a.hc[0][min(i, nx - 1)], cj = a.hc[1][min(j, ny - 1)];
+    const float4 ck = ldg4(a.hc[2] + k4);
+    const int pi = w.pi, pj = w.pj;
+    const int4 pk = w.pk;
+    const int pa[3] = {pi, pj, max(max(pk.x, pk.y), max(pk.z, pk.w))};
+    if (!w.gen) {
+        // no CPML on either derivative axis at any of the four points
+        float s = 0.f;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int k = k4 + e;
+            if (!(kz ? k < nz : k <= nz)) continue;
+            const float c[3] = {ci, cj, lane4(ck, e)};
+            set4(h, e, h_value<C>(a, i, j, k, lane4(h, e), __fsub_rn(lane4(e2n, e), lane4(e2, e)),
+                                  __fsub_rn(lane4(e1n, e), lane4(e1, e)), c[A1], c[A2], false, false, s, s));
+        }
+        st4(hq, h);
+        return;
+    }
+    // CPML on a derivative axis: the auxiliaries of the four points move as
+    // float4 (padded layout); only points inside a slab change theirs
+    const bool any1 = pa[A1] >= 0, any2 = pa[A2] >= 0;
+    const int x1 = any1 ? psi_at<A1, false>(a, pa[A1], i, j, k4) : 0;
+    const int x2 = any2 ? psi_at<A2, false>(a, pa[A2], i, j, k4) : 0;
+    float4 s1 = any1 ? ld4(a.psiH[C][0] + x1) : z4;
+    float4 s2 = any2 ? ld4(a.psiH[C][1] + x2) : z4;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int k = k4 + e;
+        if (!(kz ? k < nz : k <= nz)) continue;
+        const bool in1 = A1 == 2 ? lane4i(pk, e) >= 0 : any1;
+        const bool in2 = A2 == 2 ? lane4i(pk, e) >= 0 : any2;
+        float q1 = lane4(s1, e), q2 = lane4(s2, e);
+        const float c[3] = {ci, cj, lane4(ck, e)};
+        set4(h, e, h_value<C>(a, i, j, k, lane4(h, e), __fsub_rn(lane4(e2n, e), lane4(e2, e)),
+                              __fsub_rn(lane4(e1n, e), lane4(e1, e)), c[A1], c[A2], in1, in2, q1, q2));
+        set4(s1, e, q1);
+        set4(s2, e, q2);
+    }
+    st4(hq, h);
+    if (any1) st4(a.psiH[C][0] + x1, s1);
+    if (any2) st4(a.psiH[C][1] + x2, s2);
+}
+
+// H component C on points k4 .. k4+3 of row (i, j) (segment [ks, ke))
+template <int C>
+__device__ __forceinline__ void h_vec(const StepArgs &a, int i, const RowPos &r) {
+    const int j = r.j, k4 = r.k4;
+    const int m = j * a.g.sj + k4;
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
     const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
-    const int jk[3] = {0, j, k};
-    if ((A1 != 0 && jk[A1] >= a.g.n[A1]) || (A2 != 0 && jk[A2] >= a.g.n[A2]) || k > nz) return;
-    const int last = (A1 == 0 || A2 == 0) ? min(ie, nx) : ie;   // an x-derivative needs plane i+1
-    const int si = (int)a.g.si, s1 = stride_of<A1>(a), s2 = stride_of<A2>(a);
+    // derivative axes x and y need i < nx, j < ny (the row's own axis goes to n)
+    const bool valid = r.act && (!(A1 == 0 || A2 == 0) || i < nx) && (!(A1 == 1 || A2 == 1) || j < ny);
+    const Where w = valid ? h_where<C>(a, i, j, k4) : Where{-1, -1, make_int4(-1, -1, -1, -1), -1, false};
+    const bool row = valid;
+    const int q = i * (int)a.g.si + m;
     const float *__restrict__ E2 = a.E[A2];
     const float *__restrict__ E1 = a.E[A1];
     float *__restrict__ H = a.H[C];
-    float e2[kU], e2n[kU], e1[kU], e1n[kU], h[kU];
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 e2 = z4, e1 = z4, h = z4, e2n = z4, e1n = z4;
+    if (row) {
+        e2 = ldg4(E2 + q);
+        e1 = ldg4(E1 + q);
+        h = ld4(H + q);
+        if (A1 != 2) e2n = ldg4(E2 + q + stride_of<A1>(a));
+        if (A2 != 2) e1n = ldg4(E1 + q + stride_of<A2>(a));
+    }
+    // the next lane holds the next four points only if it is in the same run and loaded them
+    const bool nb = __shfl_down_sync(0xffffffffu, row, 1);
+    const bool edge = (threadIdx.x & 31) == 31 || k4 + 4 >= r.ke || !nb;
+    if (A1 == 2) e2n = next_k(e2, E2 + q, row && k4 + 4 <= nz, edge);
+    if (A2 == 2) e1n = next_k(e1, E1 + q, row && k4 + 4 <= nz, edge);
+    if (!row) return;
+    h_points<C>(a, i, j, k4, H + q, w, e2, e2n, e1, e1n, h);
+}
+
+// e_where: as h_where for E; CPML planes of nodes, and the Debye box
+template <int C, int P>
+__device__ __forceinline__ Where e_where(const StepArgs &a, int i, int j, int k4) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    Where w{-1, -1, make_int4(-1, -1, -1, -1), -1, false};
+    if (a.has_pml) {
+        if (A1 == 0 || A2 == 0) w.pi = a.pml[0].plane_e[i];
+        if (A1 == 1 || A2 == 1) w.pj = a.pml[1].plane_e[j];
+        if (A1 == 2 || A2 == 2) w.pk = __ldg(reinterpret_cast<const int4 *>(a.pml[2].plane_e + k4));
+    }
+    // the four points' offset in the Debye box, whose k extent is aligned to
+    // four points: all four are inside or all outside
+    const int *bx = a.jbox[C];
+    if (P > 0 && k4 >= bx[2] && k4 < bx[2] + bx[5]) w.jo4 = jbox_at<C>(a, i, j, k4);
+    w.gen = w.pi >= 0 || w.pj >= 0 || max(max(w.pk.x, w.pk.y), max(w.pk.z, w.pk.w)) >= 0 || w.jo4 >= 0;
+    return w;
+}
+
+// E component C at points k4 .. k4+3 of row (i, j) from the H values there
+// (h2 = H_{C+2}, h1 = H_{C+1}) and one step back along the derivative axes
+// (h2m along C+1, h1m along C+2), the old E ev and the material indices mv,
+// w from e_where; the new E goes to eq. Points with no CPML on a derivative
+// axis and outside the Debye box take a short path (sources included); the
+// others update CPML auxiliaries and Debye currents, the currents of all
+// four points read in one pass (sum_p hk_p J_p) and re-read from L1 for
+// their update.
+template <int C, int P>
+__device__ __forceinline__ void e_points(const StepArgs &a, int i, int j, int k4, float *eq, const Where &w,
+                                         const float4 &h2, const float4 &h2m, const float4 &h1, const float4 &h1m,
+                                         float4 ev, const uint2 mv, const float2 sv) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    const int nz = a.g.n[2];
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float ci = a.ec[0][i], cj = a.ec[1][j];
+    const float4 ck = ldg4(a.ec[2] + k4);
+    const int pi = w.pi, pj = w.pj;
+    const int4 pk = w.pk;
+    const int pa[3] = {pi, pj, max(max(pk.x, pk.y), max(pk.z, pk.w))};
+    const int jo4 = w.jo4;
+    const bool box = jo4 >= 0;
+    const int mi[4] = {(int)(mv.x & 0xffffu), (int)(mv.x >> 16), (int)(mv.y & 0xffffu), (int)(mv.y >> 16)};
+    float4 t[4];
+    unsigned flags = 0;
 #pragma unroll
-    for (int u = 0; u < kU; u++) {
-        const int q = (ib + u) * si + m;
-        if (ib + u < last) {
-            e2[u] = E2[q]; e2n[u] = E2[q + s1]; e1[u] = E1[q]; e1n[u] = E1[q + s2]; h[u] = H[q];
+    for (int e = 0; e < 4; e++) {
+        t[e] = __ldg(a.tab4[C] + mi[e]);   // index 0 (PEC, padding) for points E does not own
+        flags |= __float_as_uint(t[e].w);
+    }
+    // sources (lumped and modal) need no general path: their flags are
+    // handled by e_finish; dispersive edges lie inside the Debye box
+    if (!w.gen) {
+        float s = 0.f;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int k = k4 + e;
+            if (!(C == 2 ? k < nz : (k >= 1 && k < nz))) continue;
+            const float c[3] = {ci, cj, lane4(ck, e)};
+            set4(ev, e, e_value<C>(a, t[e], i, j, k, sv, lane4(ev, e), __fsub_rn(lane4(h2, e), lane4(h2m, e)),
+                                   __fsub_rn(lane4(h1, e), lane4(h1m, e)), c[A1], c[A2], false, false, s, s, 0.f));
+        }
+        st4(eq, ev);
+        return;
+    }
+    const bool any1 = pa[A1] >= 0, any2 = pa[A2] >= 0;
+    const int x1 = any1 ? psi_at<A1, true>(a, pa[A1], i, j, k4) : 0;
+    const int x2 = any2 ? psi_at<A2, true>(a, pa[A2], i, j, k4) : 0;
+    float4 s1 = any1 ? ld4(a.psiE[C][0] + x1) : z4;
+    float4 s2 = any2 ? ld4(a.psiE[C][1] + x2) : z4;
+    float jsum[4] = {0.f, 0.f, 0.f, 0.f};
+    const int jvol = P > 0 ? jbox_volume<C>(a) : 0;
+    // sum_p hk_p J_p of the four points (currents of points that are not
+    // dispersive are never written and stay zero; their sum is unused)
+    if (P > 0 && box) {
+#pragma unroll
+        for (int p = 0; p < (P > 0 ? P : 1); p++) {
+            const float4 jp = ld4(a.J[C] + p * jvol + jo4);
+#pragma unroll
+            for (int e = 0; e < 4; e++) jsum[e] = debye_term(a, p, lane4(jp, e), jsum[e]);
         }
     }
-    const float cj = a.hc[1][min(j, ny - 1)], ck = a.hc[2][min(k, nz - 1)];
-    const int pj = a.has_pml && j < ny ? a.pml[1].plane_h[j] : -1, pk = a.has_pml && k < nz ? a.pml[2].plane_h[k] : -1;
+    float4 eo = ev;
 #pragma unroll
-    for (int u = 0; u < kU; u++) {
-        const int i = ib + u;
-        if (i >= last) break;
-        const float ci = a.hc[0][min(i, nx - 1)];
-        const int pi = a.has_pml && i < nx ? a.pml[0].plane_h[i] : -1;
-        const float c[3] = {ci, cj, ck};
-        const int pp[3] = {pi, pj, pk};
-        H[i * si + m] = h_comp<C, true>(a, a.psiH, a.psiH, i, j, k, h[u], __fsub_rn(e2n[u], e2[u]),
-                                        __fsub_rn(e1n[u], e1[u]), c[A1], c[A2], pp[A1], pp[A2]);
+    for (int e = 0; e < 4; e++) {
+        const int k = k4 + e;
+        if (!(C == 2 ? k < nz : (k >= 1 && k < nz))) continue;
+        const bool in1 = A1 == 2 ? lane4i(pk, e) >= 0 : any1;
+        const bool in2 = A2 == 2 ? lane4i(pk, e) >= 0 : any2;
+        float q1 = lane4(s1, e), q2 = lane4(s2, e);
+        const float c[3] = {ci, cj, lane4(ck, e)};
+        set4(ev, e, e_value<C>(a, t[e], i, j, k, sv, lane4(ev, e), __fsub_rn(lane4(h2, e), lane4(h2m, e)),
+                               __fsub_rn(lane4(h1, e), lane4(h1m, e)), c[A1], c[A2], in1, in2, q1, q2, jsum[e]));
+        set4(s1, e, q1);
+        set4(s2, e, q2);
+    }
+    st4(eq, ev);
+    if (any1) st4(a.psiE[C][0] + x1, s1);
+    if (any2) st4(a.psiE[C][1] + x2, s2);
+    if (P > 0 && box && (flags & kFlagDisp)) {
+        bool disp[4];
+        float de[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int k = k4 + e;
+            disp[e] = (C == 2 ? k < nz : (k >= 1 && k < nz)) && (__float_as_uint(t[e].w) & kFlagDisp);
+            de[e] = __fsub_rn(lane4(ev, e), lane4(eo, e));
+        }
+#pragma unroll
+        for (int p = 0; p < (P > 0 ? P : 1); p++) {
+            float *jp = a.J[C] + p * jvol + jo4;
+            float4 jv = ld4(jp);
+#pragma unroll
+            for (int e = 0; e < 4; e++)
+                if (disp[e]) set4(jv, e, debye_next<C>(a, p, mi[e], de[e], lane4(jv, e)));
+            st4(jp, jv);
+        }
     }
 }
 
+// E component C on points k4 .. k4+3 of row (i, j) (segment [ks, ke))
 template <int C, int P>
-__device__ __forceinline__ void e_march(const StepArgs &a, int ib, int ie, int j, int k, int m, long long step) {
+__device__ __forceinline__ void e_vec(const StepArgs &a, int i, const RowPos &r, const float2 sv) {
+    const int j = r.j, k4 = r.k4;
+    const int m = j * a.g.sj + k4;
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
-    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
-    const int jk[3] = {0, j, k};
+    const int nx = a.g.n[0], ny = a.g.n[1];
     // own axis: index < n; transverse axes: 1 <= index < n
-    if (C != 0 && jk[C] >= a.g.n[C]) return;
-    if (A1 != 0 && (jk[A1] < 1 || jk[A1] >= a.g.n[A1])) return;
-    if (A2 != 0 && (jk[A2] < 1 || jk[A2] >= a.g.n[A2])) return;
-    const int first = C == 0 ? ib : max(ib, 1), last = min(ie, nx);
-    const int si = (int)a.g.si, s1 = stride_of<A1>(a), s2 = stride_of<A2>(a);
+    const bool valid = r.act && i < nx && (C == 0 || i >= 1) && (C == 1 ? j < ny : (j >= 1 && j < ny));
+    const Where w = valid ? e_where<C, P>(a, i, j, k4) : Where{-1, -1, make_int4(-1, -1, -1, -1), -1, false};
+    const bool row = valid;
+    const int q = i * (int)a.g.si + m;
     const float *__restrict__ H2 = a.H[A2];
     const float *__restrict__ H1 = a.H[A1];
     float *__restrict__ E = a.E[C];
-    const unsigned short *__restrict__ M = a.mat[C];
-    float h2[kU], h2m[kU], h1[kU], h1m[kU], e[kU];
-    int mi[kU];
-#pragma unroll
-    for (int u = 0; u < kU; u++) {
-        const int i = ib + u, q = i * si + m;
-        if (i >= first && i < last) {
-            h2[u] = H2[q]; h2m[u] = H2[q - s1]; h1[u] = H1[q]; h1m[u] = H1[q - s2]; e[u] = E[q]; mi[u] = M[q];
-        }
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 h2 = z4, h1 = z4, ev = z4, h2m = z4, h1m = z4;
+    uint2 mv = make_uint2(0, 0);
+    if (row) {
+        h2 = ldg4(H2 + q);
+        h1 = ldg4(H1 + q);
+        ev = ld4(E + q);
+        mv = __ldg(reinterpret_cast<const uint2 *>(a.mat[C] + q));
+        if (A1 != 2) h2m = ldg4(H2 + q - stride_of<A1>(a));
+        if (A2 != 2) h1m = ldg4(H1 + q - stride_of<A2>(a));
     }
-    const float cj = a.ec[1][j], ck = a.ec[2][k];
-    const int pj = a.has_pml ? a.pml[1].plane_e[j] : -1, pk = a.has_pml ? a.pml[2].plane_e[k] : -1;
-#pragma unroll
-    for (int u = 0; u < kU; u++) {
-        const int i = ib + u;
-        if (i < first || i >= last) continue;
-        const float c[3] = {a.ec[0][i], cj, ck};
-        const int pp[3] = {a.has_pml ? a.pml[0].plane_e[i] : -1, pj, pk};
-        E[i * si + m] = e_comp<C, P>(a, i, j, k, step, e[u], __fsub_rn(h2[u], h2m[u]), __fsub_rn(h1[u], h1m[u]),
-                                     c[A1], c[A2], pp[A1], pp[A2], mi[u]);
-    }
+    // the previous lane holds the previous four points only if it is in the same run and loaded them
+    const bool pb = __shfl_up_sync(0xffffffffu, row, 1);
+    const bool edge = (threadIdx.x & 31) == 0 || k4 == r.ks || !pb;
+    if (A1 == 2) h2m = prev_k(h2, H2 + q, row && k4 > 0, edge);
+    if (A2 == 2) h1m = prev_k(h1, H1 + q, row && k4 > 0, edge);
+    if (!row) return;
+    e_points<C, P>(a, i, j, k4, E + q, w, h2, h2m, h1, h1m, ev, mv, sv);
 }
 
-// H over node planes [i0, i1) (cem_mt_H and the unfused step)
-__global__ void __launch_bounds__(kBlock, 6) k_update_h(const StepArgs a, int i0, int i1) {
+// H over node planes [i0, i0 + gridDim.y) (cem_mt_H and the unfused step)
+// Resident blocks per SM the update kernels are compiled for (register caps
+// of 51 and 64 per thread at the default 5 and 4: occupancy hides the
+// memory latency; the rarer CPML and Debye paths spill a little)
+#ifndef CB2_H_MINBLOCKS
+#define CB2_H_MINBLOCKS 5
+#endif
+#ifndef CB2_E_MINBLOCKS
+#define CB2_E_MINBLOCKS 4
+#endif
+
+__global__ void __launch_bounds__(kBlock, CB2_H_MINBLOCKS) k_update_h(const StepArgs a, int i0) {
     const int comp = blockIdx.x % 3;
-    const int m = (blockIdx.x / 3) * kBlock + threadIdx.x;
-    if (m >= a.g.plane) return;
-    const int ib = i0 + blockIdx.y * kU, ie = min(ib + kU, i1);
-    const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
-    const int k = m - j * a.g.sj;
-    if (comp == 0) h_march<0>(a, ib, ie, j, k, m);
-    else if (comp == 1) h_march<1>(a, ib, ie, j, k, m);
-    else h_march<2>(a, ib, ie, j, k, m);
+    const RowPos r = row_pos(a.seg_h, a.g.n[1] + 1, blockIdx.x / 3);
+    const int i = i0 + blockIdx.y;
+    if (comp == 0) h_vec<0>(a, i, r);
+    else if (comp == 1) h_vec<1>(a, i, r);
+    else h_vec<2>(a, i, r);
 }
 
-// E over node planes [i0, i1) (cem_mt_E and the unfused step)
+// E over node planes [i0, i0 + gridDim.y) (cem_mt_E and the unfused step)
 template <int P>
-__global__ void __launch_bounds__(kBlock, 3) k_update_e(const StepArgs a, int i0, int i1) {
+__global__ void __launch_bounds__(kBlock, CB2_E_MINBLOCKS) k_update_e(const StepArgs a, int i0) {
     const int comp = blockIdx.x % 3;
-    const int m = (blockIdx.x / 3) * kBlock + threadIdx.x;
-    if (m >= a.g.plane) return;
-    const int ib = i0 + blockIdx.y * kU, ie = min(ib + kU, i1);
-    const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
-    const int k = m - j * a.g.sj;
-    const long long step = *a.dstep;
-    if (comp == 0) e_march<0, P>(a, ib, ie, j, k, m, step);
-    else if (comp == 1) e_march<1, P>(a, ib, ie, j, k, m, step);
-    else e_march<2, P>(a, ib, ie, j, k, m, step);
+    const RowPos r = row_pos(a.seg_e, a.g.n[1] + 1, blockIdx.x / 3);
+    const int i = i0 + blockIdx.y;
+    const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
+    if (comp == 0) e_vec<0, P>(a, i, r, sv);
+    else if (comp == 1) e_vec<1, P>(a, i, r, sv);
+    else e_vec<2, P>(a, i, r, sv);
+}
+
+constexpr unsigned kWaitLimit = 1u << 24;
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// bounded wait; on timeout the error flag is set and the copies in flight
+// get a second bounded wait, so the block never leaves with TMA writes pending
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int *err) {
+    for (unsigned it = 0; it < kWaitLimit; it++)
+        if (mbar_try(bar, parity)) return true;
+    atomicExch(err, 1);
+    for (unsigned it = 0; it < kWaitLimit; it++)
+        if (mbar_try(bar, parity)) break;
+    return false;
 }
 
 // ------------------------------------------------------- fused H + E step
@@ -504,32 +857,6 @@ constexpr int kOffH = kOffE + 9 * kEStride;                    // 2 slots x 3 co
 constexpr int kOffHn = kOffH + 6 * kHStride;                   // H_new of the current plane [3][kHJ][kHK]
 constexpr int kOffBar = (kOffHn + 3 * kHJ * kHK * 4 + 15) / 16 * 16;
 constexpr int kFusedSmem = kOffBar + 5 * 8;
-constexpr unsigned kWaitLimit = 1u << 24;
-
-__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long *bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_expect(unsigned long long *bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parity) {
-    unsigned ok;
-    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
-    return ok != 0;
-}
-// bounded wait; on timeout the error flag is set and the copies in flight
-// get a second bounded wait, so the block never leaves with TMA writes pending
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, int *err) {
-    for (unsigned it = 0; it < kWaitLimit; it++)
-        if (mbar_try(bar, parity)) return true;
-    atomicExch(err, 1);
-    for (unsigned it = 0; it < kWaitLimit; it++)
-        if (mbar_try(bar, parity)) break;
-    return false;
-}
 __device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, int x, int y, int z, unsigned long long *bar) {
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
@@ -627,7 +954,7 @@ __global__ void __launch_bounds__(kFT, 3) k_step_fused(const StepArgs a, const F
     issue_e(ib);
     issue_h(ib);
     issue_e(ib + 1);
-    const long long step = *a.dstep;
+    const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
     float hy_prev = 0.f, hz_prev = 0.f;
     if (ib >= 1) { wait_e(ib - 1); wait_h(ib - 1); }
     wait_e(ib);
@@ -670,7 +997,7 @@ __global__ void __launch_bounds__(kFT, 3) k_step_fused(const StepArgs a, const F
             const int x = tx + 4, o = (ty + 1) * kBX + x;
             float ex = Eb(i % 3, 0)[o], ey = Eb(i % 3, 1)[o], ez = Eb(i % 3, 2)[o];
             const int h = (ty + 1) * kHK + tx + 1;
-            e_point<P>(a, col, pl, i, j, k, step, hx, hy, hz, Hn[2 * kHJ * kHK + h - kHK], Hn[h - kHK],
+            e_point<P>(a, col, pl, i, j, k, sv, hx, hy, hz, Hn[2 * kHJ * kHK + h - kHK], Hn[h - kHK],
                     Hn[kHJ * kHK + h - 1], Hn[h - 1], hy_prev, hz_prev, m0, m1, m2, ex, ey, ez);
             f.En[0][q] = ex; f.En[1][q] = ey; f.En[2][q] = ez;
         }
@@ -681,7 +1008,8 @@ __global__ void __launch_bounds__(kFT, 3) k_step_fused(const StepArgs a, const F
 }
 
 // launchers of the pole-count instantiations
-using EKernel = void (*)(StepArgs, int, int);
+using EKernel = void (*)(StepArgs, int);
+using HKernel = void (*)(StepArgs, int);
 using FKernel = void (*)(StepArgs, FusedArgs, TmaMaps);
 #define CB2_POLES(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
 #define CB2_EK(p) k_update_e<p>,
@@ -699,18 +1027,36 @@ const FKernel kFKernels[] = {CB2_POLES(CB2_FK)};
 __global__ void __launch_bounds__(kBlock) k_sibc(const SibcArgs a) {
     const int e = blockIdx.x * kBlock + threadIdx.x;
     if (e >= a.ns) return;
+    // every load first: face tables (16-byte vectors), the convolution
+    // states, then the H values of the faces
+    const float4 w4 = __ldg(a.hw + e);
+    const uint4 i4 = __ldg(a.hidx + e);
+    const uchar4 c4 = __ldg(a.hcomp + e);
+    float y[kSibcTerms];
+#pragma unroll
+    for (int k = 0; k < kSibcTerms; k++)
+        if (k < a.K) y[k] = a.y[(long long)k * a.ns + e];
+    const float w[4] = {w4.x, w4.y, w4.z, w4.w};
+    const unsigned hi[4] = {i4.x, i4.y, i4.z, i4.w};
+    const int hc[4] = {c4.x, c4.y, c4.z, c4.w};
+    float h[4];
+#pragma unroll
+    for (int f = 0; f < 4; f++) h[f] = w[f] != 0.f ? a.H[hc[f]][hi[f]] : 0.f;
     float J = 0.f;
-    for (int f = 0; f < 4; f++) {
-        const float w = a.hw[4 * e + f];
-        if (w != 0.f) J += w * a.H[a.hcomp[4 * e + f]][a.hidx[4 * e + f]];
-    }
+#pragma unroll
+    for (int f = 0; f < 4; f++)
+        if (w[f] != 0.f) J += w[f] * h[f];
     float E = 0.f;
-    for (int k = 0; k < a.K; k++) {
-        float y = a.y[(long long)k * a.ns + e];
-        y += a.ome[k] * (J - y);
-        a.y[(long long)k * a.ns + e] = y;
-        E += a.c[k] * (J - y);
+#pragma unroll
+    for (int k = 0; k < kSibcTerms; k++) {
+        if (k < a.K) {
+            y[k] += a.ome[k] * (J - y[k]);
+            E += a.c[k] * (J - y[k]);
+        }
     }
+#pragma unroll
+    for (int k = 0; k < kSibcTerms; k++)
+        if (k < a.K) a.y[(long long)k * a.ns + e] = y[k];
     a.E[a.ecomp[e]][a.eidx[e]] = E;
 }
 
@@ -721,17 +1067,36 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// FP32 source values the E update of step n adds: the lumped Gaussian Vs and
+// the differentiated modal Gaussian Vm at the H time (n + 1/2) dt (reference
+// sim.c:834-838,900-909, modeport.c:124-135). Computed once per step.
+__device__ __forceinline__ void source_values(const PostArgs &a, long long n, float *out) {
+    const double tH = ((double)n + 0.5) * a.dt;
+    out[0] = a.src_port >= 0 ? (float)gauss(tH, a.src_amp, a.src_t0, a.src_tau) : 0.f;
+    out[1] = a.msrc_on ? (float)dgauss(tH, a.m_t0, a.m_tau) : 0.f;
+}
+
 // Line integrals of every input slot (warp per slot), then port V/I and the
 // source value, written as one row of the sample ring. With advance = 0 it
 // only refreshes the port voltages before the E update (vold).
-__global__ void __launch_bounds__(kBlock) k_post(const PostArgs a) {
+__global__ void __launch_bounds__(kPostThreads) k_post(const PostArgs a) {
     __shared__ double res[kMaxSlots];
+    __shared__ double val[kPostStage];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int first = a.advance ? 0 : a.nip, last = a.advance ? a.nin : a.nip + a.nport;
-    for (int s = first + warp; s < last; s += kBlock / 32) {
+    // all edge products at once (their loads overlap), then per-slot sums in
+    // a fixed order: lane-strided partial sums and a warp reduction
+    const int e0 = a.off[first], e1 = a.off[last];
+    const bool staged = e1 - e0 <= kPostStage;
+    if (staged) {
+        for (int e = e0 + threadIdx.x; e < e1; e += kPostThreads)
+            val[e - e0] = (double)a.F[a.ecomp[e]][a.eidx[e]] * a.ew[e];
+        __syncthreads();
+    }
+    for (int s = first + warp; s < last; s += kPostThreads / 32) {
         double v = 0;
         for (int e = a.off[s] + lane; e < a.off[s + 1]; e += 32)
-            v += (double)a.F[a.ecomp[e]][a.eidx[e]] * a.ew[e];
+            v += staged ? val[e - e0] : (double)a.F[a.ecomp[e]][a.eidx[e]] * a.ew[e];
         v = warp_sum(v);
         if (lane == 0) res[s] = v;
     }
@@ -744,8 +1109,8 @@ __global__ void __launch_bounds__(kBlock) k_post(const PostArgs a) {
     double *row = a.ring + (long long)(step % kRing) * a.nslot;
     const double tH = ((double)step + 0.5) * a.dt;
     const double vs = a.src_port >= 0 ? gauss(tH, a.src_amp, a.src_t0, a.src_tau) : 0.0;
-    for (int s = threadIdx.x; s < a.nip; s += kBlock) row[s] = res[s];
-    for (int p = threadIdx.x; p < a.nport; p += kBlock) {
+    for (int s = threadIdx.x; s < a.nip; s += kPostThreads) row[s] = res[s];
+    for (int p = threadIdx.x; p < a.nport; p += kPostThreads) {
         const double vnew = res[a.nip + p];
         const double V = 0.5 * (vnew + a.vold[p]);
         a.vold[p] = vnew;
@@ -758,10 +1123,16 @@ __global__ void __launch_bounds__(kBlock) k_post(const PostArgs a) {
         if (a.msrc_on) src += dgauss(tH, a.m_t0, a.m_tau);
         row[a.nip + 2 * a.nport] = src;
     }
-    for (int s = threadIdx.x; s < a.nvp; s += kBlock) row[a.nip + 2 * a.nport + 1 + s] = res[a.nip + a.nport + s];
+    for (int s = threadIdx.x; s < a.nvp; s += kPostThreads) row[a.nip + 2 * a.nport + 1 + s] = res[a.nip + a.nport + s];
     __syncthreads();
-    if (threadIdx.x == 0) *a.dstep = step + 1;
+    if (threadIdx.x == 0) {
+        *a.dstep = step + 1;
+        source_values(a, step + 1, a.srcv);
+    }
 }
+
+// source values for the step count held on the device (after it was set from the host)
+__global__ void k_source_values(const PostArgs a) { source_values(a, *a.dstep, a.srcv); }
 
 // acc[slot][f] += (sample * dt) e^{-j w t} for each pending row in step order,
 // t the slot's sampling time: (n + 1/2) dt for H-time slots, (n + 1) dt for
@@ -802,9 +1173,9 @@ struct EnergyArgs {
 };
 
 // W = 1/2 sum eps E^2 dV + 1/2 sum mu0 H^2 dV with eps = dt/cb (reference sim.c:970-994)
-__global__ void __launch_bounds__(kBlock) k_energy(const EnergyArgs a) {
+__global__ void __launch_bounds__(kBlock) k_energy(const EnergyArgs a, int i0) {
     __shared__ double red[kBlock / 32];
-    const int i = blockIdx.y;
+    const int i = i0 + blockIdx.y;
     const int m = blockIdx.x * kBlock + threadIdx.x;
     double acc = 0;
     const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
@@ -835,7 +1206,7 @@ __global__ void __launch_bounds__(kBlock) k_energy(const EnergyArgs a) {
     if (threadIdx.x == 0) {
         double s = 0;
         for (int w = 0; w < kBlock / 32; w++) s += red[w];
-        a.partial[(long long)blockIdx.y * gridDim.x + blockIdx.x] = s;
+        a.partial[(long long)i * gridDim.x + blockIdx.x] = s;
     }
 }
 
@@ -882,8 +1253,13 @@ struct Device {
     DevBuf<int> plane_h[3], plane_e[3];
     DevBuf<float> bm1_h[3], cid_h[3], bm1_e[3], cid_e[3];
     DevBuf<float> psiH[2][3][2], psiE[3][2];
-    size_t psi_len_h[3][2] = {}, psi_len_e[3][2] = {};
+    size_t psi_len_h[3][2] = {}, psi_len_e[3][2] = {};   // reference (host) lengths
+    size_t psi_dev_h[3][2] = {}, psi_dev_e[3][2] = {};   // device lengths
     int zplanes = 0;   // planes of the z CPML slabs (same count for cells and nodes)
+    int pml_planes[3] = {0, 0, 0};
+    DevBuf<int> zoff_h, zoff_e;
+    int zw_h = 0, zw_e = 0;
+    std::vector<int> zoff_host[2];   // H, E
     DevBuf<unsigned short> mat[3];
     DevBuf<float> tab[3];
     DevBuf<float4> tab4[3];
@@ -892,18 +1268,23 @@ struct Device {
     int ntab[3] = {0, 0, 0};
     DevBuf<float> J[3];
     int jbox[3][6] = {};
+    KSegs seg_h{}, seg_e{};
     DevBuf<float> wsrc[2];
     // SIBC
-    DevBuf<int> sb_ecomp, sb_hcomp;
-    DevBuf<long long> sb_eidx, sb_hidx;
-    DevBuf<float> sb_hw, sb_y;
+    DevBuf<unsigned char> sb_ecomp;
+    DevBuf<unsigned> sb_eidx;
+    DevBuf<uchar4> sb_hcomp;
+    DevBuf<uint4> sb_hidx;
+    DevBuf<float4> sb_hw;
+    DevBuf<float> sb_y;
     // probes
     int nip = 0, nport = 0, nvp = 0, nin = 0, nslot = 0;
     DevBuf<int> off;
     DevBuf<unsigned char> ecomp;
-    DevBuf<long long> eidx;
+    DevBuf<unsigned> eidx;
     DevBuf<double> ew, R, vold, ring, acc, omega;
     DevBuf<long long> dstep;
+    DevBuf<float> srcv;
     // energy
     DevBuf<double> d64[3], dd64[3], partial, scalar;
     // pending DFT rows [ring_first, ring_first + ring_count)
@@ -1008,10 +1389,13 @@ bool dev_upload(cem_sim *s, DevBuf<T> &b, const std::vector<T> &v) {
     return h2d(s, b.p, v.data(), v.size() * sizeof(T));
 }
 
+// length of a per-axis array of n cells / n+1 nodes, padded past round_up(n+1, 4)
+size_t axis_padded(int n) { return (size_t)(n + 1 + 3) / 4 * 4 + 4; }
+
 // reference index q -> padded device index
-long long dev_index(const cem_sim *s, const Device &D, size_t q) {
+unsigned dev_index(const cem_sim *s, const Device &D, size_t q) {
     const size_t i = q / s->si, r = q % s->si, j = r / s->sj, k = r % s->sj;
-    return (long long)(i * D.g.si + j * D.g.sj + k);
+    return (unsigned)(i * D.g.si + j * D.g.sj + k);   // < 2^31 (checked at device creation)
 }
 
 std::vector<float> to_f32(const std::vector<double> &v) {
@@ -1065,6 +1449,16 @@ bool build_tables(cem_sim *s, Device &D) {
     }
     std::vector<std::unordered_map<size_t, int>> disp(3);
     for (int e = 0; e < s->ndisp; e++) disp[s->d_comp[e]][s->d_idx[e]] = e;
+    // mode-source weights of Ey, Ez on the source plane (reference index j*(nz+1)+k)
+    int msrc_i = -1;
+    std::vector<float> wsrc[2];
+    if (s->msrc >= 0) {
+        const ModePort &mp = s->mport[s->msrc];
+        msrc_i = mp.def.i_src;
+        for (int c = 0; c < 2; c++) wsrc[c].assign((size_t)(s->n[1] + 1) * (s->n[2] + 1), 0.f);
+        for (size_t e = 0; e < mp.src_idx.size(); e++)
+            wsrc[mp.src_comp[e] - 1][mp.src_idx[e] % s->si] += (float)mp.src_w[e];
+    }
     const int *n = s->n;
     for (int c = 0; c < 3; c++) {
         TableBuilder tb(nfields);
@@ -1086,6 +1480,7 @@ bool build_tables(cem_sim *s, Device &D) {
                     unsigned char flag = 0;
                     auto it = src[c].find(q);
                     if (it != src[c].end()) { row[2] = (float)it->second; flag |= kFlagSrc; }
+                    if (c > 0 && i == msrc_i && wsrc[c - 1][(size_t)j * (n[2] + 1) + k] != 0.f) flag |= kFlagMode;
                     auto dt_ = disp[c].find(q);
                     if (dt_ != disp[c].end()) {
                         flag |= kFlagDisp;
@@ -1123,6 +1518,10 @@ bool build_tables(cem_sim *s, Device &D) {
             for (int a = 0; a < 3; a++) {
                 D.jbox[c][a] = box_lo[a];
                 D.jbox[c][3 + a] = box_hi[a] - box_lo[a] + 1;
+                if (a == 2) {   // k extent aligned to 4 points: the currents of four points move as a float4
+                    D.jbox[c][2] = box_lo[2] / 4 * 4;
+                    D.jbox[c][5] = (box_hi[2] + 1 - D.jbox[c][2] + 3) / 4 * 4;
+                }
             }
             const size_t vol = (size_t)D.jbox[c][3] * D.jbox[c][4] * D.jbox[c][5];
             if (!dev_alloc(s, D.J[c], vol * P)) return false;
@@ -1134,8 +1533,9 @@ bool build_tables(cem_sim *s, Device &D) {
 bool build_pml(cem_sim *s, Device &D) {
     for (int a = 0; a < 3; a++) {
         const int n = s->n[a];
-        std::vector<int> ph(n, -1), pe(n + 1, -1);
-        std::vector<float> bh(n, 0.f), chh(n, 0.f), be(n + 1, 0.f), cee(n + 1, 0.f);
+        const size_t np = axis_padded(n);   // padded so four consecutive k load as one int4
+        std::vector<int> ph(np, -1), pe(np, -1);
+        std::vector<float> bh(np, 0.f), chh(np, 0.f), be(np, 0.f), cee(np, 0.f);
         int r[2][2];
         pml_ranges(s, a, 0, r);
         const int lo_h = r[0][1] >= r[0][0] ? r[0][1] - r[0][0] + 1 : 0;
@@ -1161,20 +1561,55 @@ bool build_pml(cem_sim *s, Device &D) {
             !dev_upload(s, D.cid_h[a], chh) || !dev_upload(s, D.bm1_e[a], be) || !dev_upload(s, D.cid_e[a], cee))
             return false;
     }
-    {
+    for (int a = 0; a < 3; a++) {
         int r[2][2], planes = 0;
-        pml_ranges(s, 2, 0, r);
+        pml_ranges(s, a, 0, r);
         for (int sd = 0; sd < 2; sd++) planes += r[sd][1] >= r[sd][0] ? r[sd][1] - r[sd][0] + 1 : 0;
-        D.zplanes = planes;
+        D.pml_planes[a] = s->has_pml ? planes : 0;
     }
+    D.zplanes = D.pml_planes[2];
+    // z windows: whole 4-point groups covering the slabs of each (i, j) column
+    const int nzp = (int)axis_padded(s->n[2]);
+    for (int is_e = 0; is_e < 2; is_e++) {
+        std::vector<int> &zo = D.zoff_host[is_e];
+        zo.assign(nzp, -1);
+        int width = 0;
+        if (s->has_pml) {
+            int r[2][2];
+            pml_ranges(s, 2, is_e, r);
+            std::vector<std::pair<int, int>> win;
+            for (int sd = 0; sd < 2; sd++)
+                if (r[sd][1] >= r[sd][0]) win.push_back({r[sd][0] / 4 * 4, (r[sd][1] + 1 + 3) / 4 * 4});
+            if (win.size() == 2 && win[1].first < win[0].second) {   // overlapping windows merge
+                win[0].second = std::max(win[0].second, win[1].second);
+                win.pop_back();
+            }
+            for (const auto &wd : win) {
+                for (int k = wd.first; k < wd.second; k++) zo[k] = width + (k - wd.first);
+                width += wd.second - wd.first;
+            }
+        }
+        (is_e ? D.zw_e : D.zw_h) = width;
+        if (!dev_upload(s, is_e ? D.zoff_e : D.zoff_h, zo)) return false;
+    }
+    const size_t nx1 = s->n[0] + 1, ny1 = s->n[1] + 1;
     for (int c = 0; c < 3; c++)
         for (int w = 0; w < 2; w++) {
             D.psi_len_h[c][w] = psi_len(s, 0, c, w);
             D.psi_len_e[c][w] = psi_len(s, 1, c, w);
-            if (!dev_alloc(s, D.psiH[0][c][w], D.psi_len_h[c][w] + 1) ||
-                !dev_alloc(s, D.psiH[1][c][w], D.psi_len_h[c][w] + 1) || !dev_alloc(s, D.psiE[c][w], D.psi_len_e[c][w] + 1))
+            const int ax = (c + w + 1) % 3;
+            size_t nh = 0, ne = 0;
+            if (D.psi_len_h[c][w]) {
+                if (ax == 0) nh = ne = (size_t)D.pml_planes[0] * D.g.si;
+                else if (ax == 1) nh = ne = nx1 * D.pml_planes[1] * D.g.sj;
+                else { nh = nx1 * ny1 * D.zw_h; ne = nx1 * ny1 * D.zw_e; }
+            }
+            D.psi_dev_h[c][w] = nh;
+            D.psi_dev_e[c][w] = ne;
+            if (!dev_alloc(s, D.psiH[0][c][w], nh + 4) || !dev_alloc(s, D.psiH[1][c][w], nh + 4) ||
+                !dev_alloc(s, D.psiE[c][w], ne + 4))
                 return false;
-            // unused slots of the compact layout are read by nobody but must stay finite
+            // padding slots of the layout are read and written back unchanged: they must stay finite
             if (!zero_dev(s, D.psiH[1][c][w].p, D.psiH[1][c][w].n * 4)) return false;
         }
     return true;
@@ -1188,7 +1623,7 @@ bool build_probes(cem_sim *s, Device &D) {
     D.nslot = D.nip + 2 * D.nport + 1 + D.nvp;
     std::vector<int> off{0};
     std::vector<unsigned char> comp;
-    std::vector<long long> idx;
+    std::vector<unsigned> idx;
     std::vector<double> w;
     for (const CurrentProbe &p : s->ip) {
         for (size_t e = 0; e < p.idx.size(); e++) {
@@ -1216,26 +1651,88 @@ bool build_probes(cem_sim *s, Device &D) {
         !dev_upload(s, D.ew, w) || !dev_upload(s, D.R, R) || !dev_upload(s, D.omega, omega))
         return false;
     if (!dev_alloc(s, D.vold, std::max(D.nport, 1)) || !dev_alloc(s, D.ring, (size_t)kRing * D.nslot) ||
-        !dev_alloc(s, D.acc, (size_t)D.nslot * 2 * s->nf) || !dev_alloc(s, D.dstep, 1))
+        !dev_alloc(s, D.acc, (size_t)D.nslot * 2 * s->nf) || !dev_alloc(s, D.dstep, 1) ||
+        !dev_alloc(s, D.srcv, 2))
         return false;
     return true;
 }
 
 bool build_sibc(cem_sim *s, Device &D) {
     if (!s->nsb) return true;
-    std::vector<int> ecomp(s->sb_comp), hcomp(s->sb_hc);
-    std::vector<long long> eidx(s->nsb), hidx(4 * (size_t)s->nsb);
-    std::vector<float> hw(4 * (size_t)s->nsb);
-    for (int e = 0; e < s->nsb; e++) {
+    const size_t ns = (size_t)s->nsb;
+    std::vector<unsigned char> ecomp(ns);
+    std::vector<unsigned> eidx(ns);
+    std::vector<uchar4> hcomp(ns);
+    std::vector<uint4> hidx(ns);
+    std::vector<float4> hw(ns);
+    for (size_t e = 0; e < ns; e++) {
+        ecomp[e] = (unsigned char)s->sb_comp[e];
         eidx[e] = dev_index(s, D, s->sb_idx[e]);
-        for (int f = 0; f < 4; f++) {
-            hidx[4 * e + f] = f < s->sb_nf[e] ? dev_index(s, D, s->sb_hi[4 * e + f]) : 0;
-            hw[4 * e + f] = f < s->sb_nf[e] ? (float)s->sb_sg[4 * e + f] : 0.f;
+        unsigned char c[4] = {0, 0, 0, 0};
+        unsigned q[4] = {0, 0, 0, 0};
+        float w[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int f = 0; f < 4 && f < s->sb_nf[e]; f++) {
+            c[f] = (unsigned char)s->sb_hc[4 * e + f];
+            q[f] = dev_index(s, D, s->sb_hi[4 * e + f]);
+            w[f] = (float)s->sb_sg[4 * e + f];
         }
+        hcomp[e] = make_uchar4(c[0], c[1], c[2], c[3]);
+        hidx[e] = make_uint4(q[0], q[1], q[2], q[3]);
+        hw[e] = make_float4(w[0], w[1], w[2], w[3]);
     }
     return dev_upload(s, D.sb_ecomp, ecomp) && dev_upload(s, D.sb_hcomp, hcomp) && dev_upload(s, D.sb_eidx, eidx) &&
            dev_upload(s, D.sb_hidx, hidx) && dev_upload(s, D.sb_hw, hw) &&
-           dev_alloc(s, D.sb_y, (size_t)s->nsb * s->sibc_npole);
+           dev_alloc(s, D.sb_y, ns * s->sibc_npole);
+}
+
+// k segments of the H and E kernels: cuts at the z CPML slabs (cells for H,
+// nodes for E) and, for E, at the Debye boxes, each rounded down to a
+// multiple of 4.
+bool make_segments(cem_sim *s, const std::vector<int> &cuts, KSegs &sg) {
+    const Geom &g = s->dev->g;
+    std::vector<int> b{0, g.sj};
+    for (int c : cuts)
+        if (c > 0 && c < g.sj) b.push_back(c / 4 * 4);
+    std::sort(b.begin(), b.end());
+    b.erase(std::unique(b.begin(), b.end()), b.end());
+    if ((int)b.size() - 1 > kMaxSegs) {
+        set_error("too many k segments");
+        return false;
+    }
+    sg = KSegs{};
+    sg.n = (int)b.size() - 1;
+    const long long rows = s->n[1] + 1;
+    int blocks = 0;
+    for (int q = 0; q < sg.n; q++) {
+        const long long nk4 = (b[q + 1] - b[q]) / 4;
+        if (rows * nk4 * nk4 >= (1ll << 40) || rows * nk4 >= (1ll << 31)) {
+            set_error("grid too large for the k-segment layout");
+            return false;
+        }
+        sg.k[q] = b[q];
+        sg.blk[q] = blocks;
+        sg.magic[q] = ((1ull << 40) + (unsigned long long)nk4 - 1) / (unsigned long long)nk4;
+        blocks += (int)((rows * nk4 + kBlock - 1) / kBlock);
+    }
+    sg.k[sg.n] = b[sg.n];
+    sg.blk[sg.n] = blocks;
+    return true;
+}
+
+bool build_segments(cem_sim *s, Device &D) {
+    std::vector<int> ch, ce;
+    if (s->has_pml) {
+        int r[2][2];
+        pml_ranges(s, 2, 0, r);
+        for (int sd = 0; sd < 2; sd++)
+            if (r[sd][1] >= r[sd][0]) { ch.push_back(r[sd][0]); ch.push_back(r[sd][1] + 1); }
+        pml_ranges(s, 2, 1, r);
+        for (int sd = 0; sd < 2; sd++)
+            if (r[sd][1] >= r[sd][0]) { ce.push_back(r[sd][0]); ce.push_back(r[sd][1] + 1); }
+    }
+    for (int c = 0; c < 3; c++)
+        if (D.jbox[c][5] > 0) { ce.push_back(D.jbox[c][2]); ce.push_back(D.jbox[c][2] + D.jbox[c][5]); }
+    return make_segments(s, ch, D.seg_h) && make_segments(s, ce, D.seg_e);
 }
 
 bool build_sources(cem_sim *s, Device &D) {
@@ -1257,13 +1754,15 @@ void fill_args_for(cem_sim *s, Device &D, int cur) {
     StepArgs &a = D.sa[cur];
     a = StepArgs{};
     a.g = D.g;
+    a.seg_h = D.seg_h;
+    a.seg_e = D.seg_e;
     for (int c = 0; c < 3; c++) {
         a.E[c] = D.E[cur][c].p;
         a.H[c] = D.H[cur][c].p;
         a.hc[c] = D.hc[c].p;
         a.ec[c] = D.ec[c].p;
         a.pml[c] = PmlAxis{D.plane_h[c].p, D.plane_e[c].p, D.bm1_h[c].p, D.cid_h[c].p, D.bm1_e[c].p, D.cid_e[c].p,
-                           (int)pml_per(s, c), D.zplanes};
+                           D.pml_planes[c], D.zoff_h.p, D.zoff_e.p, D.zw_h, D.zw_e};
         for (int w = 0; w < 2; w++) {
             a.psiH[c][w] = D.psiH[cur][c][w].p;
             a.psiE[c][w] = D.psiE[c][w].p;
@@ -1298,6 +1797,7 @@ void fill_args_for(cem_sim *s, Device &D, int cur) {
         a.wsrc[1] = D.wsrc[1].p;
     }
     a.dstep = D.dstep.p;
+    a.srcv = D.srcv.p;
 
     FusedArgs &f = D.fa[cur];
     f.error = D.error.p;
@@ -1332,6 +1832,7 @@ void fill_args_for(cem_sim *s, Device &D, int cur) {
     p.ring = D.ring.p;
     for (int c = 0; c < 3; c++) { p.F[c] = D.E[cur][c].p; p.F[3 + c] = D.H[cur][c].p; }
     p.dstep = D.dstep.p;
+    p.srcv = D.srcv.p;
 
     EnergyArgs &e = D.ea[cur];
     e.g = D.g;
@@ -1405,7 +1906,7 @@ bool create_device_impl(cem_sim *s) {
     CB2_CHECK(s, cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking));
     Geom &g = D.g;
     for (int a = 0; a < 3; a++) g.n[a] = s->n[a];
-    g.sj = (s->n[2] + 1 + 3) / 4 * 4;
+    g.sj = (s->n[2] + 1 + 7) / 8 * 8;
     g.si = (long long)(s->n[1] + 1) * g.sj;
     g.plane = (int)g.si;
     g.sj_magic = ((1ull << 40) + g.sj - 1) / g.sj;
@@ -1419,12 +1920,15 @@ bool create_device_impl(cem_sim *s) {
             if (!dev_alloc(s, D.E[b][c], D.Np) || !dev_alloc(s, D.H[b][c], D.Np) ||
                 !zero_dev(s, D.E[b][c].p, D.Np * 4) || !zero_dev(s, D.H[b][c].p, D.Np * 4))
                 return false;
-        std::vector<double> hc(s->n[c]);
+        // per-axis coefficients, zero-padded so four consecutive k load as one float4
+        std::vector<double> hc(axis_padded(s->n[c]), 0.0), ec(axis_padded(s->n[c]), 0.0);
         for (int i = 0; i < s->n[c]; i++) hc[i] = s->dt / CEM_MU0 * s->idh[c][i];
-        if (!dev_upload(s, D.hc[c], to_f32(hc)) || !dev_upload(s, D.ec[c], to_f32(s->ide[c]))) return false;
+        for (int i = 0; i <= s->n[c]; i++) ec[i] = s->ide[c][i];
+        if (!dev_upload(s, D.hc[c], to_f32(hc)) || !dev_upload(s, D.ec[c], to_f32(ec))) return false;
         if (!dev_upload(s, D.d64[c], s->d[c]) || !dev_upload(s, D.dd64[c], s->dd[c])) return false;
     }
-    if (!build_pml(s, D) || !build_tables(s, D) || !build_probes(s, D) || !build_sibc(s, D) || !build_sources(s, D))
+    if (!build_pml(s, D) || !build_tables(s, D) || !build_probes(s, D) || !build_sibc(s, D) || !build_sources(s, D) ||
+        !build_segments(s, D))
         return false;
     for (int b = 0; b < 2; b++)
         for (int c = 0; c < 3; c++)
@@ -1469,23 +1973,6 @@ bool download_field(cem_sim *s, std::vector<double> &dst, const float *src) {
     return true;
 }
 
-bool upload_f32(cem_sim *s, float *dst, const std::vector<double> &src, size_t n) {
-    if (!n) return true;
-    std::vector<float> tmp(n);
-    for (size_t i = 0; i < n; i++) tmp[i] = (float)src[i];
-    return h2d(s, dst, tmp.data(), n * sizeof(float));
-}
-
-bool download_f32(cem_sim *s, std::vector<double> &dst, const float *src, size_t n) {
-    dst.resize(n);
-    if (!n) return true;
-    std::vector<float> tmp(n);
-    if (!d2h(s, tmp.data(), src, n * sizeof(float))) return false;
-    for (size_t i = 0; i < n; i++) dst[i] = tmp[i];
-    return true;
-}
-
-
 // pack the host DFT accumulators in slot order: I probes, port V/I, source, V probes
 std::vector<double *> dft_slots(cem_sim *s) {
     std::vector<double *> v;
@@ -1510,25 +1997,53 @@ bool flush_dft(cem_sim *s) {
     return true;
 }
 
-// reference compact layout <-> device layout (z-axis slabs transposed)
-bool psi_is_z(int c, int w) { return (c + w + 1) % 3 == 2; }
-
-std::vector<double> psi_to_device(const cem_sim *s, const Device &D, int c, int w, const std::vector<double> &v) {
-    if (!psi_is_z(c, w) || v.empty()) return v;
-    const size_t per = pml_per(s, 2), P = (size_t)D.zplanes;
-    std::vector<double> o(v.size());
-    for (size_t pl = 0; pl < P; pl++)
-        for (size_t x = 0; x < per; x++) o[x * P + pl] = v[pl * per + x];
-    return o;
+// Reference compact index -> device index of every auxiliary of array
+// (c, w) (derivative axis (c + w + 1) % 3), E (nodes) or H (cells).
+template <class F>
+void psi_map(const cem_sim *s, const Device &D, bool is_e, int c, int w, F visit) {
+    const int ax = (c + w + 1) % 3, nx = s->n[0], ny = s->n[1], nz = s->n[2];
+    const size_t per = pml_per(s, ax);
+    const int planes = D.pml_planes[ax];
+    for (int pl = 0; pl < planes; pl++) {
+        if (ax == 0) {
+            for (int j = 0; j <= ny; j++)
+                for (int k = 0; k <= nz; k++)
+                    visit(pl * per + (size_t)j * (nz + 1) + k, (size_t)pl * D.g.si + (size_t)j * D.g.sj + k);
+        } else if (ax == 1) {
+            for (int i = 0; i <= nx; i++)
+                for (int k = 0; k <= nz; k++)
+                    visit(pl * per + (size_t)i * (nz + 1) + k, ((size_t)i * planes + pl) * D.g.sj + k);
+        } else {
+            int r[2][2];
+            pml_ranges(s, 2, is_e, r);
+            const int nlo = r[0][1] >= r[0][0] ? r[0][1] - r[0][0] + 1 : 0;
+            const int kz = pl < nlo ? r[0][0] + pl : r[1][0] + (pl - nlo);
+            const size_t zw = is_e ? D.zw_e : D.zw_h, zo = D.zoff_host[is_e][kz];
+            for (int i = 0; i <= nx; i++)
+                for (int j = 0; j <= ny; j++)
+                    visit(pl * per + (size_t)i * (ny + 1) + j, ((size_t)i * (ny + 1) + j) * zw + zo);
+        }
+    }
 }
 
-void psi_to_host(const cem_sim *s, const Device &D, int c, int w, std::vector<double> &v) {
-    if (!psi_is_z(c, w) || v.empty()) return;
-    const size_t per = pml_per(s, 2), P = (size_t)D.zplanes;
-    std::vector<double> o(v.size());
-    for (size_t pl = 0; pl < P; pl++)
-        for (size_t x = 0; x < per; x++) o[pl * per + x] = v[x * P + pl];
-    v.swap(o);
+bool psi_upload(cem_sim *s, bool is_e, int c, int w, const std::vector<double> &v, float *dst) {
+    const Device &D = *s->dev;
+    const size_t n = is_e ? D.psi_dev_e[c][w] : D.psi_dev_h[c][w];
+    if (!n) return true;
+    std::vector<float> o(n + 4, 0.f);
+    if (!v.empty()) psi_map(s, D, is_e, c, w, [&](size_t r, size_t d) { o[d] = (float)v[r]; });
+    return h2d(s, dst, o.data(), o.size() * sizeof(float));
+}
+
+bool psi_download(cem_sim *s, bool is_e, int c, int w, std::vector<double> &v, const float *src) {
+    const Device &D = *s->dev;
+    const size_t n = is_e ? D.psi_dev_e[c][w] : D.psi_dev_h[c][w];
+    v.assign(is_e ? D.psi_len_e[c][w] : D.psi_len_h[c][w], 0.0);
+    if (!n) return true;
+    std::vector<float> o(n);
+    if (!d2h(s, o.data(), src, n * sizeof(float))) return false;
+    psi_map(s, D, is_e, c, w, [&](size_t r, size_t d) { v[r] = o[d]; });
+    return true;
 }
 
 bool upload_group(cem_sim *s, unsigned g, bool from_host) {
@@ -1548,8 +2063,8 @@ bool upload_group(cem_sim *s, unsigned g, bool from_host) {
         for (int c = 0; c < 3; c++)
             for (int w = 0; w < 2; w++) {
                 if (from_host) {
-                    if (!upload_f32(s, D.psiE[c][w].p, psi_to_device(s, D, c, w, s->psiE[c][w]), D.psi_len_e[c][w]) ||
-                        !upload_f32(s, D.psiH[D.cur][c][w].p, psi_to_device(s, D, c, w, s->psiH[c][w]), D.psi_len_h[c][w]))
+                    if (!psi_upload(s, true, c, w, s->psiE[c][w], D.psiE[c][w].p) ||
+                        !psi_upload(s, false, c, w, s->psiH[c][w], D.psiH[D.cur][c][w].p))
                         return false;
                 } else if (!zero_dev(s, D.psiE[c][w].p, D.psiE[c][w].n * 4) ||
                            !zero_dev(s, D.psiH[D.cur][c][w].p, D.psiH[D.cur][c][w].n * 4)) {
@@ -1608,13 +2123,9 @@ bool download_group(cem_sim *s, unsigned g) {
     if (g & kGroupPsi)
         for (int c = 0; c < 3; c++)
             for (int w = 0; w < 2; w++)
-                if (!download_f32(s, s->psiE[c][w], D.psiE[c][w].p, D.psi_len_e[c][w]) ||
-                    !download_f32(s, s->psiH[c][w], D.psiH[D.cur][c][w].p, D.psi_len_h[c][w]))
+                if (!psi_download(s, true, c, w, s->psiE[c][w], D.psiE[c][w].p) ||
+                    !psi_download(s, false, c, w, s->psiH[c][w], D.psiH[D.cur][c][w].p))
                     return false;
-                else {
-                    psi_to_host(s, D, c, w, s->psiE[c][w]);
-                    psi_to_host(s, D, c, w, s->psiH[c][w]);
-                }
     if (g & kGroupDebye) {
         s->d_J.assign((size_t)s->npole * s->ndisp, 0.0);
         if (s->d_Eold.size() != (size_t)s->ndisp) s->d_Eold.assign(s->ndisp, 0.0);
@@ -1667,11 +2178,13 @@ bool begin_device_op(cem_sim *s) {
     if (D.ring_count == 0) D.ring_first = s->step;
     long long st = s->step;
     CB2_CHECK(s, cudaMemcpyAsync(D.dstep.p, &st, sizeof st, cudaMemcpyHostToDevice, D.stream));
+    k_source_values<<<1, 1, 0, D.stream>>>(D.pa[D.cur]);
+    CB2_CHECK(s, cudaGetLastError());
     CB2_CHECK(s, cudaStreamSynchronize(D.stream));
     if (!D.vold_valid && D.nport) {
         PostArgs pa = D.pa[D.cur];
         pa.advance = 0;
-        k_post<<<1, kBlock, 0, D.stream>>>(pa);
+        k_post<<<1, kPostThreads, 0, D.stream>>>(pa);
         CB2_CHECK(s, cudaGetLastError());
         D.vold_valid = true;
     }
@@ -1713,7 +2226,7 @@ bool launch_fused_step(cem_sim *s) {
     PostArgs pa = D.pa[D.cur];
     pa.advance = 1;
     t_begin(3);
-    k_post<<<1, kBlock, 0, D.stream>>>(pa);
+    k_post<<<1, kPostThreads, 0, D.stream>>>(pa);
     t_end();
     D.ring_count++;
     s->step++;
@@ -1726,25 +2239,28 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
     if (phase_mask == (1 | 4 | 8) && i0 <= 0 && i1 > s->n[0] && D.use_fused) return launch_fused_step(s);
     const int nx = s->n[0];
     const dim3 blk(kBlock);
-    const int gx = (D.g.plane + kBlock - 1) / kBlock;
+    const int gxh = D.sa[D.cur].seg_h.blk[D.sa[D.cur].seg_h.n], gxe = D.sa[D.cur].seg_e.blk[D.sa[D.cur].seg_e.n];
     if (phase_mask & 1) {   // H over node planes [i0, i1) within [0, nx]
         const int a = std::max(0, i0), b = std::min(nx + 1, i1);
         if (b > a) {
             t_begin(0);
-            k_update_h<<<dim3(3 * gx, (b - a + kU - 1) / kU), blk, 0, D.stream>>>(D.sa[D.cur], a, b);
+            for (int c0 = a; c0 < b; c0 += kMaxGridY)
+                k_update_h<<<dim3(3 * gxh, std::min(kMaxGridY, b - c0)), blk, 0, D.stream>>>(D.sa[D.cur], c0);
             t_end();
         }
     }
     if (phase_mask & 2) {   // port voltages before the E update
         PostArgs pa = D.pa[D.cur];
         pa.advance = 0;
-        if (D.nport) k_post<<<1, kBlock, 0, D.stream>>>(pa);
+        if (D.nport) k_post<<<1, kPostThreads, 0, D.stream>>>(pa);
     }
     if (phase_mask & 4) {   // E over node planes [i0, i1) within [0, nx)
         const int a = std::max(0, i0), b = std::min(nx, i1);
         if (b > a) {
             t_begin(1);
-            kEKernels[s->npole]<<<dim3(3 * gx, (b - a + kU - 1) / kU), blk, 0, D.stream>>>(D.sa[D.cur], a, b);
+            for (int c0 = a; c0 < b; c0 += kMaxGridY)
+                kEKernels[s->npole]<<<dim3(3 * gxe, std::min(kMaxGridY, b - c0)), blk, 0, D.stream>>>(D.sa[D.cur],
+                                                                                                       c0);
             t_end();
         }
     }
@@ -1754,7 +2270,7 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
         PostArgs pa = D.pa[D.cur];
         pa.advance = 1;
         t_begin(3);
-        k_post<<<1, kBlock, 0, D.stream>>>(pa);
+        k_post<<<1, kPostThreads, 0, D.stream>>>(pa);
         t_end();
         D.ring_count++;
         s->step++;
@@ -1837,7 +2353,8 @@ bool energy_on_device(cem_sim *s, double *out) {
     if (!begin_device_op(s)) return false;
     Device &D = *s->dev;
     const int gx = (D.g.plane + kBlock - 1) / kBlock;
-    k_energy<<<dim3(gx, s->n[0] + 1), kBlock, 0, D.stream>>>(D.ea[D.cur]);
+    for (int c0 = 0; c0 <= s->n[0]; c0 += kMaxGridY)
+        k_energy<<<dim3(gx, std::min(kMaxGridY, s->n[0] + 1 - c0)), kBlock, 0, D.stream>>>(D.ea[D.cur], c0);
     k_sum<<<1, 1024, 0, D.stream>>>(D.partial.p, (long long)gx * (s->n[0] + 1), D.scalar.p);
     CB2_CHECK(s, cudaGetLastError());
     CB2_CHECK(s, cudaMemcpyAsync(out, D.scalar.p, sizeof(double), cudaMemcpyDeviceToHost, D.stream));
@@ -1912,7 +2429,8 @@ bool energy_noalloc(cem_sim *s, double *out) {
     if (!scratch) return false;
     EnergyArgs ea = D.ea[D.cur];
     ea.partial = scratch;
-    k_energy<<<dim3(gx, s->n[0] + 1), kBlock, 0, D.stream>>>(ea);
+    for (int c0 = 0; c0 <= s->n[0]; c0 += kMaxGridY)
+        k_energy<<<dim3(gx, std::min(kMaxGridY, s->n[0] + 1 - c0)), kBlock, 0, D.stream>>>(ea, c0);
     k_sum<<<1, 1024, 0, D.stream>>>(scratch, nblk, scratch + kNoAllocPartials);
     CB2_CHECK(s, cudaGetLastError());
     CB2_CHECK(s, cudaMemcpyAsync(out, scratch + kNoAllocPartials, sizeof(double), cudaMemcpyDeviceToHost, D.stream));
@@ -2003,11 +2521,14 @@ int cemx_sizes(const cem_sim *s, long long *out, int n) {
                      (long long)D.mat[c].n * 2 + (long long)D.tab[c].n * 4 + (long long)D.J[c].n * 4;
             for (int w = 0; w < 2; w++) bytes += (long long)(D.psiE[c][w].n + 2 * D.psiH[0][c][w].n) * 4;
         }
-        bytes += (long long)(D.sb_y.n + D.sb_hw.n) * 4 + (long long)(D.sb_eidx.n + D.sb_hidx.n) * 8 +
+        bytes += (long long)D.sb_y.n * 4 + (long long)(D.sb_hw.n + D.sb_hidx.n) * 16 + (long long)D.sb_eidx.n * 4 +
                  (long long)(D.ring.n + D.acc.n) * 8;
         v[11] = bytes;
     }
-    v[12] = 3 + (s->nsb ? 1 : 0);
+    // kernels per step: H and E (or one fused kernel), SIBC when present, the probe pass
+    int upd = 2;
+    if (s->dev && s->dev->use_fused) upd = 1;
+    v[12] = upd + 1 + (s->nsb ? 1 : 0);
     for (int q = 0; q < n && q < 13; q++) out[q] = v[q];
     return 0;
 }

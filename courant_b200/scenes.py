@@ -214,3 +214,17 @@ def gcpw_line(c: Courant, *, w=0.45e-3, gap=0.2e-3, h=0.254e-3, er=4.3, length=1
         meta["iprobes"] = [s.addIProbe(X, (ip1 + ip2) // 2, ja, jb, kh - 1, kt)]
     s.finalize(cfl)
     return s, meta
+
+
+def modeport_scene(c: Courant):
+    """Small lossy GCPW between 2D eigenmode ports, exercising every step
+    kernel at once: CPML on five faces, a 4-pole Djordjevic-Sarkar substrate,
+    35 um copper with Huray-rough surface impedance, a solder mask, the modal
+    source plane, and the port and probe line integrals. 1600 steps (the modal
+    pulse peaks near step 1250)."""
+    s, meta = gcpw_line(c, length=2e-3, hmin=50e-6, hmax=250e-6, dx=125e-6, yair=0.5e-3, zair=0.7e-3, npml=6,
+                        feed=1e-3, mon=0.5e-3, nf=8, tcu=35e-6, mask=20e-6, debye_poles=4, sigma_cu=5.8e7,
+                        huray=(0.5e-6, 2.0e11), modeports=True, probes=True, steps=1600)
+    meta["vprobes"] = list(range(c.ex.cem_plan_nvprobe(s.h)))
+    meta["iprobes"] = list(range(c.ex.cem_plan_niprobe(s.h)))
+    return s, meta

@@ -53,14 +53,18 @@ def spectrum_errors(gpu, orc, meta):
 
 
 @pytest.mark.parametrize("fused", [False, True], ids=["separate", "fused"])
-@pytest.mark.parametrize("fn", [scenes.parity_scene, scenes.lossy_scene], ids=["parity", "lossy"])
+@pytest.mark.parametrize("fn", [scenes.parity_scene, scenes.lossy_scene, scenes.modeport_scene],
+                         ids=["parity", "lossy", "modeport"])
 def test_scene_against_oracle(lib, oracle_lib, fn, fused):
     """At step 600 (fields near their peak, the step of the reference's own
     GPU-vs-CPU check) every component is within relative L2 1e-5 of the f64
     oracle, and max|diff|/max|field| per E/H family as the reference measures
     it. At the end of the run, where the fields have decayed to a few percent
-    of their peak, errors are measured against each component's peak norm
-    over the run; spectra and energy against their own magnitude."""
+    of their peak, errors are measured against the largest peak norm of the
+    component's family (E or H) over the run: FP32 rounding scales with the
+    whole field, so a small component such as the longitudinal E of a line
+    carries errors of its family's size. Spectra and energy against their own
+    magnitude."""
     s, meta = fn(lib)
     s.useFused(fused)
     n = meta["steps"]
@@ -80,7 +84,8 @@ def test_scene_against_oracle(lib, oracle_lib, fn, fused):
                 scale = max(np.max(np.abs(o.field(c))) for c in fam)
                 assert worst / scale < FIELD_TOL
     assert s.steps == o.steps == n
-    e = field_errors(s, o, peak)
+    fam = np.repeat([peak[:3].max(), peak[3:].max()], 3)
+    e = field_errors(s, o, fam)
     assert max(e.values()) < FIELD_TOL, e
     sp = spectrum_errors(s, o, meta)
     assert max(sp.values()) < SPEC_TOL, sp
