@@ -144,6 +144,14 @@ _EXT_PROTOS = [
     ("cemx_release_device", _i, [_p]),
     ("cemx_use_fused", _i, [_p, _i]),
     ("cemx_energy_noalloc", _i, [_p, _dp]),
+    ("cemx_batch_create", _p, [_i]),
+    ("cemx_batch_destroy", None, [_p]),
+    ("cemx_batch_add", _i, [_p, _p, _l]),
+    ("cemx_batch_remove", _i, [_p, _p]),
+    ("cemx_batch_left", _l, [_p, _p]),
+    ("cemx_batch_run", _i, [_p, _l]),
+    ("cemx_batch_tune", _i, [_p, _i]),
+    ("cemx_batch_stats", _i, [_p, _dp, _i]),
 ]
 
 
@@ -214,6 +222,13 @@ class Courant:
         v = _f64([x for c in S for x in (c.real, c.imag)])
         self.ex.cem_s2_renormalize(_ptr(v), z1, z2, zref)
         return [complex(v[2 * q], v[2 * q + 1]) for q in range(4)]
+
+    def createBatch(self, device: int = -1) -> "Batch":
+        """Simulations advanced together on one device (include/courant_b200.h)."""
+        h = self.ex.cemx_batch_create(device)
+        if not h:
+            raise CourantError(f"cemx_batch_create: {self.last_error()}")
+        return Batch(self, h)
 
     def selectDevice(self, device: int):
         if self.ex.cemx_select_device(device) != 0:
@@ -503,3 +518,54 @@ def s_params(v1, i1, v2, i2, R):
     b1 = (v1 - R * i1) / (2 * sq)
     b2 = (v2 - R * i2) / (2 * sq)
     return b1 / a1, b2 / a1
+
+
+class Batch:
+    """Several finalized simulations advanced together on one device: batched
+    launches over a work-list across the members, graph-captured chunks.
+    Results stay readable through each Sim between runs."""
+
+    def __init__(self, c: Courant, h):
+        self.c, self.h = c, h
+        self.members: list[Sim] = []
+
+    def _check(self, rc: int, what: str) -> int:
+        if rc < 0:
+            raise CourantError(f"{what}: {self.c.last_error()}")
+        return rc
+
+    def add(self, sim: "Sim", steps: int) -> int:
+        rc = self._check(self.c.ex.cemx_batch_add(self.h, sim.h, int(steps)), "batch_add")
+        self.members.append(sim)
+        return rc
+
+    def remove(self, sim: "Sim"):
+        self._check(self.c.ex.cemx_batch_remove(self.h, sim.h), "batch_remove")
+        self.members.remove(sim)
+
+    def left(self, sim: "Sim") -> int:
+        return int(self.c.ex.cemx_batch_left(self.h, sim.h))
+
+    def run(self, max_steps: int) -> int:
+        """Advance every member by up to max_steps; returns members still short of their budget."""
+        return self._check(self.c.ex.cemx_batch_run(self.h, int(max_steps)), "batch_run")
+
+    def tune(self, on: bool = True) -> bool:
+        return bool(self.c.ex.cemx_batch_tune(self.h, int(on)))
+
+    def stats(self) -> dict:
+        v = (C.c_double * 6)()
+        self._check(self.c.ex.cemx_batch_stats(self.h, v, 6), "batch_stats")
+        return {"ms": v[0], "steps": int(v[1]), "launches": int(v[2]), "chunk": int(v[3]), "order": int(v[4]),
+                "members": int(v[5])}
+
+    def destroy(self):
+        if getattr(self, "h", None):
+            self.c.ex.cemx_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

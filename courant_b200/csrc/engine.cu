@@ -31,6 +31,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -170,14 +171,16 @@ struct PostArgs {
 
 // --------------------------------------------------------------- helpers
 
+// Source waveforms, with every rounding explicit so that each kernel that
+// inlines them gives the same bits.
 __device__ __forceinline__ double gauss(double t, double amp, double t0, double tau) {
-    const double x = (t - t0) / tau;
-    return amp * exp(-x * x);
+    const double x = __ddiv_rn(__dsub_rn(t, t0), tau);
+    return __dmul_rn(amp, exp(-__dmul_rn(x, x)));
 }
 
 __device__ __forceinline__ double dgauss(double t, double t0, double tau) {
-    const double x = (t - t0) / tau;
-    return -2 * x * exp(-x * x);
+    const double x = __ddiv_rn(__dsub_rn(t, t0), tau);
+    return __dmul_rn(__dmul_rn(-2.0, x), exp(-__dmul_rn(x, x)));
 }
 
 // ------------------------------------------------- per-point arithmetic
@@ -1024,9 +1027,7 @@ const FKernel kFKernels[] = {CB2_POLES(CB2_FK)};
 
 // E = sum_k c_k (J - y_k) with y_k += (1 - e_k)(J - y_k), J from the faces' H.
 // (reference sibc.c:256-269)
-__global__ void __launch_bounds__(kBlock) k_sibc(const SibcArgs a) {
-    const int e = blockIdx.x * kBlock + threadIdx.x;
-    if (e >= a.ns) return;
+__device__ __forceinline__ void sibc_edge(const SibcArgs &a, int e) {
     // every load first: face tables (16-byte vectors), the convolution
     // states, then the H values of the faces
     const float4 w4 = __ldg(a.hw + e);
@@ -1042,22 +1043,28 @@ __global__ void __launch_bounds__(kBlock) k_sibc(const SibcArgs a) {
     float h[4];
 #pragma unroll
     for (int f = 0; f < 4; f++) h[f] = w[f] != 0.f ? a.H[hc[f]][hi[f]] : 0.f;
+    // explicit roundings: the same bits in every kernel that inlines this
     float J = 0.f;
 #pragma unroll
     for (int f = 0; f < 4; f++)
-        if (w[f] != 0.f) J += w[f] * h[f];
+        if (w[f] != 0.f) J = __fmaf_rn(w[f], h[f], J);
     float E = 0.f;
 #pragma unroll
     for (int k = 0; k < kSibcTerms; k++) {
         if (k < a.K) {
-            y[k] += a.ome[k] * (J - y[k]);
-            E += a.c[k] * (J - y[k]);
+            y[k] = __fmaf_rn(a.ome[k], __fsub_rn(J, y[k]), y[k]);
+            E = __fmaf_rn(a.c[k], __fsub_rn(J, y[k]), E);
         }
     }
 #pragma unroll
     for (int k = 0; k < kSibcTerms; k++)
         if (k < a.K) a.y[(long long)k * a.ns + e] = y[k];
     a.E[a.ecomp[e]][a.eidx[e]] = E;
+}
+
+__global__ void __launch_bounds__(kBlock) k_sibc(const SibcArgs a) {
+    const int e = blockIdx.x * kBlock + threadIdx.x;
+    if (e < a.ns) sibc_edge(a, e);
 }
 
 // ------------------------------------------------- probes, ports, DFT ring
@@ -1071,7 +1078,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 // the differentiated modal Gaussian Vm at the H time (n + 1/2) dt (reference
 // sim.c:834-838,900-909, modeport.c:124-135). Computed once per step.
 __device__ __forceinline__ void source_values(const PostArgs &a, long long n, float *out) {
-    const double tH = ((double)n + 0.5) * a.dt;
+    const double tH = __dmul_rn(__dadd_rn((double)n, 0.5), a.dt);
     out[0] = a.src_port >= 0 ? (float)gauss(tH, a.src_amp, a.src_t0, a.src_tau) : 0.f;
     out[1] = a.msrc_on ? (float)dgauss(tH, a.m_t0, a.m_tau) : 0.f;
 }
@@ -1079,7 +1086,7 @@ __device__ __forceinline__ void source_values(const PostArgs &a, long long n, fl
 // Line integrals of every input slot (warp per slot), then port V/I and the
 // source value, written as one row of the sample ring. With advance = 0 it
 // only refreshes the port voltages before the E update (vold).
-__global__ void __launch_bounds__(kPostThreads) k_post(const PostArgs a) {
+__device__ __forceinline__ void post_block(const PostArgs &a) {
     __shared__ double res[kMaxSlots];
     __shared__ double val[kPostStage];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1090,13 +1097,13 @@ __global__ void __launch_bounds__(kPostThreads) k_post(const PostArgs a) {
     const bool staged = e1 - e0 <= kPostStage;
     if (staged) {
         for (int e = e0 + threadIdx.x; e < e1; e += kPostThreads)
-            val[e - e0] = (double)a.F[a.ecomp[e]][a.eidx[e]] * a.ew[e];
+            val[e - e0] = __dmul_rn((double)a.F[a.ecomp[e]][a.eidx[e]], a.ew[e]);
         __syncthreads();
     }
     for (int s = first + warp; s < last; s += kPostThreads / 32) {
         double v = 0;
         for (int e = a.off[s] + lane; e < a.off[s + 1]; e += 32)
-            v += staged ? val[e - e0] : (double)a.F[a.ecomp[e]][a.eidx[e]] * a.ew[e];
+            v = __dadd_rn(v, staged ? val[e - e0] : __dmul_rn((double)a.F[a.ecomp[e]][a.eidx[e]], a.ew[e]));
         v = warp_sum(v);
         if (lane == 0) res[s] = v;
     }
@@ -1107,20 +1114,20 @@ __global__ void __launch_bounds__(kPostThreads) k_post(const PostArgs a) {
         return;
     }
     double *row = a.ring + (long long)(step % kRing) * a.nslot;
-    const double tH = ((double)step + 0.5) * a.dt;
+    const double tH = __dmul_rn(__dadd_rn((double)step, 0.5), a.dt);
     const double vs = a.src_port >= 0 ? gauss(tH, a.src_amp, a.src_t0, a.src_tau) : 0.0;
     for (int s = threadIdx.x; s < a.nip; s += kPostThreads) row[s] = res[s];
     for (int p = threadIdx.x; p < a.nport; p += kPostThreads) {
         const double vnew = res[a.nip + p];
-        const double V = 0.5 * (vnew + a.vold[p]);
+        const double V = __dmul_rn(0.5, __dadd_rn(vnew, a.vold[p]));
         a.vold[p] = vnew;
-        const double I = ((p == a.src_port ? vs : 0.0) - V) / a.R[p];
+        const double I = __ddiv_rn(__dsub_rn(p == a.src_port ? vs : 0.0, V), a.R[p]);
         row[a.nip + 2 * p] = V;
         row[a.nip + 2 * p + 1] = I;
     }
     if (threadIdx.x == 0) {
         double src = a.src_port >= 0 ? vs : 0.0;
-        if (a.msrc_on) src += dgauss(tH, a.m_t0, a.m_tau);
+        if (a.msrc_on) src = __dadd_rn(src, dgauss(tH, a.m_t0, a.m_tau));
         row[a.nip + 2 * a.nport] = src;
     }
     for (int s = threadIdx.x; s < a.nvp; s += kPostThreads) row[a.nip + 2 * a.nport + 1 + s] = res[a.nip + a.nport + s];
@@ -1130,6 +1137,8 @@ __global__ void __launch_bounds__(kPostThreads) k_post(const PostArgs a) {
         source_values(a, step + 1, a.srcv);
     }
 }
+
+__global__ void __launch_bounds__(kPostThreads) k_post(const PostArgs a) { post_block(a); }
 
 // source values for the step count held on the device (after it was set from the host)
 __global__ void k_source_values(const PostArgs a) { source_values(a, *a.dstep, a.srcv); }
@@ -1159,6 +1168,68 @@ __global__ void k_dft(const double *ring, int nslot, int first_e_slot, long long
     a[0] = re;
     a[1] = im;
 }
+
+// ------------------------------------------------------- batched kernels
+//
+// Several simulations on one device advance together: each launch walks a
+// work-list of blocks across all of them. A block stages its simulation's
+// arguments in shared memory and then runs exactly the per-simulation code
+// (h_vec, e_vec, sibc_edge, post_block), so every simulation computes the
+// same bits alone and in a batch.
+
+// this simulation's arguments, copied to shared memory by the whole block
+template <class T>
+__device__ __forceinline__ const T &stage_args(const T *src, unsigned *buf) {
+    static_assert(sizeof(T) % 4 == 0, "arguments copied as 4-byte words");
+    const unsigned *s = reinterpret_cast<const unsigned *>(src);
+    for (int q = threadIdx.x; q < (int)(sizeof(T) / 4); q += blockDim.x) buf[q] = s[q];
+    __syncthreads();
+    return *reinterpret_cast<const T *>(buf);
+}
+
+// work entry: x simulation, y block of the plane (component = y % 3), z node plane
+__global__ void __launch_bounds__(kBlock, CB2_H_MINBLOCKS) k_batch_h(const StepArgs *args, const int4 *work) {
+    __shared__ unsigned buf[sizeof(StepArgs) / 4];
+    const int4 w = work[blockIdx.x];
+    const StepArgs &a = stage_args(args + w.x, buf);
+    const RowPos r = row_pos(a.seg_h, a.g.n[1] + 1, w.y / 3);
+    const int comp = w.y % 3;
+    if (comp == 0) h_vec<0>(a, w.z, r);
+    else if (comp == 1) h_vec<1>(a, w.z, r);
+    else h_vec<2>(a, w.z, r);
+}
+
+template <int P>
+__global__ void __launch_bounds__(kBlock, CB2_E_MINBLOCKS) k_batch_e(const StepArgs *args, const int4 *work) {
+    __shared__ unsigned buf[sizeof(StepArgs) / 4];
+    const int4 w = work[blockIdx.x];
+    const StepArgs &a = stage_args(args + w.x, buf);
+    const RowPos r = row_pos(a.seg_e, a.g.n[1] + 1, w.y / 3);
+    const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
+    const int comp = w.y % 3;
+    if (comp == 0) e_vec<0, P>(a, w.z, r, sv);
+    else if (comp == 1) e_vec<1, P>(a, w.z, r, sv);
+    else e_vec<2, P>(a, w.z, r, sv);
+}
+
+using BEKernel = void (*)(const StepArgs *, const int4 *);
+#define CB2_BE(p) k_batch_e<p>,
+const BEKernel kBEKernels[] = {CB2_BE(0) CB2_BE(1) CB2_BE(2) CB2_BE(3) CB2_BE(4) CB2_BE(5) CB2_BE(6) CB2_BE(7) CB2_BE(8)
+                                   CB2_BE(9) CB2_BE(10) CB2_BE(11) CB2_BE(12) CB2_BE(13) CB2_BE(14) CB2_BE(15)
+                                       CB2_BE(16)};
+#undef CB2_BE
+
+// work entry: x simulation, y first edge of the block
+__global__ void __launch_bounds__(kBlock) k_batch_sibc(const SibcArgs *args, const int2 *work) {
+    __shared__ unsigned buf[sizeof(SibcArgs) / 4];
+    const int2 w = work[blockIdx.x];
+    const SibcArgs &a = stage_args(args + w.x, buf);
+    const int e = w.y + threadIdx.x;
+    if (e < a.ns) sibc_edge(a, e);
+}
+
+// one block per simulation
+__global__ void __launch_bounds__(kPostThreads) k_batch_post(const PostArgs *args) { post_block(args[blockIdx.x]); }
 
 // ----------------------------------------------------------------- energy
 
@@ -2486,6 +2557,183 @@ bool profiled_steps(cem_sim *s, long n, double *kernel_ms, long *launches) {
 }
 }  // namespace
 
+// ------------------------------------------------------------------ batches
+
+// Simulations advanced together on one device (cemx_batch_*). Each member
+// keeps its own device state; the batch holds device copies of the members'
+// kernel arguments and the work-lists of the batched kernels, rebuilt when
+// the set of members still short of their step budget changes, and a CUDA
+// graph of `chunk` batched steps, captured once per work-list.
+struct cemx_batch {
+    struct Member {
+        cem_sim *s;
+        long left;   // steps still to run
+    };
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<Member> members;
+    std::vector<int> active;                 // members in the work-lists
+    DevBuf<StepArgs> args;
+    DevBuf<SibcArgs> sargs;
+    DevBuf<PostArgs> pargs;
+    DevBuf<int4> work_h;
+    std::map<int, DevBuf<int4>> work_e;      // by pole count
+    DevBuf<int2> work_s;
+    size_t nh = 0, ns = 0;
+    std::map<int, size_t> ne;
+    bool dirty = true;
+    int order = 0;                           // work-list order: 0 member-major, 1 plane-interleaved
+    int chunk = 64;                          // steps per graph launch
+    bool tune = false, tuned = false;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0;
+    long last_steps = 0, last_launches = 0;
+};
+
+namespace {
+
+bool batch_fail(const char *what, cudaError_t e) {
+    char msg[256];
+    std::snprintf(msg, sizeof msg, "batch: CUDA %s: %s", what, cudaGetErrorString(e));
+    set_error(msg);
+    return false;
+}
+#define CB2_BCHECK(call)                                   \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return batch_fail(#call, e_); \
+    } while (0)
+
+template <class T>
+bool batch_upload(DevBuf<T> &b, const std::vector<T> &v) {
+    if (b.p) { cudaFree(b.p); b.p = nullptr; b.n = 0; }
+    if (v.empty()) return true;
+    CB2_BCHECK(cudaMalloc(&b.p, v.size() * sizeof(T)));
+    b.n = v.size();
+    CB2_BCHECK(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return true;
+}
+
+void batch_drop_graph(cemx_batch *b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->graph_steps = 0;
+}
+
+// work-lists of the members still short of their budget
+bool batch_rebuild(cemx_batch *b) {
+    batch_drop_graph(b);
+    b->active.clear();
+    for (int m = 0; m < (int)b->members.size(); m++)
+        if (b->members[m].left > 0) b->active.push_back(m);
+    std::vector<StepArgs> sa;
+    std::vector<SibcArgs> sb;
+    std::vector<PostArgs> pa;
+    std::vector<int4> wh;
+    std::map<int, std::vector<int4>> we;
+    std::vector<int2> ws;
+    int maxp = 0;
+    for (int x = 0; x < (int)b->active.size(); x++) {
+        cem_sim *s = b->members[b->active[x]].s;
+        Device &D = *s->dev;
+        sa.push_back(D.sa[D.cur]);
+        sb.push_back(D.sb[D.cur]);
+        pa.push_back(D.pa[D.cur]);
+        pa.back().advance = 1;
+        maxp = std::max(maxp, s->n[0] + 1);
+        for (int e0 = 0; e0 < s->nsb; e0 += kBlock) ws.push_back(make_int2(x, e0));
+    }
+    // H over planes 0..nx, E over 0..nx-1; member-major, or plane by plane across members
+    auto add_plane = [&](int x, int i) {
+        cem_sim *s = b->members[b->active[x]].s;
+        const StepArgs &a = sa[x];
+        if (i <= s->n[0])
+            for (int bx = 0; bx < 3 * a.seg_h.blk[a.seg_h.n]; bx++) wh.push_back(make_int4(x, bx, i, 0));
+        if (i < s->n[0])
+            for (int bx = 0; bx < 3 * a.seg_e.blk[a.seg_e.n]; bx++) we[s->npole].push_back(make_int4(x, bx, i, 0));
+    };
+    if (b->order == 0) {
+        for (int x = 0; x < (int)b->active.size(); x++)
+            for (int i = 0; i <= b->members[b->active[x]].s->n[0]; i++) add_plane(x, i);
+    } else {
+        for (int i = 0; i < maxp; i++)
+            for (int x = 0; x < (int)b->active.size(); x++) add_plane(x, i);
+    }
+    if (!batch_upload(b->args, sa) || !batch_upload(b->sargs, sb) || !batch_upload(b->pargs, pa) ||
+        !batch_upload(b->work_h, wh) || !batch_upload(b->work_s, ws))
+        return false;
+    b->work_e.clear();
+    b->ne.clear();
+    for (auto &kv : we) {
+        if (!batch_upload(b->work_e[kv.first], kv.second)) return false;
+        b->ne[kv.first] = kv.second.size();
+    }
+    b->nh = wh.size();
+    b->ns = ws.size();
+    b->dirty = false;
+    return true;
+}
+
+// one batched time step: H, E (one launch per pole count), SIBC, probes
+int batch_step(cemx_batch *b) {
+    int launches = 0;
+    if (b->nh) { k_batch_h<<<(unsigned)b->nh, kBlock, 0, b->stream>>>(b->args.p, b->work_h.p); launches++; }
+    for (auto &kv : b->ne)
+        if (kv.second) {
+            kBEKernels[kv.first]<<<(unsigned)kv.second, kBlock, 0, b->stream>>>(b->args.p, b->work_e[kv.first].p);
+            launches++;
+        }
+    if (b->ns) { k_batch_sibc<<<(unsigned)b->ns, kBlock, 0, b->stream>>>(b->sargs.p, b->work_s.p); launches++; }
+    k_batch_post<<<(unsigned)b->active.size(), kPostThreads, 0, b->stream>>>(b->pargs.p);
+    return launches + 1;
+}
+
+// n batched steps, through the cached graph when n is the chunk length
+bool batch_launch(cemx_batch *b, int n) {
+    if (n == b->chunk) {
+        if (!b->graph || b->graph_steps != n) {
+            batch_drop_graph(b);
+            cudaGraph_t g = nullptr;
+            CB2_BCHECK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            for (int q = 0; q < n; q++) batch_step(b);
+            CB2_BCHECK(cudaStreamEndCapture(b->stream, &g));
+            const cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) { b->graph = nullptr; return batch_fail("cudaGraphInstantiate", e); }
+            b->graph_steps = n;
+        }
+        CB2_BCHECK(cudaGraphLaunch(b->graph, b->stream));
+        b->last_launches += 1;
+    } else {
+        for (int q = 0; q < n; q++) b->last_launches += batch_step(b);
+    }
+    CB2_BCHECK(cudaGetLastError());
+    return true;
+}
+
+// Per-composition choice of chunk length and work-list order, found by timing
+// real batched steps once and kept for the process.
+std::mutex g_tune_mu;
+std::map<std::string, std::pair<int, int>> g_tuned;
+
+std::string batch_signature(const cemx_batch *b) {
+    std::vector<std::string> v;
+    for (int m : b->active) {
+        const cem_sim *s = b->members[m].s;
+        char k[96];
+        std::snprintf(k, sizeof k, "%dx%dx%d/p%d/s%d", s->n[0], s->n[1], s->n[2], s->npole, s->nsb);
+        v.push_back(k);
+    }
+    std::sort(v.begin(), v.end());
+    std::string sig;
+    for (auto &x : v) sig += x + ";";
+    return sig;
+}
+
+}  // namespace
+
 extern "C" {
 
 int cemx_step_timed(cem_sim *s, long n, double *gpu_ms) {
@@ -2562,6 +2810,203 @@ int cemx_energy_noalloc(cem_sim *s, double *out) {
     if (!s || !out) { set_error("cemx_energy_noalloc: null argument"); return -1; }
     if (!s->finalized) { set_error("not finalized"); return -1; }
     return energy_noalloc(s, out) ? 0 : -1;
+}
+
+
+cemx_batch *cemx_batch_create(int device) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        set_error("no CUDA device: libcourant_b200 steps only on the GPU");
+        return nullptr;
+    }
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) { set_error("no current CUDA device"); return nullptr; }
+    if (device >= n) { set_error("no such CUDA device"); return nullptr; }
+    cemx_batch *b = new cemx_batch;
+    b->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+        set_error("batch: cannot create its stream");
+        cemx_batch_destroy(b);
+        return nullptr;
+    }
+    return b;
+}
+
+void cemx_batch_destroy(cemx_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_drop_graph(b);
+    b->work_e.clear();
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+int cemx_batch_add(cemx_batch *b, cem_sim *s, long steps) {
+    if (!b || !s) { set_error("batch: null argument"); return -1; }
+    if (!s->finalized) { set_error("not finalized"); return -1; }
+    if (steps < 0) { set_error("batch: negative step count"); return -1; }
+    for (auto &m : b->members)
+        if (m.s == s) { set_error("batch: simulation already a member"); return -1; }
+    const int prev = g_selected_device;
+    g_selected_device = b->device;
+    const bool ok = create_device(s);
+    g_selected_device = prev;
+    if (!ok) return -1;
+    if (s->dev->device != b->device) { set_error("batch: simulation lives on another device"); return -1; }
+    b->members.push_back({s, steps});
+    b->dirty = true;
+    return (int)b->members.size() - 1;
+}
+
+int cemx_batch_remove(cemx_batch *b, cem_sim *s) {
+    if (!b) { set_error("batch: null argument"); return -1; }
+    for (size_t m = 0; m < b->members.size(); m++)
+        if (b->members[m].s == s) {
+            cudaSetDevice(b->device);
+            cudaStreamSynchronize(b->stream);
+            b->members.erase(b->members.begin() + m);
+            b->dirty = true;
+            return 0;
+        }
+    set_error("batch: not a member");
+    return -1;
+}
+
+long cemx_batch_left(const cemx_batch *b, const cem_sim *s) {
+    if (!b) return -1;
+    for (const auto &m : b->members)
+        if (m.s == s) return m.left;
+    return -1;
+}
+
+int cemx_batch_tune(cemx_batch *b, int on) {
+    if (!b) return -1;
+    const int prev = b->tune ? 1 : 0;
+    b->tune = on != 0;
+    b->tuned = false;
+    return prev;
+}
+
+int cemx_batch_run(cemx_batch *b, long max_steps) {
+    if (!b) { set_error("batch: null argument"); return -1; }
+    if (cudaSetDevice(b->device) != cudaSuccess) { set_error("batch: cannot select its device"); return -1; }
+    std::vector<cem_sim *> touched;
+    for (auto &m : b->members)
+        if (m.left > 0) {
+            if (!begin_device_op(m.s)) return -1;
+            touched.push_back(m.s);
+        }
+    b->last_ms = 0;
+    b->last_steps = 0;
+    b->last_launches = 0;
+    if (cudaEventRecord(b->ev0, b->stream) != cudaSuccess) { set_error("batch: event"); return -1; }
+    long done = 0;
+    while (done < max_steps) {
+        if (b->dirty && !batch_rebuild(b)) return -1;
+        if (b->active.empty()) break;
+        if (b->tune && !b->tuned) {
+            // chunk length and work-list order: cached per composition, else timed on real steps
+            const std::string sig = batch_signature(b);
+            std::pair<int, int> best{b->chunk, b->order};
+            bool cached = false;
+            {
+                std::lock_guard<std::mutex> lock(g_tune_mu);
+                auto it = g_tuned.find(sig);
+                if (it != g_tuned.end()) { best = it->second; cached = true; }
+            }
+            if (!cached) {
+                long minleft = max_steps - done;
+                for (int m : b->active) minleft = std::min(minleft, b->members[m].left);
+                float best_ms = 1e30f;
+                for (int order = 0; order < 2; order++)
+                    for (int ch : {16, 64, 256}) {
+                        if (2 * ch > minleft) continue;   // one warm-up and one timed chunk
+                        if (b->order != order) { b->order = order; if (!batch_rebuild(b)) return -1; }
+                        b->chunk = ch;
+                        float ms = 0;
+                        for (int rep = 0; rep < 2; rep++) {
+                            for (int m : b->active) {
+                                Device &D = *b->members[m].s->dev;
+                                if (D.ring_count + ch > kRing) {
+                                    cudaStreamSynchronize(b->stream);
+                                    if (!flush_dft(b->members[m].s) || cudaStreamSynchronize(D.stream) != cudaSuccess)
+                                        return -1;
+                                }
+                            }
+                            cudaEvent_t t0, t1;
+                            cudaEventCreate(&t0);
+                            cudaEventCreate(&t1);
+                            cudaEventRecord(t0, b->stream);
+                            if (!batch_launch(b, ch)) return -1;
+                            cudaEventRecord(t1, b->stream);
+                            cudaEventSynchronize(t1);
+                            cudaEventElapsedTime(&ms, t0, t1);
+                            cudaEventDestroy(t0);
+                            cudaEventDestroy(t1);
+                            for (int m : b->active) {
+                                b->members[m].s->step += ch;
+                                b->members[m].s->dev->ring_count += ch;
+                                b->members[m].left -= ch;
+                            }
+                            done += ch;
+                            minleft -= ch;
+                            b->last_steps += ch;
+                        }
+                        if (ms / ch < best_ms) { best_ms = ms / ch; best = {ch, order}; }
+                    }
+                std::lock_guard<std::mutex> lock(g_tune_mu);
+                g_tuned[sig] = best;
+            }
+            b->tuned = true;
+            if (b->order != best.second) { b->order = best.second; b->dirty = true; }
+            b->chunk = best.first;
+            for (int m : b->active)
+                if (b->members[m].left <= 0) b->dirty = true;
+            continue;
+        }
+        long n = std::min<long>(b->chunk, max_steps - done);
+        for (int m : b->active) n = std::min(n, b->members[m].left);
+        for (int m : b->active) {
+            Device &D = *b->members[m].s->dev;
+            if (D.ring_count + n > kRing) {   // room in the sample ring for n rows
+                cudaStreamSynchronize(b->stream);
+                if (!flush_dft(b->members[m].s) || cudaStreamSynchronize(D.stream) != cudaSuccess) return -1;
+            }
+        }
+        if (!batch_launch(b, (int)n)) return -1;
+        for (int m : b->active) {
+            cemx_batch::Member &mb = b->members[m];
+            mb.s->step += n;
+            mb.s->dev->ring_count += n;
+            mb.left -= n;
+            if (mb.left == 0) b->dirty = true;
+        }
+        done += n;
+        b->last_steps += n;
+    }
+    float ms = 0;
+    if (cudaEventRecord(b->ev1, b->stream) != cudaSuccess || cudaEventSynchronize(b->ev1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, b->ev0, b->ev1) != cudaSuccess) {
+        set_error("batch: a batched launch failed");
+        return -1;
+    }
+    b->last_ms = ms;
+    for (cem_sim *s : touched)
+        if (!end_device_op(s)) return -1;
+    int left = 0;
+    for (auto &m : b->members) left += m.left > 0;
+    return left;
+}
+
+int cemx_batch_stats(const cemx_batch *b, double *out, int n) {
+    if (!b) return -1;
+    const double v[6] = {b->last_ms, (double)b->last_steps, (double)b->last_launches, (double)b->chunk,
+                         (double)b->order, (double)b->members.size()};
+    for (int q = 0; q < n && q < 6; q++) out[q] = v[q];
+    return 0;
 }
 
 int cemx_synchronize(cem_sim *s) {

@@ -68,6 +68,46 @@ CEM_API int cemx_use_fused(cem_sim *s, int on);
  * grid needs more than 65536 partials (use cem_energy). Returns 0 or -1. */
 CEM_API int cemx_energy_noalloc(cem_sim *s, double *energy);
 
+/* Batches (no counterpart in the reference core). A batch advances several
+ * finalized simulations on one device together: every batched launch walks a
+ * work-list of blocks across all members (H, E, surface impedance, probes),
+ * and runs of `chunk` steps replay one captured CUDA graph. Each member
+ * computes the same bits as when stepped alone with cem_step. Members keep
+ * their own device state, so results are read with the usual courant.h calls
+ * between runs. A simulation belongs to at most one batch and must not be
+ * stepped by other calls while it is a member. */
+typedef struct cemx_batch cemx_batch;
+
+/* A batch on CUDA device `device` (-1: the current device); NULL on error. */
+CEM_API cemx_batch *cemx_batch_create(int device);
+
+/* Stop and free the batch (not its members). */
+CEM_API void cemx_batch_destroy(cemx_batch *b);
+
+/* Add a finalized simulation with a budget of `steps` further steps; creates
+ * its device state on the batch's device. Returns its member index or -1. */
+CEM_API int cemx_batch_add(cemx_batch *b, cem_sim *s, long steps);
+
+/* Remove a member (its state stays on the device). Returns 0 or -1. */
+CEM_API int cemx_batch_remove(cemx_batch *b, cem_sim *s);
+
+/* Steps a member still has to run, or -1 when s is not a member. */
+CEM_API long cemx_batch_left(const cemx_batch *b, const cem_sim *s);
+
+/* Advance every member by up to max_steps (each stops at its budget).
+ * Returns the number of members still short of their budget, or -1. */
+CEM_API int cemx_batch_run(cemx_batch *b, long max_steps);
+
+/* on = 1: the next run picks the graph length (16, 64 or 256 steps) and the
+ * work-list order by timing real steps, once per batch composition per
+ * process. Returns the previous setting. */
+CEM_API int cemx_batch_tune(cemx_batch *b, int on);
+
+/* Statistics of the last run, n entries of: device ms, steps, launches
+ * (graph launches count once), graph length, work-list order, members.
+ * Returns 0 or -1. */
+CEM_API int cemx_batch_stats(const cemx_batch *b, double *out, int n);
+
 /* Wait for all device work of s. Returns 0 or -1. */
 CEM_API int cemx_synchronize(cem_sim *s);
 

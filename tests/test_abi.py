@@ -86,6 +86,13 @@ def test_step_without_gpu_fails_loudly(lib, capfd):
     assert "no CUDA device" in capfd.readouterr().err
 
 
+@pytest.mark.skipif(HAS_CUDA, reason="checks the no-GPU path")
+def test_batch_without_gpu_fails_loudly(lib):
+    from courant_b200.api import CourantError
+    with pytest.raises(CourantError, match="no CUDA device"):
+        lib.createBatch()
+
+
 def test_field_pointer_before_finalize_is_writable(lib):
     x = np.linspace(0, 1e-3, 5)
     s = lib.createSim(x, x, x)

@@ -1,0 +1,105 @@
+"""Batches (cemx_batch_*): simulations of different sizes, pole counts and
+step budgets advanced together must give exactly what each gives alone with
+cem_step, stop at their own budgets, and keep doing so when members leave,
+join between runs, or the batch tunes its graph length and work order."""
+import numpy as np
+import pytest
+
+from courant_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+SCENES = [scenes.parity_scene, scenes.lossy_scene, scenes.modeport_scene]
+
+
+def results(s, meta):
+    out = {f"f{c}": s.field(c) for c in range(6)}
+    for p in meta.get("ports", []):
+        out[f"V{p}"], out[f"I{p}"] = s.portV(p), s.portI(p)
+    for p in meta.get("vprobes", []):
+        out[f"vp{p}"] = s.vprobe(p)
+    for p in meta.get("iprobes", []):
+        out[f"ip{p}"] = s.iprobe(p)
+    out["src"] = s.sourceSpectrum()
+    out["energy"] = np.array([s.energy()])
+    return out
+
+
+def assert_same(a, b):
+    assert a.keys() == b.keys()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def alone(lib, fn, n):
+    s, meta = fn(lib)
+    s.step(n)
+    r = results(s, meta)
+    s.destroy()
+    return r
+
+
+@pytest.mark.parametrize("tune", [False, True], ids=["fixed", "tuned"])
+def test_batch_matches_alone(lib, tune):
+    budgets = [700, 450, 1100]
+    ref = [alone(lib, fn, n) for fn, n in zip(SCENES, budgets)]
+    b = lib.createBatch()
+    b.tune(tune)
+    sims = [fn(lib) for fn in SCENES]
+    for (s, _), n in zip(sims, budgets):
+        b.add(s, n)
+    left = b.run(300)                   # every member advances 300 steps
+    assert left == 3
+    assert [s.steps for s, _ in sims] == [300, 300, 300]
+    while b.run(10_000):                # each stops at its own budget
+        pass
+    assert [s.steps for s, _ in sims] == budgets
+    assert [b.left(s) for s, _ in sims] == [0, 0, 0]
+    for (s, meta), r in zip(sims, ref):
+        assert_same(results(s, meta), r)
+    st = b.stats()
+    assert st["members"] == 3
+    b.destroy()
+    for s, _ in sims:
+        s.destroy()
+
+
+def test_batch_members_join_and_leave(lib):
+    """A member added after others ran, and one removed part-way, still match."""
+    ref_par = alone(lib, scenes.parity_scene, 900)
+    ref_lossy = alone(lib, scenes.lossy_scene, 500)
+    b = lib.createBatch()
+    p, pm = scenes.parity_scene(lib)
+    q, qm = scenes.lossy_scene(lib)
+    x, _ = scenes.parity_scene(lib)
+    b.add(p, 900)
+    b.add(x, 900)
+    b.run(256)
+    b.add(q, 500)                        # joins at a chunk boundary
+    b.run(100)
+    b.remove(x)                          # leaves; stepping it alone afterwards still works
+    x.step(3)
+    while b.run(1000):
+        pass
+    assert p.steps == 900 and q.steps == 500 and x.steps == 359
+    assert_same(results(p, pm), ref_par)
+    assert_same(results(q, qm), ref_lossy)
+    b.destroy()
+    for s in (p, q, x):
+        s.destroy()
+
+
+def test_batch_rejects_misuse(lib):
+    from courant_b200.api import CourantError
+    b = lib.createBatch()
+    s, _ = scenes.parity_scene(lib)
+    b.add(s, 10)
+    with pytest.raises(CourantError, match="already a member"):
+        b.add(s, 10)
+    with pytest.raises(CourantError, match="negative"):
+        t, _ = scenes.parity_scene(lib)
+        b.add(t, -1)
+    assert b.run(5) == 1 and s.steps == 5
+    assert b.run(100) == 0 and s.steps == 10
+    b.destroy()
+    s.destroy()
