@@ -32,6 +32,27 @@ def test_gcpw_plan_live_against_reference(lib, ref_lib):
     assert a.conductorFitError() == b.conductorFitError()
 
 
+@pytest.mark.parametrize("ports", ["mode", "lumped"])
+def test_seeded_board_plan_live_against_reference(lib, ref_lib, ports):
+    """The seeded board generator builds the same plan on both libraries
+    (4-pole Debye stackup, ground plane with clearances, staircased traces,
+    vias, mode or lumped ports)."""
+    from courant_b200 import boards
+    a, ma = boards.seeded_board(ref_lib, 11, 6e4, ports=ports, nf=4)
+    b, mb = boards.seeded_board(lib, 11, 6e4, ports=ports, nf=4)
+    assert ma["dims"] == mb["dims"] and ma["steps"] == mb["steps"]
+    assert cmp_plans(a.plan(), b.plan()) == []
+
+
+def test_seeded_board_is_deterministic(lib):
+    from courant_b200 import boards
+    a, _ = boards.seeded_board(lib, 5, 5e4, ports="lumped", nf=2)
+    b, _ = boards.seeded_board(lib, 5, 5e4, ports="lumped", nf=2)
+    c, _ = boards.seeded_board(lib, 6, 5e4, ports="lumped", nf=2)
+    assert cmp_plans(a.plan(), b.plan()) == []
+    assert cmp_plans(a.plan(), c.plan()) != []
+
+
 def test_djordjevic_sarkar_fit(lib, golden):
     g = golden["ds_fit"]
     m = lib.fitDjordjevicSarkar(*g["args"])
