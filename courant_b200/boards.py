@@ -45,10 +45,12 @@ def _dims(cells: float) -> tuple[int, int, int]:
 
 def seeded_board(c: Courant, seed: int, cells: float = 2e6, *, ports: str = "mode", nf: int = 32,
                  fmax: float = 20e9, steps: int | None = None, traces: int = 20, vias: int = 30,
-                 npml: int = 8, cfl: float = 0.99):
+                 npml: int = 8, cfl: float = 0.99, excite: int = 1):
     """Finalized board simulation and its metadata (dims, cells, ports,
     frequencies, step count). `cells` sets the grid size; `traces` and `vias`
-    scale down for small grids so features stay at least two cells wide."""
+    scale down for small grids so features stay at least two cells wide;
+    `excite` (1 or 2) picks the driven port, the two excitations of a full
+    2-port measurement."""
     rng = np.random.Generator(np.random.PCG64(seed))
     nx, ny, nz = _dims(cells)
     cores = rng.uniform(0.2e-3, 1.0e-3, 3)
@@ -144,19 +146,19 @@ def seeded_board(c: Courant, seed: int, cells: float = 2e6, *, ports: str = "mod
         s.pecBox(xs[vi], xs[vi + e], ys[vj], ys[vj + e], 0.0, zl[3])
     tau = math.sqrt(6.9) / (math.pi * 1.25 * fmax)
     freqs = np.linspace(fmax / nf, fmax, nf)
-    meta = {"seed": seed, "dims": (nx, ny, nz), "cells": nx * ny * nz, "tau": tau, "freqs": freqs}
+    meta = {"seed": seed, "dims": (nx, ny, nz), "cells": nx * ny * nz, "tau": tau, "freqs": freqs, "excite": excite}
     ktop = kl[3]
     if ports == "mode":
         d = dict(j0=0, j1=ny, k0=0, k1=nz, vj=t0_j, vk0=kl[1], vk1=ktop, vsign=-1, ja=max(t0_j - 1, 0),
                  jb=t0_j + t0_w, ka=ktop - 1, kb=ktop, f0=0.5 * fmax, neff0=math.sqrt((float(eps[2]) + 1) / 2))
         p1 = s.addModePort(dict(d, dir=1, iSrc=npml + 2, iMon=npml + 6, xRef=xs[npml + 8]))
         p2 = s.addModePort(dict(d, dir=-1, iSrc=nx - npml - 2, iMon=nx - npml - 7, xRef=xs[nx - npml - 8]))
-        s.setModeExcitation(p1, 4.5 * tau, tau)
+        s.setModeExcitation(p1 if excite == 1 else p2, 4.5 * tau, tau)
         meta["modeports"] = [p1, p2]
     else:
         p1 = s.addLumpedPort(Z, npml + 4, t0_j, kl[1], ktop, -1, 50.0)     # L2 ground to the L4 trace
         p2 = s.addLumpedPort(Z, nx - npml - 4, t0_j, kl[1], ktop, -1, 50.0)
-        s.setGaussian(p1, 1.0, 4.5 * tau, tau)
+        s.setGaussian(p1 if excite == 1 else p2, 1.0, 4.5 * tau, tau)
         meta["ports"] = [p1, p2]
     s.setFrequencies(freqs)
     s.finalize(cfl)

@@ -1,0 +1,215 @@
+"""Serving board simulations on one GPU with continuous batching.
+
+A `Server` accepts requests (a builder returning a finalized simulation, a
+step count) as they arrive. Builder threads do the host set-up (plan, mode
+solves) in parallel; the GPU thread admits built simulations into one
+`cemx_batch` while their estimated device footprint fits the HBM budget, runs
+the batch in chunks, and hands every simulation that reached its step count
+to finisher threads, which extract its S-parameters and free it, while the
+batch goes on with the others. Requests that arrive while others are on the
+GPU join at the next chunk boundary, so their work overlaps on the device.
+Each simulation computes the same bits as when it runs alone.
+
+`plain_loop` is the baseline: the same requests one at a time, set-up, steps
+and results in order, on the same GPU.
+
+Times are wall clock; `summary()` gives p50/p95/p99 time-to-S-parameters
+(arrival to result) and solves per hour.
+"""
+from __future__ import annotations
+
+import queue
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .api import Courant, Sim, s_params
+
+
+def footprint(sim: Sim) -> int:
+    """Device bytes a simulation will hold, from its sizes before its device
+    state exists: padded FP32 fields (6), u16 material indices (3), CPML
+    auxiliaries (padded layout, about 1.5x the compact count), Debye currents,
+    surface-impedance states, and a 10% margin for tables and probes."""
+    z = sim.sizes()
+    nx, ny, nz = sim.nx, sim.ny, sim.nz
+    sj = (nz + 1 + 7) // 8 * 8
+    npts = (nx + 1) * (ny + 1) * sj
+    b = npts * (6 * 4 + 3 * 2)
+    b += int(1.5 * 4 * (z["psiE"] + 2 * z["psiH"]))
+    b += int(1.3 * 4 * z["npole"] * z["ndisp"])
+    b += 4 * z["sibc_terms"] * z["nsibc"] + 48 * z["nsibc"]
+    return int(b * 1.1)
+
+
+def results(sim: Sim, meta: dict) -> dict:
+    """S11 and S21 of a two-port with port 1 excited: from the modal waves of
+    mode ports, or from the port spectra of lumped ports."""
+    if "modeports" in meta:
+        p1, p2 = meta["modeports"]
+        w1, w2 = sim.modePortWaves(p1), sim.modePortWaves(p2)
+        return {"S11": w1["b"] / w1["a"], "S21": w2["b"] / w1["a"]}
+    p1, p2 = meta["ports"]
+    s11, s21 = s_params(sim.portV(p1), sim.portI(p1), sim.portV(p2), sim.portI(p2), 50.0)
+    return {"S11": s11, "S21": s21}
+
+
+@dataclass
+class Request:
+    build: object                 # callable(Courant) -> (Sim, meta)
+    steps: int
+    tag: object = None
+    arrival: float = 0.0
+    admitted: float = 0.0
+    done: float = 0.0
+    result: dict | None = None
+    error: str | None = None
+    cells: int = 0
+    event: threading.Event = field(default_factory=threading.Event)
+
+
+class Server:
+    def __init__(self, lib: Courant, budget_bytes: float = 160e9, chunk: int = 512, builders: int = 4,
+                 finishers: int = 4, device: int = -1, tune: bool = True):
+        self.lib = lib
+        self.budget = int(budget_bytes)
+        self.chunk = chunk
+        self.batch = lib.createBatch(device)
+        self.batch.tune(tune)
+        self.incoming: queue.Queue = queue.Queue()
+        self.built: list = []          # (request, sim, meta, bytes) ready for admission, in arrival order
+        self.lock = threading.Lock()
+        self.wake = threading.Event()
+        self.members: dict = {}        # sim handle -> (request, sim, meta, bytes)
+        self.used = 0
+        self.finished: list[Request] = []
+        self.build_pool = ThreadPoolExecutor(builders)
+        self.finish_pool = ThreadPoolExecutor(finishers)
+        self.stop = False
+        self.gpu_ms = 0.0
+        self.thread = threading.Thread(target=self._gpu_loop, daemon=True)
+        self.thread.start()
+
+    # ---- requests
+    def submit(self, build, steps: int, tag=None) -> Request:
+        r = Request(build, int(steps), tag, arrival=time.perf_counter())
+        self.build_pool.submit(self._build, r)
+        return r
+
+    def _build(self, r: Request):
+        try:
+            sim, meta = r.build(self.lib)
+            r.cells = meta.get("cells", sim.nx * sim.ny * sim.nz)
+            nbytes = footprint(sim)
+            if nbytes > self.budget:
+                raise RuntimeError(f"needs {nbytes / 1e9:.1f} GB, above the {self.budget / 1e9:.1f} GB budget")
+            with self.lock:
+                self.built.append((r, sim, meta, nbytes))
+        except Exception as e:   # reported on the request
+            r.error = str(e)
+            r.done = time.perf_counter()
+            r.event.set()
+        self.wake.set()
+
+    # ---- the GPU thread
+    def _admit(self):
+        with self.lock:
+            keep = []
+            for item in self.built:
+                r, sim, meta, nbytes = item
+                if self.used + nbytes <= self.budget:
+                    self.batch.add(sim, r.steps)
+                    self.members[sim.h] = item
+                    self.used += nbytes
+                    r.admitted = time.perf_counter()
+                else:
+                    keep.append(item)
+            self.built = keep
+
+    def _finish(self, item):
+        r, sim, meta, nbytes = item
+        try:
+            r.result = results(sim, meta)
+        except Exception as e:
+            r.error = str(e)
+        sim.destroy()
+        with self.lock:
+            self.used -= nbytes
+        r.done = time.perf_counter()
+        self.finished.append(r)
+        r.event.set()
+        self.wake.set()
+
+    def _gpu_loop(self):
+        while not self.stop:
+            self._admit()
+            if not self.members:
+                self.wake.wait(0.01)
+                self.wake.clear()
+                continue
+            self.batch.run(self.chunk)
+            self.gpu_ms += self.batch.stats()["ms"]
+            for h, item in list(self.members.items()):
+                sim = item[1]
+                if self.batch.left(sim) == 0:
+                    self.batch.remove(sim)
+                    del self.members[h]
+                    self.finish_pool.submit(self._finish, item)
+
+    def close(self):
+        self.stop = True
+        self.wake.set()
+        self.thread.join()
+        self.build_pool.shutdown(wait=True)
+        self.finish_pool.shutdown(wait=True)
+        self.batch.destroy()
+
+
+def plain_loop(lib: Courant, requests: list[Request], arrivals: list[float]) -> list[Request]:
+    """The baseline: each request alone, in arrival order (set-up, steps,
+    results), waiting for its arrival time; arrivals relative to the start."""
+    t0 = time.perf_counter()
+    for r, at in zip(requests, arrivals):
+        now = time.perf_counter() - t0
+        if at > now:
+            time.sleep(at - now)
+        r.arrival = t0 + at
+        try:
+            sim, meta = r.build(lib)
+            r.cells = meta.get("cells", sim.nx * sim.ny * sim.nz)
+            sim.step(r.steps)
+            r.result = results(sim, meta)
+            sim.destroy()
+        except Exception as e:
+            r.error = str(e)
+        r.done = time.perf_counter()
+    return requests
+
+
+def serve_all(server: Server, requests: list[Request], arrivals: list[float]) -> list[Request]:
+    """Submit the requests at their arrival times (relative to now) and wait for all."""
+    t0 = time.perf_counter()
+    out = []
+    for r, at in zip(requests, arrivals):
+        now = time.perf_counter() - t0
+        if at > now:
+            time.sleep(at - now)
+        out.append(server.submit(r.build, r.steps, r.tag))
+    for r in out:
+        r.event.wait()
+    return out
+
+
+def summary(reqs: list[Request], t_start: float, t_end: float) -> dict:
+    lat = np.array([r.done - r.arrival for r in reqs if r.error is None])
+    cells = sum(r.cells * r.steps for r in reqs if r.error is None)
+    wall = t_end - t_start
+    return {"solves": int(len(lat)), "errors": sum(r.error is not None for r in reqs), "wall_s": wall,
+            "solves_per_hour": len(lat) / wall * 3600 if wall > 0 else None,
+            "cell_updates_per_s": cells / wall if wall > 0 else None,
+            "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+            "p95_s": float(np.percentile(lat, 95)) if len(lat) else None,
+            "p99_s": float(np.percentile(lat, 99)) if len(lat) else None}
