@@ -80,8 +80,8 @@ def seeded_board(c: Courant, seed: int, cells: float = 2e6, *, ports: str = "mod
     big = 1.0
     for q in range(3):
         s.materialBoxDebye(-big, big, -big, big, zl[q], zl[q + 1], fits[q])
-    # keep copper away from the CPML
-    i_lo, i_hi = npml + 2, nx - npml - 2
+    # keep copper away from the CPML, and the x ends (the port cross-sections) clear of all but trace 0
+    i_lo, i_hi = npml + 12, max(nx - npml - 12, npml + 20)
     j_lo, j_hi = npml + 2, ny - npml - 2
     xs, ys = x, y
     # L2 ground plane with clearances
