@@ -18,6 +18,11 @@ C ABI for one whole excitation (40 000 steps) with the plan and state
 uploaded from host memory inside the timed region and the spectra read back
 to the host after every chunk.
 
+On one GPU the line also carries `batching` (a mix of seeded boards stepped
+one at a time with cem_step against one batch) and `serving` (a Poisson stream
+of board requests through the plain FIFO loop against the continuously
+batching server, p50/p95/p99 time-to-S-parameters and solves/hour).
+
 --impl reference times the reference's own CPU core (oracle/_ref, OpenMP on
 all host cores) on the same workload, a bounded sample of steps per
 benchmark step.
@@ -190,6 +195,95 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
+def batch_compare(lib, runs: int, seed: int = 2026) -> dict:
+    """Batched uneven instances (a bounded stand-in for the 96-board mix): runs/2
+    seeded boards with cells log-uniform in 5e4-1e6, steps uniform in 2000-6000,
+    both excitations each; one at a time with cem_step (the plain path, set-up
+    excluded) against one batch (graph-captured batched launches, tuned once).
+    Results must be bit-identical; reports solves/hour and cell-updates/s."""
+    import numpy as np
+    from courant_b200 import boards, serve
+    rng = np.random.Generator(np.random.PCG64(seed))
+    half = max(runs // 2, 1)
+    cells = np.exp(rng.uniform(np.log(5e4), np.log(1e6), half))
+    steps = rng.integers(2000, 6000, half)
+    spec = [(q, float(cells[q]), int(steps[q]), ex) for q in range(half) for ex in (1, 2)]
+
+    def build():
+        return [boards.seeded_board(lib, q, cl, ports="lumped", nf=16, excite=ex) for q, cl, _, ex in spec]
+
+    sims = build()
+    work = sum(m["cells"] * n for (_, m), (_, _, n, _) in zip(sims, spec))
+    t0 = time.perf_counter()
+    for (s, _), (_, _, n, _) in zip(sims, spec):
+        s.step(n)
+    for s, _ in sims:
+        s.synchronize()
+    t_plain = time.perf_counter() - t0
+    plain = [serve.results(s, m)["S21"] for s, m in sims]
+    for s, _ in sims:
+        s.destroy()
+    sims = build()
+    b = lib.createBatch()
+    b.tune(True)
+    for (s, _), (_, _, n, _) in zip(sims, spec):
+        b.add(s, n)
+    t0 = time.perf_counter()
+    while b.run(1 << 30):
+        pass
+    t_batch = time.perf_counter() - t0
+    st = b.stats()
+    same = all(np.array_equal(a, serve.results(s, m)["S21"]) for a, (s, m) in zip(plain, sims))
+    b.destroy()
+    for s, _ in sims:
+        s.destroy()
+    n = len(spec)
+    return {"runs": n, "cell_updates": work, "same_results": same,
+            "plain": {"wall_s": t_plain, "solves_per_hour": n / t_plain * 3600, "cell_updates_per_s": work / t_plain},
+            "batched": {"wall_s": t_batch, "solves_per_hour": n / t_batch * 3600, "cell_updates_per_s": work / t_batch,
+                        "graph_steps": st["chunk"], "work_order": st["order"]},
+            "speedup": t_plain / t_batch,
+            "note": "wall time of the stepping only (set-up and S-parameters excluded); inputs resident"}
+
+
+def serve_compare(lib, n: int, rate: float, seed: int = 7) -> dict:
+    """Serving (a bounded stand-in for the Poisson request stream): n requests at
+    `rate` per second, seeded boards with cells log-uniform in 1e5-2e6, steps
+    uniform in 2000-6000, a quarter with 2D mode ports, the rest lumped, 16
+    frequencies; the plain FIFO loop (set-up, steps, S-parameters one request at
+    a time) against the continuously batching server. Times are wall clock from
+    arrival to S-parameters."""
+    import functools
+    import numpy as np
+    from courant_b200 import boards, serve
+    rng = np.random.Generator(np.random.PCG64(seed))
+    cells = np.exp(rng.uniform(np.log(1e5), np.log(2e6), n))
+    steps = rng.integers(2000, 6000, n)
+    kinds = rng.integers(0, 4, n)
+    arr = np.cumsum(rng.exponential(1 / rate, n))
+    arr -= arr[0]
+
+    def req(q):
+        ports = "mode" if kinds[q] == 0 else "lumped"
+        return serve.Request(functools.partial(boards.seeded_board, seed=100 + q, cells=float(cells[q]), ports=ports,
+                                               nf=16), int(steps[q]))
+
+    t0 = time.perf_counter()
+    plain = serve.plain_loop(lib, [req(q) for q in range(n)], list(arr))
+    sp = serve.summary(plain, t0, time.perf_counter())
+    srv = serve.Server(lib, chunk=512, builders=8, finishers=8)
+    t0 = time.perf_counter()
+    got = serve.serve_all(srv, [req(q) for q in range(n)], list(arr))
+    t1 = time.perf_counter()
+    srv.close()
+    ss = serve.summary(got, t0, t1)
+    same = all((a.result is None) == (g.result is None) and
+               (a.result is None or np.array_equal(a.result["S21"], g.result["S21"])) for a, g in zip(plain, got))
+    return {"requests": n, "rate_per_s": rate, "same_results": same, "plain_fifo": sp, "served": ss,
+            "gpu_busy_s": srv.gpu_ms / 1e3,
+            "solves_per_hour_vs_plain": ss["solves_per_hour"] / sp["solves_per_hour"] if sp["solves_per_hour"] else None}
+
+
 def run_b200(args) -> None:
     import torch
     import torch.distributed as dist
@@ -280,6 +374,14 @@ def run_b200(args) -> None:
                "steps": n_chunks, "time_steps": n_chunks * chunk,
                "note": "first step uploads plan and state (device_bytes); spectra and energy read after every step"}
 
+    batching = serving = None
+    if rank == 0 and world == 1 and args.batch_runs > 0:
+        log("batching comparison ...")
+        batching = batch_compare(lib, args.batch_runs)
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        log("serving comparison ...")
+        serving = serve_compare(lib, args.serve_requests, args.serve_rate)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         oracle = _oracle()
@@ -308,6 +410,8 @@ def run_b200(args) -> None:
             "e2e": e2e,
             "cpu_baseline": cpu,
             "gpu_launches": launches,
+            "batching": batching,
+            "serving": serving,
         }
         print(json.dumps(line))
     if world > 1:
@@ -328,6 +432,9 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-runs", type=int, default=16, help="runs in the batched-vs-plain comparison (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=12, help="requests in the serving comparison (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=8.0, help="request arrival rate of the serving comparison, 1/s")
     args = ap.parse_args()
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
     if args.impl == "reference":
