@@ -284,29 +284,51 @@ def serve_compare(lib, n: int, rate: float, seed: int = 7) -> dict:
             "solves_per_hour_vs_plain": ss["solves_per_hour"] / sp["solves_per_hour"] if sp["solves_per_hour"] else None}
 
 
+class Ranks:
+    """Replica plumbing of a multi-GPU run: one process per GPU, no collective
+    on the data path; a barrier around the timed region and the maximum of a
+    per-rank time (nccl on GPUs; gloo works the same way on CPU)."""
+
+    def __init__(self, world: int, backend: str = "nccl", device: str = "cuda"):
+        import torch.distributed as dist
+        self.world, self.device, self.dist = world, device, dist
+        if world > 1 and not dist.is_initialized():
+            import datetime
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.world == 1:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+def replica_rate(world: int, cells: int, time_steps: int, max_ms: float) -> float:
+    """Whole-job cell-updates/s of `world` replicas that each advanced `cells`
+    cells by `time_steps` steps, timed by the slowest rank."""
+    return world * cells * time_steps / (max_ms / 1e3)
+
+
 def run_b200(args) -> None:
     import torch
-    import torch.distributed as dist
     from courant_b200.api import Courant
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(world)
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     lib = Courant()
     lib.selectDevice(local)
@@ -325,7 +347,7 @@ def run_b200(args) -> None:
         barrier()
     gpu_ms = max_over_ranks(gpu_ms)
     cells = meta["cells"]
-    value = world * cells * chunk * args.steps / (gpu_ms / 1e3)
+    value = replica_rate(world, cells, chunk * args.steps, gpu_ms)
 
     # per-kernel device time (event pair per launch) for the roofline
     prof = s.profileSteps(args.profile_steps)
@@ -414,8 +436,7 @@ def run_b200(args) -> None:
             "serving": serving,
         }
         print(json.dumps(line))
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 def main() -> None:
