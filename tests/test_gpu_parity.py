@@ -211,6 +211,12 @@ def test_gcpw_lumped_sparams(lib, oracle_lib, fused):
         sel = (f >= 1e9) & (np.abs(r) > 0.01)
         ddb, ddeg = db_deg(g[sel], r[sel])
         assert ddb.max() < 1e-3 and ddeg.max() < 0.01, (ddb.max(), ddeg.max())
+    # the same gate through Touchstone files, as a user would compare them
+    from courant_b200 import touchstone
+    a = touchstone.write_s2p(None, f, g11, g21, title="gcpw b200")
+    b = touchstone.write_s2p(None, f, r11, r21, title="gcpw oracle")
+    cmp = touchstone.compare(touchstone.read_s2p(a), touchstone.read_s2p(b), "b200")
+    assert cmp["ok"], cmp
 
 
 @pytest.mark.parametrize("prog", ["test_checkpoint", "test_mode2d", "test_cavity", "test_cpml", "test_sibc"])
