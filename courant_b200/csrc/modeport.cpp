@@ -11,6 +11,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #ifndef M_PI
@@ -101,6 +102,49 @@ namespace {
 // f0 and seeding each solve with the previous mode so the same mode is
 // tracked; kappa -> beta by the arcsine mapping of the leapfrog grid, Z0 from
 // the mode's own V and I. (reference modeport.c:146-201)
+//
+// The upward and the downward walk each start with a fresh solve at the
+// frequency nearest f0 and share nothing else, so they run on two threads,
+// each with its own cross-section; the downward walk keeps the port's own
+// cross-section, which ends on the lowest frequency's mode as in a walk up
+// then down. Both walks compute the starting frequency alike; the upward
+// one stores it.
+int port_sweep(const cem_sim *s, ModePort &p, cem_mode2d *xs, int q0, int stepq) {
+    const int nf = s->nf;
+    const cem_mode_port_def &d = p.def;
+    const int ny = d.j1 - d.j0, nz = d.k1 - d.k0;
+    const int nst = ny * (nz + 1) + (ny + 1) * nz;
+    std::vector<double> start(2 * (size_t)nst);
+    const double dx = s->d[0][d.i_mon];
+    cem_mode2d_solve(xs, warp(s, s->freq[q0]), d.neff0, nullptr, 300, 1e-13);
+    for (int q = q0; q >= 0 && q < nf; q += stepq) {
+        const double fw = warp(s, s->freq[q]);
+        const double ng = cem_mode2d_beta(xs) / (2 * M_PI * mode_freq_hint(xs) / CEM_C0);
+        std::memcpy(start.data(), cem_mode2d_eu(xs), 2 * ny * (nz + 1) * sizeof(double));
+        std::memcpy(start.data() + 2 * ny * (nz + 1), cem_mode2d_ev(xs), 2 * (ny + 1) * nz * sizeof(double));
+        if (cem_mode2d_solve(xs, fw, ng, start.data(), 300, 1e-13)) return -1;
+        if (stepq < 0 && q == q0) continue;
+        const cplx kc = cem_mode2d_beta(xs) - cplx(0.0, 1.0) * cem_mode2d_alpha(xs);
+        const cplx b3 = 2 / dx * std::asin(kc * dx / 2.0);
+        p.kappa[2 * q] = std::real(kc); p.kappa[2 * q + 1] = std::imag(kc);
+        p.beta[q] = std::real(b3);
+        p.alpha[q] = -std::imag(b3);
+        if (s->sibc_on) {
+            double zr, zi;
+            cem_conductor_zs(s, s->freq[q], &zr, &zi);
+            p.alpha_c[q] = cem_mode2d_conductor_alpha(xs, zr);
+            p.alpha[q] += p.alpha_c[q];
+        }
+        double V[2], Iv[2];
+        cem_mode2d_vi(xs, d.vj - d.j0, d.vk0 - d.k0, d.vk1 - d.k0, d.ja - d.j0, d.jb - d.j0, d.ka - d.k0, d.kb - d.k0,
+                      V, Iv);
+        // cem_mode2d_vi returns -sum Ez dz; the port voltage is vsign * sum Ez dz
+        const cplx Z = (double)(-d.vsign) * cplx(V[0], V[1]) / cplx(Iv[0], Iv[1]);
+        p.z0[2 * q] = std::real(Z); p.z0[2 * q + 1] = std::imag(Z);
+    }
+    return 0;
+}
+
 int solve_port_modes(cem_sim *s, ModePort &p) {
     const int nf = s->nf;
     const cem_mode_port_def &d = p.def;
@@ -109,45 +153,36 @@ int solve_port_modes(cem_sim *s, ModePort &p) {
     p.alpha.assign(nf, 0.0);
     p.kappa.assign(2 * nf, 0.0);
     p.alpha_c.assign(nf, 0.0);
-    const int ny = d.j1 - d.j0, nz = d.k1 - d.k0;
-    const int nst = ny * (nz + 1) + (ny + 1) * nz;
-    std::vector<double> start(2 * (size_t)nst);
-    const double dx = s->d[0][d.i_mon];
     int q0 = 0;
     for (int q = 0; q < nf; q++)
         if (std::fabs(s->freq[q] - d.f0) < std::fabs(s->freq[q0] - d.f0)) q0 = q;
-    for (int pass = 0; pass < 2; pass++) {
-        cem_mode2d_solve(p.xs, warp(s, s->freq[q0]), d.neff0, nullptr, 300, 1e-13);
-        const int stepq = pass == 0 ? 1 : -1;
-        for (int q = q0; q >= 0 && q < nf; q += stepq) {
-            const double fw = warp(s, s->freq[q]);
-            const double ng = cem_mode2d_beta(p.xs) / (2 * M_PI * mode_freq_hint(p.xs) / CEM_C0);
-            std::memcpy(start.data(), cem_mode2d_eu(p.xs), 2 * ny * (nz + 1) * sizeof(double));
-            std::memcpy(start.data() + 2 * ny * (nz + 1), cem_mode2d_ev(p.xs), 2 * (ny + 1) * nz * sizeof(double));
-            if (cem_mode2d_solve(p.xs, fw, ng, start.data(), 300, 1e-13)) {
-                set_error("mode port: eigenmode did not converge at an output frequency");
-                return -1;
-            }
-            const cplx kc = cem_mode2d_beta(p.xs) - cplx(0.0, 1.0) * cem_mode2d_alpha(p.xs);
-            const cplx b3 = 2 / dx * std::asin(kc * dx / 2.0);
-            p.kappa[2 * q] = std::real(kc); p.kappa[2 * q + 1] = std::imag(kc);
-            p.beta[q] = std::real(b3);
-            p.alpha[q] = -std::imag(b3);
-            if (s->sibc_on) {
-                double zr, zi;
-                cem_conductor_zs(s, s->freq[q], &zr, &zi);
-                p.alpha_c[q] = cem_mode2d_conductor_alpha(p.xs, zr);
-                p.alpha[q] += p.alpha_c[q];
-            }
-            double V[2], Iv[2];
-            cem_mode2d_vi(p.xs, d.vj - d.j0, d.vk0 - d.k0, d.vk1 - d.k0, d.ja - d.j0, d.jb - d.j0, d.ka - d.k0,
-                          d.kb - d.k0, V, Iv);
-            // cem_mode2d_vi returns -sum Ez dz; the port voltage is vsign * sum Ez dz
-            const cplx Z = (double)(-d.vsign) * cplx(V[0], V[1]) / cplx(Iv[0], Iv[1]);
-            p.z0[2 * q] = std::real(Z); p.z0[2 * q + 1] = std::imag(Z);
-        }
+    cem_mode2d *up = cem_cross_section_x(s, d.i_mon, d.j0, d.j1, d.k0, d.k1);
+    if (!up) return -1;
+    int rc_up = 0;
+    std::thread t([&] { rc_up = port_sweep(s, p, up, q0, 1); });
+    const int rc_down = port_sweep(s, p, p.xs, q0, -1);
+    t.join();
+    cem_mode2d_destroy(up);
+    if (rc_up || rc_down) {
+        set_error("mode port: eigenmode did not converge at an output frequency");
+        return -1;
     }
     p.solved = true;
+    return 0;
+}
+
+// the output-frequency modes of every mode port not solved yet, one thread per port
+int solve_all_ports(cem_sim *s) {
+    std::vector<std::thread> th;
+    std::vector<int> rc(s->mport.size(), 0);
+    for (size_t q = 0; q < s->mport.size(); q++)
+        if (!s->mport[q].solved) th.emplace_back([s, q, &rc] { rc[q] = solve_port_modes(s, s->mport[q]); });
+    for (auto &t : th) t.join();
+    for (int r : rc)
+        if (r) {
+            set_error("mode port: eigenmode did not converge at an output frequency");
+            return -1;
+        }
     return 0;
 }
 
@@ -196,7 +231,7 @@ int cem_set_mode_excitation(cem_sim *s, int port, double t0, double tau) {
 int cem_mode_port_waves(cem_sim *s, int port, double *a, double *b, double *z0, double *beta) {
     if (port < 0 || port >= (int)s->mport.size() || !s->finalized) { set_error("bad mode port"); return -1; }
     ModePort &p = s->mport[port];
-    if (!p.solved && solve_port_modes(s, p)) return -1;
+    if (!p.solved && solve_all_ports(s)) return -1;
     const double *V0 = cem_vprobe(s, p.vp0), *V1 = cem_vprobe(s, p.vp1), *Ix = cem_iprobe(s, p.ip);
     const cem_mode_port_def &d = p.def;
     const double dx = s->d[0][d.i_mon];
