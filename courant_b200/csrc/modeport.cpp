@@ -11,6 +11,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -45,9 +46,11 @@ void modeports_release(cem_sim *s) {
 
 // Solve each port's mode at f0 on the monitor-plane cross-section and turn
 // its transverse E into source weights on the i_src plane, oriented so the
-// source voltage is positive. (reference modeport.c:70-122)
-int modeports_finalize(cem_sim *s) {
-    for (ModePort &p : s->mport) {
+// source voltage is positive. (reference modeport.c:70-122) The ports are
+// independent and are solved on one thread each.
+namespace {
+int finalize_port(cem_sim *s, ModePort &p) {
+    {
         const cem_mode_port_def &d = p.def;
         p.xs = cem_cross_section_x(s, d.i_mon, d.j0, d.j1, d.k0, d.k1);
         if (!p.xs) return -1;
@@ -91,6 +94,26 @@ int modeports_finalize(cem_sim *s) {
         if (-V[0] * d.vsign < 0)
             for (double &w : p.src_w) w = -w;
     }
+    return 0;
+}
+}  // namespace
+
+int modeports_finalize(cem_sim *s) {
+    // errors are kept per thread: each port's message comes back with its return code
+    std::vector<int> rc(s->mport.size(), 0);
+    std::vector<std::string> msg(s->mport.size());
+    std::vector<std::thread> th;
+    for (size_t q = 0; q < s->mport.size(); q++)
+        th.emplace_back([s, q, &rc, &msg] {
+            rc[q] = finalize_port(s, s->mport[q]);
+            if (rc[q]) msg[q] = cem_last_error();
+        });
+    for (auto &t : th) t.join();
+    for (size_t q = 0; q < rc.size(); q++)
+        if (rc[q]) {
+            set_error(msg[q].c_str());
+            return -1;
+        }
     return 0;
 }
 
@@ -175,12 +198,17 @@ int solve_port_modes(cem_sim *s, ModePort &p) {
 int solve_all_ports(cem_sim *s) {
     std::vector<std::thread> th;
     std::vector<int> rc(s->mport.size(), 0);
+    std::vector<std::string> msg(s->mport.size());
     for (size_t q = 0; q < s->mport.size(); q++)
-        if (!s->mport[q].solved) th.emplace_back([s, q, &rc] { rc[q] = solve_port_modes(s, s->mport[q]); });
+        if (!s->mport[q].solved)
+            th.emplace_back([s, q, &rc, &msg] {
+                rc[q] = solve_port_modes(s, s->mport[q]);
+                if (rc[q]) msg[q] = cem_last_error();
+            });
     for (auto &t : th) t.join();
-    for (int r : rc)
-        if (r) {
-            set_error("mode port: eigenmode did not converge at an output frequency");
+    for (size_t q = 0; q < rc.size(); q++)
+        if (rc[q]) {
+            set_error(msg[q].c_str());
             return -1;
         }
     return 0;
