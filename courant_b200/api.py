@@ -144,6 +144,7 @@ _EXT_PROTOS = [
     ("cemx_release_device", _i, [_p]),
     ("cemx_use_fused", _i, [_p, _i]),
     ("cemx_energy_noalloc", _i, [_p, _dp]),
+    ("cemx_prepare_device", _i, [_p, _i]),
     ("cemx_batch_create", _p, [_i]),
     ("cemx_batch_destroy", None, [_p]),
     ("cemx_batch_add", _i, [_p, _p, _l]),
@@ -492,6 +493,10 @@ class Sim:
     def useFused(self, on: bool = True) -> bool:
         """Select the single-pass fused H+E kernel (True) or the separate kernels."""
         return bool(self.c.ex.cemx_use_fused(self.h, int(on)))
+
+    def prepareDevice(self, device: int = -1):
+        """Create the device state now rather than at the first step."""
+        self._check(self.c.ex.cemx_prepare_device(self.h, device), "prepare_device")
 
     def releaseDevice(self):
         self._check(self.c.ex.cemx_release_device(self.h), "release_device")

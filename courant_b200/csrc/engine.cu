@@ -2791,6 +2791,15 @@ int cemx_select_device(int device) {
     return 0;
 }
 
+int cemx_prepare_device(cem_sim *s, int device) {
+    if (!s || !s->finalized) { set_error("not finalized"); return -1; }
+    const int prev = g_selected_device;
+    if (device >= 0) g_selected_device = device;
+    const bool ok = begin_device_op(s) && end_device_op(s);
+    g_selected_device = prev;
+    return ok ? 0 : -1;
+}
+
 int cemx_release_device(cem_sim *s) {
     if (!s->dev) return 0;
     if (engine_pull(s, kGroupAll)) return -1;

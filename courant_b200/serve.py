@@ -2,11 +2,12 @@
 
 A `Server` accepts requests (a builder returning a finalized simulation, a
 step count) as they arrive. Builder threads do the host set-up (plan, mode
-solves) in parallel; the GPU thread admits built simulations into one
-`cemx_batch` while their estimated device footprint fits the HBM budget, runs
-the batch in chunks, and hands every simulation that reached its step count
-to finisher threads, which extract its S-parameters and free it, while the
-batch goes on with the others. Requests that arrive while others are on the
+solves) in parallel; the GPU thread admits built simulations while their
+estimated device footprint fits the HBM budget, loader threads create their
+device state (tables, uploads), and the GPU thread adds them to one
+`cemx_batch`, runs the batch in chunks, and hands every simulation that
+reached its step count to finisher threads, which extract its S-parameters
+and free it, while the batch goes on with the others. Requests that arrive while others are on the
 GPU join at the next chunk boundary, so their work overlaps on the device.
 Each simulation computes the same bits as when it runs alone.
 
@@ -87,7 +88,10 @@ class Server:
         self.used = 0
         self.finished: list[Request] = []
         self.build_pool = ThreadPoolExecutor(builders)
+        self.load_pool = ThreadPoolExecutor(2)
         self.finish_pool = ThreadPoolExecutor(finishers)
+        self.loaded: list = []         # admitted and on the device, waiting to join the batch
+        self.device = device
         self.stop = False
         self.gpu_ms = 0.0
         self.thread = threading.Thread(target=self._gpu_loop, daemon=True)
@@ -115,19 +119,38 @@ class Server:
         self.wake.set()
 
     # ---- the GPU thread
+    def _load(self, item):
+        r, sim, meta, nbytes = item
+        try:
+            sim.prepareDevice(self.device)
+            with self.lock:
+                self.loaded.append(item)
+        except Exception as e:
+            r.error = str(e)
+            sim.destroy()
+            with self.lock:
+                self.used -= nbytes
+            r.done = time.perf_counter()
+            r.event.set()
+        self.wake.set()
+
     def _admit(self):
         with self.lock:
             keep = []
             for item in self.built:
                 r, sim, meta, nbytes = item
                 if self.used + nbytes <= self.budget:
-                    self.batch.add(sim, r.steps)
-                    self.members[sim.h] = item
                     self.used += nbytes
                     r.admitted = time.perf_counter()
+                    self.load_pool.submit(self._load, item)
                 else:
                     keep.append(item)
             self.built = keep
+            ready, self.loaded = self.loaded, []
+        for item in ready:
+            r, sim, meta, nbytes = item
+            self.batch.add(sim, r.steps)
+            self.members[sim.h] = item
 
     def _finish(self, item):
         r, sim, meta, nbytes = item
@@ -164,6 +187,7 @@ class Server:
         self.wake.set()
         self.thread.join()
         self.build_pool.shutdown(wait=True)
+        self.load_pool.shutdown(wait=True)
         self.finish_pool.shutdown(wait=True)
         self.batch.destroy()
 

@@ -1,9 +1,11 @@
 /*
  * courant_b200.h - extensions of libcourant_b200 beyond courant.h.
  *
- * These entry points have no counterpart in the reference core: they expose
- * device-side timing and sizes of a simulation for benchmarking and
- * profiling. Everything else a caller needs is in courant.h.
+ * These entry points have no counterpart in the reference core: device-side
+ * timing and sizes for benchmarking and profiling, device selection and
+ * device-state control, the kernel choice, an energy evaluation that
+ * allocates nothing, and batches of simulations advanced together. Everything
+ * else a caller needs is in courant.h.
  */
 #ifndef COURANT_B200_H
 #define COURANT_B200_H
@@ -37,6 +39,12 @@ CEM_API int cemx_sizes(const cem_sim *s, long long *out, int n);
 /* CUDA device on which simulations created (first stepped) afterwards by
  * this thread will live; default: the current device. Returns 0 or -1. */
 CEM_API int cemx_select_device(int device);
+
+/* Create the device state of s now (plan tables, fields, uploads) on CUDA
+ * device `device` (-1: the thread's selected or current device), instead of at
+ * its first step; lets a caller move this host work off a thread that keeps
+ * the GPU busy. Returns 0 or -1. */
+CEM_API int cemx_prepare_device(cem_sim *s, int device);
 
 /* Copy the time-dependent state of s to the host and release its device
  * memory; the next device operation uploads plan and state again. Returns 0
