@@ -107,7 +107,6 @@ struct StepArgs {
     const unsigned short *mat[3];
     const float *tab[3];          // field-major: ca-1, cb, cs, beta_p/dt (p = 0..P-1)
     const float4 *tab4[3];        // packed per entry: ca-1, cb, cs, flags (bit pattern)
-    const unsigned char *tflag[3];
     int ntab[3];
     int npole;
     float omk[kMaxPoles], hk[kMaxPoles];
@@ -1334,7 +1333,6 @@ struct Device {
     DevBuf<unsigned short> mat[3];
     DevBuf<float> tab[3];
     DevBuf<float4> tab4[3];
-    DevBuf<unsigned char> tflag[3];
     DevBuf<double> cb64[3];
     int ntab[3] = {0, 0, 0};
     DevBuf<float> J[3];
@@ -1572,7 +1570,6 @@ bool build_tables(cem_sim *s, Device &D) {
         D.ntab[c] = (int)tb.flags.size();
         if (!dev_upload(s, D.mat[c], mat)) return false;
         if (!dev_upload(s, D.tab[c], tb.field_major())) return false;
-        if (!dev_upload(s, D.tflag[c], tb.flags)) return false;
         {
             const size_t ne = tb.flags.size();
             std::vector<float4> packed(ne);
@@ -1840,7 +1837,6 @@ void fill_args_for(cem_sim *s, Device &D, int cur) {
         }
         a.mat[c] = D.mat[c].p;
         a.tab[c] = D.tab[c].p;
-        a.tflag[c] = D.tflag[c].p;
         a.tab4[c] = D.tab4[c].p;
         a.ntab[c] = D.ntab[c];
         a.J[c] = D.J[c].p;
