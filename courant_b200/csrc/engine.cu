@@ -94,9 +94,26 @@ struct KSegs {
     unsigned long long magic[kMaxSegs];   // row of segment thread t: (t * magic) >> 40
 };
 
+// The fast pieces of the update kernels: runs of blocks of the k-segment
+// layout in which no point of any component has a CPML auxiliary on a
+// derivative axis or (E) a Debye current, on every node plane of [p0, p1).
+// Piece q covers segment-linear threads [t0, t0 + nt) (thread t: row
+// t / nk4, 4-point group t % nk4) of the segment [ks, ke); the fast kernels
+// walk the pieces on a (blocks, planes) grid, the general blocks go to a
+// work-list.
+struct FastSegs {
+    int n;
+    int ks[kMaxSegs], ke[kMaxSegs];
+    int t0[kMaxSegs], nt[kMaxSegs];
+    int blk[kMaxSegs + 1];                // first block of each piece; blk[n]: blocks per plane and component
+    unsigned long long magic[kMaxSegs];   // row of thread t: (t * magic) >> 40
+    int p0, p1;
+};
+
 struct StepArgs {
     Geom g;
     KSegs seg_h, seg_e;
+    FastSegs fast_h, fast_e;
     float *E[3], *H[3];
     const float *hc[3];      // dt/mu0 * idh per axis (cells)
     const float *ec[3];      // ide per axis (nodes)
@@ -587,8 +604,10 @@ __device__ __forceinline__ void h_points(const StepArgs &a, int i, int j, int k4
     if (any2) st4(a.psiH[C][1] + x2, s2);
 }
 
-// H component C on points k4 .. k4+3 of row (i, j) (segment [ks, ke))
-template <int C>
+// H component C on points k4 .. k4+3 of row (i, j) (segment [ks, ke)).
+// FAST: the block lies where no point has a CPML auxiliary (short path only,
+// fewer registers); the arithmetic is the same.
+template <int C, bool FAST>
 __device__ __forceinline__ void h_vec(const StepArgs &a, int i, const RowPos &r) {
     const int j = r.j, k4 = r.k4;
     const int m = j * a.g.sj + k4;
@@ -596,7 +615,7 @@ __device__ __forceinline__ void h_vec(const StepArgs &a, int i, const RowPos &r)
     const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
     // derivative axes x and y need i < nx, j < ny (the row's own axis goes to n)
     const bool valid = r.act && (!(A1 == 0 || A2 == 0) || i < nx) && (!(A1 == 1 || A2 == 1) || j < ny);
-    const Where w = valid ? h_where<C>(a, i, j, k4) : Where{-1, -1, make_int4(-1, -1, -1, -1), -1, false};
+    const Where w = valid && !FAST ? h_where<C>(a, i, j, k4) : Where{-1, -1, make_int4(-1, -1, -1, -1), -1, false};
     const bool row = valid;
     const int q = i * (int)a.g.si + m;
     const float *__restrict__ E2 = a.E[A2];
@@ -738,8 +757,9 @@ __device__ __forceinline__ void e_points(const StepArgs &a, int i, int j, int k4
     }
 }
 
-// E component C on points k4 .. k4+3 of row (i, j) (segment [ks, ke))
-template <int C, int P>
+// E component C on points k4 .. k4+3 of row (i, j) (segment [ks, ke));
+// FAST as for h_vec: no CPML auxiliary and no Debye current in the block.
+template <int C, int P, bool FAST>
 __device__ __forceinline__ void e_vec(const StepArgs &a, int i, const RowPos &r, const float2 sv) {
     const int j = r.j, k4 = r.k4;
     const int m = j * a.g.sj + k4;
@@ -747,7 +767,7 @@ __device__ __forceinline__ void e_vec(const StepArgs &a, int i, const RowPos &r,
     const int nx = a.g.n[0], ny = a.g.n[1];
     // own axis: index < n; transverse axes: 1 <= index < n
     const bool valid = r.act && i < nx && (C == 0 || i >= 1) && (C == 1 ? j < ny : (j >= 1 && j < ny));
-    const Where w = valid ? e_where<C, P>(a, i, j, k4) : Where{-1, -1, make_int4(-1, -1, -1, -1), -1, false};
+    const Where w = valid && !FAST ? e_where<C, P>(a, i, j, k4) : Where{-1, -1, make_int4(-1, -1, -1, -1), -1, false};
     const bool row = valid;
     const int q = i * (int)a.g.si + m;
     const float *__restrict__ H2 = a.H[A2];
@@ -773,6 +793,117 @@ __device__ __forceinline__ void e_vec(const StepArgs &a, int i, const RowPos &r,
     e_points<C, P>(a, i, j, k4, E + q, w, h2, h2m, h1, h1m, ev, mv, sv);
 }
 
+// Position of this thread in the fast pieces f (block bx of the plane):
+// row j, first point k4, its segment's k range, and whether the next lane
+// holds the next four points of the same row (`cont`).
+struct LeanPos {
+    int j, k4, ks, ke;
+    bool act, cont;
+};
+
+__device__ __forceinline__ LeanPos lean_pos(const FastSegs &f, int bx) {
+    int q = 0;
+    while (q + 1 < f.n && bx >= f.blk[q + 1]) q++;
+    const int tl = (bx - f.blk[q]) * kBlock + threadIdx.x;
+    LeanPos p;
+    p.act = tl < f.nt[q];
+    const int t = f.t0[q] + (p.act ? tl : f.nt[q] - 1);
+    p.ks = f.ks[q];
+    p.ke = f.ke[q];
+    const int nk4 = (p.ke - p.ks) >> 2;
+    p.j = (int)(((unsigned long long)t * f.magic[q]) >> 40);
+    p.k4 = p.ks + 4 * (t - p.j * nk4);
+    p.cont = (threadIdx.x & 31) != 31 && p.k4 + 4 < p.ke && tl + 1 < f.nt[q];
+    return p;
+}
+
+// H component C at points k4 .. k4+3 of row (i, j) of a fast piece: the
+// short path of h_points (no auxiliaries), every rounding the same. All
+// lanes of the warp call it (the k+1 neighbours move by shuffle).
+template <int C>
+__device__ __forceinline__ void h_lean(const StepArgs &a, int i, const LeanPos &p) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    constexpr bool kz = A1 == 2 || A2 == 2;
+    const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
+    const int j = p.j, k4 = p.k4;
+    const bool row = p.act && (!(A1 == 0 || A2 == 0) || i < nx) && (!(A1 == 1 || A2 == 1) || j < ny);
+    const int q = i * (int)a.g.si + j * a.g.sj + k4;
+    const float *__restrict__ E2 = a.E[A2];
+    const float *__restrict__ E1 = a.E[A1];
+    float *__restrict__ H = a.H[C];
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 e2 = z4, e1 = z4, h = z4, e2n = z4, e1n = z4;
+    if (row) {
+        e2 = ldg4(E2 + q);
+        e1 = ldg4(E1 + q);
+        h = ld4(H + q);
+        if (A1 != 2) e2n = ldg4(E2 + q + stride_of<A1>(a));
+        if (A2 != 2) e1n = ldg4(E1 + q + stride_of<A2>(a));
+    }
+    if (A1 == 2) e2n = next_k(e2, E2 + q, row && k4 + 4 <= nz, !p.cont);
+    if (A2 == 2) e1n = next_k(e1, E1 + q, row && k4 + 4 <= nz, !p.cont);
+    if (!row) return;
+    const float ci = __ldg(a.hc[0] + i), cj = __ldg(a.hc[1] + j);
+    const float4 ck = ldg4(a.hc[2] + k4);
+    float s = 0.f;
+    float4 r = h;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int k = k4 + e;
+        const float c[3] = {ci, cj, lane4(ck, e)};
+        const float v = h_value<C>(a, i, j, k, lane4(h, e), __fsub_rn(lane4(e2n, e), lane4(e2, e)),
+                                   __fsub_rn(lane4(e1n, e), lane4(e1, e)), c[A1], c[A2], false, false, s, s);
+        if (kz ? k < nz : k <= nz) set4(r, e, v);
+    }
+    st4(H + q, r);
+}
+
+// E component C at points k4 .. k4+3 of row (i, j) of a fast piece: the
+// short path of e_points (material table, sources; no auxiliaries, no Debye
+// currents), every rounding the same
+template <int C>
+__device__ __forceinline__ void e_lean(const StepArgs &a, int i, const LeanPos &p, const float2 sv) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    const int ny = a.g.n[1], nz = a.g.n[2];
+    const int j = p.j, k4 = p.k4;
+    const bool row = p.act && (C == 0 || i >= 1) && (C == 1 ? j < ny : (j >= 1 && j < ny));
+    const int q = i * (int)a.g.si + j * a.g.sj + k4;
+    const float *__restrict__ H2 = a.H[A2];
+    const float *__restrict__ H1 = a.H[A1];
+    float *__restrict__ E = a.E[C];
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 h2 = z4, h1 = z4, ev = z4, h2m = z4, h1m = z4;
+    uint2 mv = make_uint2(0, 0);
+    if (row) {
+        h2 = ldg4(H2 + q);
+        h1 = ldg4(H1 + q);
+        ev = ld4(E + q);
+        mv = __ldg(reinterpret_cast<const uint2 *>(a.mat[C] + q));
+        if (A1 != 2) h2m = ldg4(H2 + q - stride_of<A1>(a));
+        if (A2 != 2) h1m = ldg4(H1 + q - stride_of<A2>(a));
+    }
+    // the previous lane holds the previous four points unless this lane starts a warp or a row
+    const bool first = (threadIdx.x & 31) == 0 || k4 == p.ks;
+    if (A1 == 2) h2m = prev_k(h2, H2 + q, row && k4 > 0, first);
+    if (A2 == 2) h1m = prev_k(h1, H1 + q, row && k4 > 0, first);
+    if (!row) return;
+    const float ci = __ldg(a.ec[0] + i), cj = __ldg(a.ec[1] + j);
+    const float4 ck = ldg4(a.ec[2] + k4);
+    const int mi[4] = {(int)(mv.x & 0xffffu), (int)(mv.x >> 16), (int)(mv.y & 0xffffu), (int)(mv.y >> 16)};
+    float s = 0.f;
+    float4 r = ev;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int k = k4 + e;
+        const float4 t = __ldg(a.tab4[C] + mi[e]);
+        const float c[3] = {ci, cj, lane4(ck, e)};
+        const float v = e_value<C>(a, t, i, j, k, sv, lane4(ev, e), __fsub_rn(lane4(h2, e), lane4(h2m, e)),
+                                   __fsub_rn(lane4(h1, e), lane4(h1m, e)), c[A1], c[A2], false, false, s, s, 0.f);
+        if (C == 2 ? k < nz : (k >= 1 && k < nz)) set4(r, e, v);
+    }
+    st4(E + q, r);
+}
+
 // H over node planes [i0, i0 + gridDim.y) (cem_mt_H and the unfused step)
 // Resident blocks per SM the update kernels are compiled for (register caps
 // of 51 and 64 per thread at the default 5 and 4: occupancy hides the
@@ -784,25 +915,56 @@ __device__ __forceinline__ void e_vec(const StepArgs &a, int i, const RowPos &r,
 #define CB2_E_MINBLOCKS 4
 #endif
 
-__global__ void __launch_bounds__(kBlock, CB2_H_MINBLOCKS) k_update_h(const StepArgs a, int i0) {
+#ifndef CB2_HF_MINBLOCKS
+#define CB2_HF_MINBLOCKS 8
+#endif
+#ifndef CB2_EF_MINBLOCKS
+#define CB2_EF_MINBLOCKS 5
+#endif
+
+// H on the fast pieces of node planes [i0, i0 + gridDim.y); block x: piece
+// block x / 3, component x % 3
+__global__ void __launch_bounds__(kBlock, CB2_HF_MINBLOCKS) k_update_h_fast(const StepArgs a, int i0) {
     const int comp = blockIdx.x % 3;
-    const RowPos r = row_pos(a.seg_h, a.g.n[1] + 1, blockIdx.x / 3);
+    const LeanPos p = lean_pos(a.fast_h, blockIdx.x / 3);
     const int i = i0 + blockIdx.y;
-    if (comp == 0) h_vec<0>(a, i, r);
-    else if (comp == 1) h_vec<1>(a, i, r);
-    else h_vec<2>(a, i, r);
+    if (comp == 0) h_lean<0>(a, i, p);
+    else if (comp == 1) h_lean<1>(a, i, p);
+    else h_lean<2>(a, i, p);
 }
 
-// E over node planes [i0, i0 + gridDim.y) (cem_mt_E and the unfused step)
-template <int P>
-__global__ void __launch_bounds__(kBlock, CB2_E_MINBLOCKS) k_update_e(const StepArgs a, int i0) {
+// E on the fast pieces of node planes [i0, i0 + gridDim.y)
+__global__ void __launch_bounds__(kBlock, CB2_EF_MINBLOCKS) k_update_e_fast(const StepArgs a, int i0) {
     const int comp = blockIdx.x % 3;
-    const RowPos r = row_pos(a.seg_e, a.g.n[1] + 1, blockIdx.x / 3);
+    const LeanPos p = lean_pos(a.fast_e, blockIdx.x / 3);
     const int i = i0 + blockIdx.y;
     const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
-    if (comp == 0) e_vec<0, P>(a, i, r, sv);
-    else if (comp == 1) e_vec<1, P>(a, i, r, sv);
-    else e_vec<2, P>(a, i, r, sv);
+    if (comp == 0) e_lean<0>(a, i, p, sv);
+    else if (comp == 1) e_lean<1>(a, i, p, sv);
+    else e_lean<2>(a, i, p, sv);
+}
+
+// Work entry of the general blocks: x node plane, y block of the plane
+// (component y % 3, block y / 3 of the k-segment layout).
+__global__ void __launch_bounds__(kBlock, CB2_H_MINBLOCKS) k_update_h(const StepArgs a, const int2 *work) {
+    const int2 w = work[blockIdx.x];
+    const int comp = w.y % 3;
+    const RowPos r = row_pos(a.seg_h, a.g.n[1] + 1, w.y / 3);
+    if (comp == 0) h_vec<0, false>(a, w.x, r);
+    else if (comp == 1) h_vec<1, false>(a, w.x, r);
+    else h_vec<2, false>(a, w.x, r);
+}
+
+// E over the general blocks (P Debye poles)
+template <int P>
+__global__ void __launch_bounds__(kBlock, CB2_E_MINBLOCKS) k_update_e(const StepArgs a, const int2 *work) {
+    const int2 w = work[blockIdx.x];
+    const int comp = w.y % 3;
+    const RowPos r = row_pos(a.seg_e, a.g.n[1] + 1, w.y / 3);
+    const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
+    if (comp == 0) e_vec<0, P, false>(a, w.x, r, sv);
+    else if (comp == 1) e_vec<1, P, false>(a, w.x, r, sv);
+    else e_vec<2, P, false>(a, w.x, r, sv);
 }
 
 constexpr unsigned kWaitLimit = 1u << 24;
@@ -1010,7 +1172,7 @@ __global__ void __launch_bounds__(kFT, 3) k_step_fused(const StepArgs a, const F
 }
 
 // launchers of the pole-count instantiations
-using EKernel = void (*)(StepArgs, int);
+using EKernel = void (*)(StepArgs, const int2 *);
 using HKernel = void (*)(StepArgs, int);
 using FKernel = void (*)(StepArgs, FusedArgs, TmaMaps);
 #define CB2_POLES(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
@@ -1187,32 +1349,35 @@ __device__ __forceinline__ const T &stage_args(const T *src, unsigned *buf) {
 }
 
 // work entry: x simulation, y block of the plane (component = y % 3), z node plane
-__global__ void __launch_bounds__(kBlock, CB2_H_MINBLOCKS) k_batch_h(const StepArgs *args, const int4 *work) {
+template <bool FAST>
+__global__ void __launch_bounds__(kBlock, FAST ? CB2_HF_MINBLOCKS : CB2_H_MINBLOCKS)
+    k_batch_h(const StepArgs *args, const int4 *work) {
     __shared__ unsigned buf[sizeof(StepArgs) / 4];
     const int4 w = work[blockIdx.x];
     const StepArgs &a = stage_args(args + w.x, buf);
     const RowPos r = row_pos(a.seg_h, a.g.n[1] + 1, w.y / 3);
     const int comp = w.y % 3;
-    if (comp == 0) h_vec<0>(a, w.z, r);
-    else if (comp == 1) h_vec<1>(a, w.z, r);
-    else h_vec<2>(a, w.z, r);
+    if (comp == 0) h_vec<0, FAST>(a, w.z, r);
+    else if (comp == 1) h_vec<1, FAST>(a, w.z, r);
+    else h_vec<2, FAST>(a, w.z, r);
 }
 
-template <int P>
-__global__ void __launch_bounds__(kBlock, CB2_E_MINBLOCKS) k_batch_e(const StepArgs *args, const int4 *work) {
+template <int P, bool FAST>
+__global__ void __launch_bounds__(kBlock, FAST ? CB2_EF_MINBLOCKS : CB2_E_MINBLOCKS)
+    k_batch_e(const StepArgs *args, const int4 *work) {
     __shared__ unsigned buf[sizeof(StepArgs) / 4];
     const int4 w = work[blockIdx.x];
     const StepArgs &a = stage_args(args + w.x, buf);
     const RowPos r = row_pos(a.seg_e, a.g.n[1] + 1, w.y / 3);
     const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
     const int comp = w.y % 3;
-    if (comp == 0) e_vec<0, P>(a, w.z, r, sv);
-    else if (comp == 1) e_vec<1, P>(a, w.z, r, sv);
-    else e_vec<2, P>(a, w.z, r, sv);
+    if (comp == 0) e_vec<0, P, FAST>(a, w.z, r, sv);
+    else if (comp == 1) e_vec<1, P, FAST>(a, w.z, r, sv);
+    else e_vec<2, P, FAST>(a, w.z, r, sv);
 }
 
 using BEKernel = void (*)(const StepArgs *, const int4 *);
-#define CB2_BE(p) k_batch_e<p>,
+#define CB2_BE(p) k_batch_e<p, false>,
 const BEKernel kBEKernels[] = {CB2_BE(0) CB2_BE(1) CB2_BE(2) CB2_BE(3) CB2_BE(4) CB2_BE(5) CB2_BE(6) CB2_BE(7) CB2_BE(8)
                                    CB2_BE(9) CB2_BE(10) CB2_BE(11) CB2_BE(12) CB2_BE(13) CB2_BE(14) CB2_BE(15)
                                        CB2_BE(16)};
@@ -1338,6 +1503,15 @@ struct Device {
     DevBuf<float> J[3];
     int jbox[3][6] = {};
     KSegs seg_h{}, seg_e{};
+    // Update kernels [H, E]: the fast pieces, and the work-list of the
+    // general blocks, entries (node plane, block of the plane incl.
+    // component) in plane order; wl_start[u][i] is the first entry of plane
+    // i. gen_blk[u][i * blocks[u] + b]: block b of plane i is general.
+    FastSegs fast[2]{};
+    DevBuf<int2> wl[2];
+    std::vector<int> wl_start[2];
+    std::vector<unsigned char> gen_blk[2];
+    int blocks[2] = {0, 0};
     DevBuf<float> wsrc[2];
     // SIBC
     DevBuf<unsigned char> sb_ecomp;
@@ -1803,6 +1977,111 @@ bool build_segments(cem_sim *s, Device &D) {
     return make_segments(s, ch, D.seg_h) && make_segments(s, ce, D.seg_e);
 }
 
+// Which blocks of the update kernels may meet a CPML auxiliary on a
+// derivative axis or (E) a Debye current: a block (node plane i, block b of
+// a k segment, all three components) is general when plane i lies in an x
+// slab, its segment reaches a z slab, one of its rows lies in a y slab, or
+// (E) it overlaps a component's Debye box. The other blocks run the short
+// path only, in kernels compiled without the general one.
+bool build_worklists(cem_sim *s, Device &D) {
+    const int nx = s->n[0], ny = s->n[1], nz = s->n[2];
+    const int rows = ny + 1;
+    auto slab = [&](int a, int is_e, int idx) {
+        if (!s->has_pml) return false;
+        int r[2][2];
+        pml_ranges(s, a, is_e, r);
+        if (idx >= s->n[a] && !is_e) return false;   // cells end at n-1
+        for (int sd = 0; sd < 2; sd++)
+            if (idx >= r[sd][0] && idx <= r[sd][1]) return true;
+        return false;
+    };
+    for (int u = 0; u < 2; u++) {
+        const KSegs &sg = u ? D.seg_e : D.seg_h;
+        const int planes = u ? nx : nx + 1;
+        const int nb = sg.blk[sg.n];
+        D.blocks[u] = nb;
+        std::vector<unsigned char> gen((size_t)planes * nb, 0);
+        for (int q = 0; q < sg.n; q++) {
+            const int ks = sg.k[q], ke = sg.k[q + 1], nk4 = (ke - ks) / 4;
+            bool zs = false;
+            for (int k = ks; k < ke; k++) zs = zs || slab(2, u, k);
+            for (int b = sg.blk[q]; b < sg.blk[q + 1]; b++) {
+                const long long t0 = (long long)(b - sg.blk[q]) * kBlock;
+                const long long t1 = std::min<long long>(t0 + kBlock, (long long)rows * nk4);
+                const int j0 = (int)(t0 / nk4), j1 = (int)((t1 - 1) / nk4);
+                bool ys = false;
+                for (int j = j0; j <= j1; j++) ys = ys || slab(1, u, j);
+                for (int i = 0; i < planes; i++) {
+                    bool g = zs || ys || slab(0, u, i);
+                    for (int c = 0; u && c < 3 && !g; c++) {
+                        const int *bx = D.jbox[c];
+                        if (bx[3] * bx[4] * bx[5] == 0) continue;
+                        g = i >= bx[0] && i < bx[0] + bx[3] && j1 >= bx[1] && j0 < bx[1] + bx[4] && ke > bx[2] &&
+                            ks < bx[2] + bx[5];
+                    }
+                    gen[(size_t)i * nb + b] = g;
+                }
+            }
+        }
+        // fast planes: the longest run of planes outside the x slabs; fast
+        // blocks: general on none of them; pieces: runs of fast blocks
+        int p0 = 0, p1 = 0;
+        for (int i = 0; i < planes;) {
+            if (slab(0, u, i)) { i++; continue; }
+            int e = i;
+            while (e < planes && !slab(0, u, e)) e++;
+            if (e - i > p1 - p0) { p0 = i; p1 = e; }
+            i = e;
+        }
+        std::vector<unsigned char> fastb(nb, p1 > p0);
+        for (int b = 0; b < nb; b++)
+            for (int i = p0; i < p1 && fastb[b]; i++) fastb[b] = !gen[(size_t)i * nb + b];
+        FastSegs f{};
+        f.p0 = p0;
+        f.p1 = p1;
+        int fb = 0;
+        for (int q = 0; q < sg.n; q++) {
+            const long long nthr = (long long)rows * ((sg.k[q + 1] - sg.k[q]) / 4);
+            for (int b = sg.blk[q]; b < sg.blk[q + 1];) {
+                if (!fastb[b]) { b++; continue; }
+                int e = b;
+                while (e < sg.blk[q + 1] && fastb[e]) e++;
+                if (f.n == kMaxSegs) {   // no room for another piece: these blocks stay general
+                    std::fill(fastb.begin() + b, fastb.begin() + e, 0);
+                } else {
+                    const long long t0 = (long long)(b - sg.blk[q]) * kBlock;
+                    f.ks[f.n] = sg.k[q];
+                    f.ke[f.n] = sg.k[q + 1];
+                    f.t0[f.n] = (int)t0;
+                    f.nt[f.n] = (int)(std::min<long long>((long long)(e - sg.blk[q]) * kBlock, nthr) - t0);
+                    f.magic[f.n] = sg.magic[q];
+                    f.blk[f.n] = fb;
+                    fb += e - b;
+                    f.n++;
+                }
+                b = e;
+            }
+        }
+        f.blk[f.n] = fb;
+        for (int i = 0; i < planes; i++)
+            for (int b = 0; b < nb; b++) gen[(size_t)i * nb + b] = !(i >= p0 && i < p1 && fastb[b]);
+        std::vector<int2> wl;
+        std::vector<int> &st = D.wl_start[u];
+        st.assign(planes + 1, 0);
+        for (int i = 0; i < planes; i++) {
+            st[i] = (int)wl.size();
+            for (int b = 0; b < nb; b++)
+                if (gen[(size_t)i * nb + b])
+                    for (int c = 0; c < 3; c++) wl.push_back(make_int2(i, 3 * b + c));
+        }
+        st[planes] = (int)wl.size();
+        if (!wl.empty() && !dev_upload(s, D.wl[u], wl)) return false;
+        D.fast[u] = f;
+        D.gen_blk[u] = std::move(gen);
+    }
+    return true;
+}
+
 bool build_sources(cem_sim *s, Device &D) {
     const size_t plane = (size_t)(s->n[1] + 1) * (s->n[2] + 1);
     if (s->msrc >= 0) {
@@ -1824,6 +2103,8 @@ void fill_args_for(cem_sim *s, Device &D, int cur) {
     a.g = D.g;
     a.seg_h = D.seg_h;
     a.seg_e = D.seg_e;
+    a.fast_h = D.fast[0];
+    a.fast_e = D.fast[1];
     for (int c = 0; c < 3; c++) {
         a.E[c] = D.E[cur][c].p;
         a.H[c] = D.H[cur][c].p;
@@ -1995,7 +2276,7 @@ bool create_device_impl(cem_sim *s) {
         if (!dev_upload(s, D.d64[c], s->d[c]) || !dev_upload(s, D.dd64[c], s->dd[c])) return false;
     }
     if (!build_pml(s, D) || !build_tables(s, D) || !build_probes(s, D) || !build_sibc(s, D) || !build_sources(s, D) ||
-        !build_segments(s, D))
+        !build_segments(s, D) || !build_worklists(s, D))
         return false;
     for (int b = 0; b < 2; b++)
         for (int c = 0; c < 3; c++)
@@ -2306,13 +2587,27 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
     if (phase_mask == (1 | 4 | 8) && i0 <= 0 && i1 > s->n[0] && D.use_fused) return launch_fused_step(s);
     const int nx = s->n[0];
     const dim3 blk(kBlock);
-    const int gxh = D.sa[D.cur].seg_h.blk[D.sa[D.cur].seg_h.n], gxe = D.sa[D.cur].seg_e.blk[D.sa[D.cur].seg_e.n];
+    // general work-list entries of update u for node planes [a, b)
+    auto span = [&](int u, int a, int b, const int2 *&p) {
+        const std::vector<int> &st = D.wl_start[u];
+        p = D.wl[u].p + st[a];
+        return (unsigned)(st[b] - st[a]);
+    };
+    // fast pieces of update u on node planes [a, b)
+    auto fast = [&](int u, int a, int b, auto kernel) {
+        const FastSegs &f = D.fast[u];
+        const int c0 = std::max(a, f.p0), c1 = std::min(b, f.p1);
+        if (f.n == 0) return;
+        for (int c = c0; c < c1; c += kMaxGridY)
+            kernel<<<dim3(3 * f.blk[f.n], std::min(kMaxGridY, c1 - c)), blk, 0, D.stream>>>(D.sa[D.cur], c);
+    };
     if (phase_mask & 1) {   // H over node planes [i0, i1) within [0, nx]
         const int a = std::max(0, i0), b = std::min(nx + 1, i1);
         if (b > a) {
             t_begin(0);
-            for (int c0 = a; c0 < b; c0 += kMaxGridY)
-                k_update_h<<<dim3(3 * gxh, std::min(kMaxGridY, b - c0)), blk, 0, D.stream>>>(D.sa[D.cur], c0);
+            fast(0, a, b, k_update_h_fast);
+            const int2 *w;
+            if (unsigned n = span(0, a, b, w)) k_update_h<<<n, blk, 0, D.stream>>>(D.sa[D.cur], w);
             t_end();
         }
     }
@@ -2325,9 +2620,9 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
         const int a = std::max(0, i0), b = std::min(nx, i1);
         if (b > a) {
             t_begin(1);
-            for (int c0 = a; c0 < b; c0 += kMaxGridY)
-                kEKernels[s->npole]<<<dim3(3 * gxe, std::min(kMaxGridY, b - c0)), blk, 0, D.stream>>>(D.sa[D.cur],
-                                                                                                       c0);
+            fast(1, a, b, k_update_e_fast);
+            const int2 *w;
+            if (unsigned n = span(1, a, b, w)) kEKernels[s->npole]<<<n, blk, 0, D.stream>>>(D.sa[D.cur], w);
             t_end();
         }
     }
@@ -2572,10 +2867,11 @@ struct cemx_batch {
     DevBuf<StepArgs> args;
     DevBuf<SibcArgs> sargs;
     DevBuf<PostArgs> pargs;
-    DevBuf<int4> work_h;
-    std::map<int, DevBuf<int4>> work_e;      // by pole count
+    DevBuf<int4> work_h[2];                  // H blocks: fast, general
+    DevBuf<int4> work_ef;                    // E fast blocks of all members
+    std::map<int, DevBuf<int4>> work_e;      // E general blocks, by pole count
     DevBuf<int2> work_s;
-    size_t nh = 0, ns = 0;
+    size_t nh[2] = {0, 0}, nef = 0, ns = 0;
     std::map<int, size_t> ne;
     bool dirty = true;
     int order = 0;                           // work-list order: 0 member-major, 1 plane-interleaved
@@ -2627,7 +2923,7 @@ bool batch_rebuild(cemx_batch *b) {
     std::vector<StepArgs> sa;
     std::vector<SibcArgs> sb;
     std::vector<PostArgs> pa;
-    std::vector<int4> wh;
+    std::vector<int4> wh[2], wef;
     std::map<int, std::vector<int4>> we;
     std::vector<int2> ws;
     int maxp = 0;
@@ -2641,14 +2937,20 @@ bool batch_rebuild(cemx_batch *b) {
         maxp = std::max(maxp, s->n[0] + 1);
         for (int e0 = 0; e0 < s->nsb; e0 += kBlock) ws.push_back(make_int2(x, e0));
     }
-    // H over planes 0..nx, E over 0..nx-1; member-major, or plane by plane across members
+    // H over planes 0..nx, E over 0..nx-1; member-major, or plane by plane
+    // across members; fast and general blocks as the member's own lists
     auto add_plane = [&](int x, int i) {
         cem_sim *s = b->members[b->active[x]].s;
-        const StepArgs &a = sa[x];
+        const Device &D = *s->dev;
         if (i <= s->n[0])
-            for (int bx = 0; bx < 3 * a.seg_h.blk[a.seg_h.n]; bx++) wh.push_back(make_int4(x, bx, i, 0));
+            for (int bx = 0; bx < 3 * D.blocks[0]; bx++)
+                wh[D.gen_blk[0][(size_t)i * D.blocks[0] + bx / 3]].push_back(make_int4(x, bx, i, 0));
         if (i < s->n[0])
-            for (int bx = 0; bx < 3 * a.seg_e.blk[a.seg_e.n]; bx++) we[s->npole].push_back(make_int4(x, bx, i, 0));
+            for (int bx = 0; bx < 3 * D.blocks[1]; bx++) {
+                const int4 e = make_int4(x, bx, i, 0);
+                if (D.gen_blk[1][(size_t)i * D.blocks[1] + bx / 3]) we[s->npole].push_back(e);
+                else wef.push_back(e);
+            }
     };
     if (b->order == 0) {
         for (int x = 0; x < (int)b->active.size(); x++)
@@ -2658,7 +2960,8 @@ bool batch_rebuild(cemx_batch *b) {
             for (int x = 0; x < (int)b->active.size(); x++) add_plane(x, i);
     }
     if (!batch_upload(b->args, sa) || !batch_upload(b->sargs, sb) || !batch_upload(b->pargs, pa) ||
-        !batch_upload(b->work_h, wh) || !batch_upload(b->work_s, ws))
+        !batch_upload(b->work_h[0], wh[0]) || !batch_upload(b->work_h[1], wh[1]) || !batch_upload(b->work_ef, wef) ||
+        !batch_upload(b->work_s, ws))
         return false;
     b->work_e.clear();
     b->ne.clear();
@@ -2666,16 +2969,21 @@ bool batch_rebuild(cemx_batch *b) {
         if (!batch_upload(b->work_e[kv.first], kv.second)) return false;
         b->ne[kv.first] = kv.second.size();
     }
-    b->nh = wh.size();
+    b->nh[0] = wh[0].size();
+    b->nh[1] = wh[1].size();
+    b->nef = wef.size();
     b->ns = ws.size();
     b->dirty = false;
     return true;
 }
 
-// one batched time step: H, E (one launch per pole count), SIBC, probes
+// one batched time step: H (fast, general blocks), E (fast blocks; general
+// blocks one launch per pole count), SIBC, probes
 int batch_step(cemx_batch *b) {
     int launches = 0;
-    if (b->nh) { k_batch_h<<<(unsigned)b->nh, kBlock, 0, b->stream>>>(b->args.p, b->work_h.p); launches++; }
+    if (b->nh[0]) { k_batch_h<true><<<(unsigned)b->nh[0], kBlock, 0, b->stream>>>(b->args.p, b->work_h[0].p); launches++; }
+    if (b->nh[1]) { k_batch_h<false><<<(unsigned)b->nh[1], kBlock, 0, b->stream>>>(b->args.p, b->work_h[1].p); launches++; }
+    if (b->nef) { k_batch_e<0, true><<<(unsigned)b->nef, kBlock, 0, b->stream>>>(b->args.p, b->work_ef.p); launches++; }
     for (auto &kv : b->ne)
         if (kv.second) {
             kBEKernels[kv.first]<<<(unsigned)kv.second, kBlock, 0, b->stream>>>(b->args.p, b->work_e[kv.first].p);
@@ -2769,9 +3077,16 @@ int cemx_sizes(const cem_sim *s, long long *out, int n) {
                  (long long)(D.ring.n + D.acc.n) * 8;
         v[11] = bytes;
     }
-    // kernels per step: H and E (or one fused kernel), SIBC when present, the probe pass
-    int upd = 2;
+    // kernels per step: H and E, each over its fast and general blocks (or one
+    // fused kernel), SIBC when present, the probe pass
+    int upd = 4;
     if (s->dev && s->dev->use_fused) upd = 1;
+    else if (s->dev)
+        for (int u = 0; u < 2; u++) {
+            const FastSegs &f = s->dev->fast[u];
+            upd -= f.n == 0 || f.p1 <= f.p0;
+            upd -= s->dev->wl_start[u].empty() || s->dev->wl_start[u].back() == 0;
+        }
     v[12] = upd + 1 + (s->nsb ? 1 : 0);
     for (int q = 0; q < n && q < 13; q++) out[q] = v[q];
     return 0;
