@@ -1928,13 +1928,16 @@ bool build_sibc(cem_sim *s, Device &D) {
 }
 
 // k segments of the H and E kernels: cuts at the z CPML slabs (cells for H,
-// nodes for E) and, for E, at the Debye boxes, each rounded down to a
-// multiple of 4.
+// nodes for E) and, for E, at the Debye boxes. `cuts` holds [start, end)
+// pairs; a start is rounded down and an end up to a multiple of 4, so that a
+// slab's segment holds every 4-point group that reaches into it.
 bool make_segments(cem_sim *s, const std::vector<int> &cuts, KSegs &sg) {
     const Geom &g = s->dev->g;
     std::vector<int> b{0, g.sj};
-    for (int c : cuts)
-        if (c > 0 && c < g.sj) b.push_back(c / 4 * 4);
+    for (size_t q = 0; q < cuts.size(); q++) {
+        const int c = q % 2 ? (cuts[q] + 3) / 4 * 4 : cuts[q] / 4 * 4;
+        if (c > 0 && c < g.sj) b.push_back(c);
+    }
     std::sort(b.begin(), b.end());
     b.erase(std::unique(b.begin(), b.end()), b.end());
     if ((int)b.size() - 1 > kMaxSegs) {
