@@ -1543,7 +1543,15 @@ struct Device {
     EnergyArgs ea[2]{};
     FusedArgs fa[2]{};
 
+    // second stream and fork/join events: the general blocks of an update run
+    // beside its fast pieces
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+
     ~Device() {
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -2255,6 +2263,9 @@ bool create_device_impl(cem_sim *s) {
     if (const char *e = std::getenv("CEM_B200_FUSED")) D.use_fused = e[0] == '1';
     if (s->kernel_choice >= 0) D.use_fused = s->kernel_choice == 1;
     CB2_CHECK(s, cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking));
+    CB2_CHECK(s, cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
+    CB2_CHECK(s, cudaEventCreateWithFlags(&D.fork, cudaEventDisableTiming));
+    CB2_CHECK(s, cudaEventCreateWithFlags(&D.join, cudaEventDisableTiming));
     Geom &g = D.g;
     for (int a = 0; a < 3; a++) g.n[a] = s->n[a];
     g.sj = (s->n[2] + 1 + 7) / 8 * 8;
@@ -2604,13 +2615,26 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
         for (int c = c0; c < c1; c += kMaxGridY)
             kernel<<<dim3(3 * f.blk[f.n], std::min(kMaxGridY, c1 - c)), blk, 0, D.stream>>>(D.sa[D.cur], c);
     };
+    // the general blocks go to the side stream (after the work so far on the
+    // main one), the fast pieces to the main stream, which then waits for both
+    auto fork = [&]() {
+        cudaEventRecord(D.fork, D.stream);
+        cudaStreamWaitEvent(D.side, D.fork, 0);
+    };
+    auto join = [&]() { cudaStreamWaitEvent(D.stream, D.join, 0); };
     if (phase_mask & 1) {   // H over node planes [i0, i1) within [0, nx]
         const int a = std::max(0, i0), b = std::min(nx + 1, i1);
         if (b > a) {
             t_begin(0);
-            fast(0, a, b, k_update_h_fast);
             const int2 *w;
-            if (unsigned n = span(0, a, b, w)) k_update_h<<<n, blk, 0, D.stream>>>(D.sa[D.cur], w);
+            const unsigned n = span(0, a, b, w);
+            if (n) {
+                fork();
+                k_update_h<<<n, blk, 0, D.side>>>(D.sa[D.cur], w);
+                cudaEventRecord(D.join, D.side);
+            }
+            fast(0, a, b, k_update_h_fast);
+            if (n) join();
             t_end();
         }
     }
@@ -2623,9 +2647,15 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
         const int a = std::max(0, i0), b = std::min(nx, i1);
         if (b > a) {
             t_begin(1);
-            fast(1, a, b, k_update_e_fast);
             const int2 *w;
-            if (unsigned n = span(1, a, b, w)) kEKernels[s->npole]<<<n, blk, 0, D.stream>>>(D.sa[D.cur], w);
+            const unsigned n = span(1, a, b, w);
+            if (n) {
+                fork();
+                kEKernels[s->npole]<<<n, blk, 0, D.side>>>(D.sa[D.cur], w);
+                cudaEventRecord(D.join, D.side);
+            }
+            fast(1, a, b, k_update_e_fast);
+            if (n) join();
             t_end();
         }
     }
