@@ -2913,6 +2913,8 @@ struct cemx_batch {
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t side = nullptr;             // general blocks, beside the fast ones
+    cudaEvent_t fork = nullptr, join = nullptr;
     double last_ms = 0;
     long last_steps = 0, last_launches = 0;
 };
@@ -3014,14 +3016,32 @@ bool batch_rebuild(cemx_batch *b) {
 // blocks one launch per pole count), SIBC, probes
 int batch_step(cemx_batch *b) {
     int launches = 0;
+    // general blocks on the side stream beside the fast ones, joined before the next phase
+    auto fork = [&]() {
+        cudaEventRecord(b->fork, b->stream);
+        cudaStreamWaitEvent(b->side, b->fork, 0);
+    };
+    auto join = [&]() {
+        cudaEventRecord(b->join, b->side);
+        cudaStreamWaitEvent(b->stream, b->join, 0);
+    };
+    if (b->nh[1]) {
+        fork();
+        k_batch_h<false><<<(unsigned)b->nh[1], kBlock, 0, b->side>>>(b->args.p, b->work_h[1].p);
+        launches++;
+    }
     if (b->nh[0]) { k_batch_h<true><<<(unsigned)b->nh[0], kBlock, 0, b->stream>>>(b->args.p, b->work_h[0].p); launches++; }
-    if (b->nh[1]) { k_batch_h<false><<<(unsigned)b->nh[1], kBlock, 0, b->stream>>>(b->args.p, b->work_h[1].p); launches++; }
-    if (b->nef) { k_batch_e<0, true><<<(unsigned)b->nef, kBlock, 0, b->stream>>>(b->args.p, b->work_ef.p); launches++; }
+    if (b->nh[1]) join();
+    bool side = false;
     for (auto &kv : b->ne)
         if (kv.second) {
-            kBEKernels[kv.first]<<<(unsigned)kv.second, kBlock, 0, b->stream>>>(b->args.p, b->work_e[kv.first].p);
+            if (!side) fork();
+            side = true;
+            kBEKernels[kv.first]<<<(unsigned)kv.second, kBlock, 0, b->side>>>(b->args.p, b->work_e[kv.first].p);
             launches++;
         }
+    if (b->nef) { k_batch_e<0, true><<<(unsigned)b->nef, kBlock, 0, b->stream>>>(b->args.p, b->work_ef.p); launches++; }
+    if (side) join();
     if (b->ns) { k_batch_sibc<<<(unsigned)b->ns, kBlock, 0, b->stream>>>(b->sargs.p, b->work_s.p); launches++; }
     k_batch_post<<<(unsigned)b->active.size(), kPostThreads, 0, b->stream>>>(b->pargs.p);
     return launches + 1;
@@ -3177,7 +3197,10 @@ cemx_batch *cemx_batch_create(int device) {
     cemx_batch *b = new cemx_batch;
     b->device = device;
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess) {
         set_error("batch: cannot create its stream");
         cemx_batch_destroy(b);
         return nullptr;
@@ -3193,6 +3216,9 @@ void cemx_batch_destroy(cemx_batch *b) {
     b->work_e.clear();
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->join) cudaEventDestroy(b->join);
+    if (b->side) cudaStreamDestroy(b->side);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
