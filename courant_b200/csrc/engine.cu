@@ -82,38 +82,30 @@ struct PmlAxis {
 // Host copies use the reference's compact layout (sim.c:655-678) and are
 // converted at transfer.
 
-// The update kernels cover each node plane in k segments: the k axis is cut
-// at the CPML slab and Debye box boundaries (rounded down to multiples of 4),
-// and threads are laid out row by row within one segment, so the threads of
-// a warp share their k pattern and mostly take the same branch.
-constexpr int kMaxSegs = 12;
-struct KSegs {
-    int n;                                // segments
-    int k[kMaxSegs + 1];                  // boundaries: k[0] = 0, k[n] = sj, all multiples of 4
-    int blk[kMaxSegs + 1];                // first block of each segment; blk[n]: blocks per plane and component
-    unsigned long long magic[kMaxSegs];   // row of segment thread t: (t * magic) >> 40
-};
-
-// The fast pieces of the update kernels: runs of blocks of the k-segment
-// layout in which no point of any component has a CPML auxiliary on a
-// derivative axis or (E) a Debye current, on every node plane of [p0, p1).
-// Piece q covers segment-linear threads [t0, t0 + nt) (thread t: row
-// t / nk4, 4-point group t % nk4) of the segment [ks, ke); the fast kernels
-// walk the pieces on a (blocks, planes) grid, the general blocks go to a
-// work-list.
-struct FastSegs {
+// Thread spaces of the update kernels. A space is a list of rectangles of a
+// node plane: k range [ks, ke) in whole 4-point groups, rows [js, js + rows).
+// One thread per 4-point group; the rectangles' threads follow one another
+// (rectangle q holds threads [t0[q], t0[q + 1])), row by row within a
+// rectangle, so the threads of a row are consecutive (k neighbours move by
+// shuffle) and a warp mostly shares its k pattern. The k axis is cut at the z
+// CPML slabs and (E) the Debye boxes, the rows at the inner edges of the y
+// slabs and (E) the boxes' rows. Each update has three spaces: the fast
+// rectangles (no point of any component has a CPML auxiliary on a
+// derivative axis or a Debye current) and the general ones of the interior
+// node planes [p0, p1), and all rectangles for the other planes.
+constexpr int kMaxRects = 12;
+struct Space {
     int n;
-    int ks[kMaxSegs], ke[kMaxSegs];
-    int t0[kMaxSegs], nt[kMaxSegs];
-    int blk[kMaxSegs + 1];                // first block of each piece; blk[n]: blocks per plane and component
-    unsigned long long magic[kMaxSegs];   // row of thread t: (t * magic) >> 40
-    int p0, p1;
+    int ks[kMaxRects], ke[kMaxRects], js[kMaxRects];
+    int t0[kMaxRects + 1];                  // t0[n]: threads of the space
+    unsigned long long magic[kMaxRects];    // row in its rectangle of thread t - t0: ((t - t0) * magic) >> 40
 };
+constexpr int kFast = 0, kGeneral = 1, kAll = 2;
 
 struct StepArgs {
     Geom g;
-    KSegs seg_h, seg_e;
-    FastSegs fast_h, fast_e;
+    Space sp[2][3];          // [H, E][kFast, kGeneral, kAll]
+    int p0[2], p1[2];        // interior node planes of H and E
     float *E[3], *H[3];
     const float *hc[3];      // dt/mu0 * idh per axis (cells)
     const float *ec[3];      // ide per axis (nodes)
@@ -482,24 +474,30 @@ __device__ __forceinline__ float4 prev_k(const float4 &v, const float *p, bool n
     return make_float4(w, v.x, v.y, v.z);
 }
 
-// Position of this thread: row j and first point k4 of its four, inside the
-// k segment [ks, ke) that block b (per component) belongs to.
+// Position of this thread (block b of a space): row j and first point k4 of
+// its four, the k range [ks, ke) of its rectangle, whether it has work
+// (`act`; a thread past the end takes the last thread's position) and whether
+// the next lane holds the next four points of the same row (`cont`).
 struct RowPos {
     int j, k4, ks, ke;
-    bool act;
+    bool act, cont;
 };
 
-__device__ __forceinline__ RowPos row_pos(const KSegs &sg, int rows, int b) {
-    int s = 0;
-    while (s + 1 < sg.n && b >= sg.blk[s + 1]) s++;
+__device__ __forceinline__ RowPos space_pos(const Space &sp, int b) {
+    const int t = b * kBlock + threadIdx.x, nt = sp.t0[sp.n];
     RowPos r;
-    r.ks = sg.k[s];
-    r.ke = sg.k[s + 1];
+    r.act = t < nt;
+    const int tc = r.act ? t : nt - 1;
+    int q = 0;
+    while (q + 1 < sp.n && tc >= sp.t0[q + 1]) q++;
+    const int tl = tc - sp.t0[q];
+    r.ks = sp.ks[q];
+    r.ke = sp.ke[q];
     const int nk4 = (r.ke - r.ks) >> 2;
-    const int t = (b - sg.blk[s]) * kBlock + threadIdx.x;
-    r.act = t < rows * nk4;
-    r.j = r.act ? (int)(((unsigned long long)t * sg.magic[s]) >> 40) : 0;
-    r.k4 = r.ks + 4 * (t - r.j * nk4);
+    const int row = (int)(((unsigned long long)tl * sp.magic[q]) >> 40);
+    r.j = sp.js[q] + row;
+    r.k4 = r.ks + 4 * (tl - row * nk4);
+    r.cont = (threadIdx.x & 31) != 31 && r.k4 + 4 < r.ke && t + 1 < nt;
     return r;
 }
 
@@ -793,35 +791,11 @@ __device__ __forceinline__ void e_vec(const StepArgs &a, int i, const RowPos &r,
     e_points<C, P>(a, i, j, k4, E + q, w, h2, h2m, h1, h1m, ev, mv, sv);
 }
 
-// Position of this thread in the fast pieces f (block bx of the plane):
-// row j, first point k4, its segment's k range, and whether the next lane
-// holds the next four points of the same row (`cont`).
-struct LeanPos {
-    int j, k4, ks, ke;
-    bool act, cont;
-};
-
-__device__ __forceinline__ LeanPos lean_pos(const FastSegs &f, int bx) {
-    int q = 0;
-    while (q + 1 < f.n && bx >= f.blk[q + 1]) q++;
-    const int tl = (bx - f.blk[q]) * kBlock + threadIdx.x;
-    LeanPos p;
-    p.act = tl < f.nt[q];
-    const int t = f.t0[q] + (p.act ? tl : f.nt[q] - 1);
-    p.ks = f.ks[q];
-    p.ke = f.ke[q];
-    const int nk4 = (p.ke - p.ks) >> 2;
-    p.j = (int)(((unsigned long long)t * f.magic[q]) >> 40);
-    p.k4 = p.ks + 4 * (t - p.j * nk4);
-    p.cont = (threadIdx.x & 31) != 31 && p.k4 + 4 < p.ke && tl + 1 < f.nt[q];
-    return p;
-}
-
 // H component C at points k4 .. k4+3 of row (i, j) of a fast piece: the
 // short path of h_points (no auxiliaries), every rounding the same. All
 // lanes of the warp call it (the k+1 neighbours move by shuffle).
 template <int C>
-__device__ __forceinline__ void h_lean(const StepArgs &a, int i, const LeanPos &p) {
+__device__ __forceinline__ void h_lean(const StepArgs &a, int i, const RowPos &p) {
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
     constexpr bool kz = A1 == 2 || A2 == 2;
     const int nx = a.g.n[0], ny = a.g.n[1], nz = a.g.n[2];
@@ -862,7 +836,7 @@ __device__ __forceinline__ void h_lean(const StepArgs &a, int i, const LeanPos &
 // short path of e_points (material table, sources; no auxiliaries, no Debye
 // currents), every rounding the same
 template <int C>
-__device__ __forceinline__ void e_lean(const StepArgs &a, int i, const LeanPos &p, const float2 sv) {
+__device__ __forceinline__ void e_lean(const StepArgs &a, int i, const RowPos &p, const float2 sv) {
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
     const int ny = a.g.n[1], nz = a.g.n[2];
     const int j = p.j, k4 = p.k4;
@@ -922,21 +896,21 @@ __device__ __forceinline__ void e_lean(const StepArgs &a, int i, const LeanPos &
 #define CB2_EF_MINBLOCKS 5
 #endif
 
-// H on the fast pieces of node planes [i0, i0 + gridDim.y); block x: piece
-// block x / 3, component x % 3
+// H on the fast rectangles of node planes [i0, i0 + gridDim.y); block x:
+// block x / 3 of the space, component x % 3
 __global__ void __launch_bounds__(kBlock, CB2_HF_MINBLOCKS) k_update_h_fast(const StepArgs a, int i0) {
     const int comp = blockIdx.x % 3;
-    const LeanPos p = lean_pos(a.fast_h, blockIdx.x / 3);
+    const RowPos p = space_pos(a.sp[0][kFast], blockIdx.x / 3);
     const int i = i0 + blockIdx.y;
     if (comp == 0) h_lean<0>(a, i, p);
     else if (comp == 1) h_lean<1>(a, i, p);
     else h_lean<2>(a, i, p);
 }
 
-// E on the fast pieces of node planes [i0, i0 + gridDim.y)
+// E on the fast rectangles of node planes [i0, i0 + gridDim.y)
 __global__ void __launch_bounds__(kBlock, CB2_EF_MINBLOCKS) k_update_e_fast(const StepArgs a, int i0) {
     const int comp = blockIdx.x % 3;
-    const LeanPos p = lean_pos(a.fast_e, blockIdx.x / 3);
+    const RowPos p = space_pos(a.sp[1][kFast], blockIdx.x / 3);
     const int i = i0 + blockIdx.y;
     const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
     if (comp == 0) e_lean<0>(a, i, p, sv);
@@ -944,12 +918,19 @@ __global__ void __launch_bounds__(kBlock, CB2_EF_MINBLOCKS) k_update_e_fast(cons
     else e_lean<2>(a, i, p, sv);
 }
 
-// Work entry of the general blocks: x node plane, y block of the plane
-// (component y % 3, block y / 3 of the k-segment layout).
+// Position in the general space of update U: the general rectangles on an
+// interior node plane i, all rectangles on the others
+template <int U>
+__device__ __forceinline__ RowPos general_pos(const StepArgs &a, int i, int b) {
+    return i >= a.p0[U] && i < a.p1[U] ? space_pos(a.sp[U][kGeneral], b) : space_pos(a.sp[U][kAll], b);
+}
+
+// Work entry of the general blocks: x node plane, y block of the plane's
+// general space (component y % 3, block y / 3).
 __global__ void __launch_bounds__(kBlock, CB2_H_MINBLOCKS) k_update_h(const StepArgs a, const int2 *work) {
     const int2 w = work[blockIdx.x];
     const int comp = w.y % 3;
-    const RowPos r = row_pos(a.seg_h, a.g.n[1] + 1, w.y / 3);
+    const RowPos r = general_pos<0>(a, w.x, w.y / 3);
     if (comp == 0) h_vec<0, false>(a, w.x, r);
     else if (comp == 1) h_vec<1, false>(a, w.x, r);
     else h_vec<2, false>(a, w.x, r);
@@ -960,7 +941,7 @@ template <int P>
 __global__ void __launch_bounds__(kBlock, CB2_E_MINBLOCKS) k_update_e(const StepArgs a, const int2 *work) {
     const int2 w = work[blockIdx.x];
     const int comp = w.y % 3;
-    const RowPos r = row_pos(a.seg_e, a.g.n[1] + 1, w.y / 3);
+    const RowPos r = general_pos<1>(a, w.x, w.y / 3);
     const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
     if (comp == 0) e_vec<0, P, false>(a, w.x, r, sv);
     else if (comp == 1) e_vec<1, P, false>(a, w.x, r, sv);
@@ -1355,7 +1336,7 @@ __global__ void __launch_bounds__(kBlock, FAST ? CB2_HF_MINBLOCKS : CB2_H_MINBLO
     __shared__ unsigned buf[sizeof(StepArgs) / 4];
     const int4 w = work[blockIdx.x];
     const StepArgs &a = stage_args(args + w.x, buf);
-    const RowPos r = row_pos(a.seg_h, a.g.n[1] + 1, w.y / 3);
+    const RowPos r = FAST ? space_pos(a.sp[0][kFast], w.y / 3) : general_pos<0>(a, w.z, w.y / 3);
     const int comp = w.y % 3;
     if (comp == 0) h_vec<0, FAST>(a, w.z, r);
     else if (comp == 1) h_vec<1, FAST>(a, w.z, r);
@@ -1368,7 +1349,7 @@ __global__ void __launch_bounds__(kBlock, FAST ? CB2_EF_MINBLOCKS : CB2_E_MINBLO
     __shared__ unsigned buf[sizeof(StepArgs) / 4];
     const int4 w = work[blockIdx.x];
     const StepArgs &a = stage_args(args + w.x, buf);
-    const RowPos r = row_pos(a.seg_e, a.g.n[1] + 1, w.y / 3);
+    const RowPos r = FAST ? space_pos(a.sp[1][kFast], w.y / 3) : general_pos<1>(a, w.z, w.y / 3);
     const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
     const int comp = w.y % 3;
     if (comp == 0) e_vec<0, P, FAST>(a, w.z, r, sv);
@@ -1502,16 +1483,14 @@ struct Device {
     int ntab[3] = {0, 0, 0};
     DevBuf<float> J[3];
     int jbox[3][6] = {};
-    KSegs seg_h{}, seg_e{};
-    // Update kernels [H, E]: the fast pieces, and the work-list of the
-    // general blocks, entries (node plane, block of the plane incl.
-    // component) in plane order; wl_start[u][i] is the first entry of plane
-    // i. gen_blk[u][i * blocks[u] + b]: block b of plane i is general.
-    FastSegs fast[2]{};
+    // Update kernels [H, E]: thread spaces [kFast, kGeneral, kAll], the
+    // interior node planes [p0, p1), and the work-list of the general blocks
+    // (entries: node plane, block of the plane's general space incl.
+    // component) in plane order; wl_start[u][i] is the first entry of plane i.
+    Space sp[2][3]{};
+    int p0[2] = {0, 0}, p1[2] = {0, 0};
     DevBuf<int2> wl[2];
     std::vector<int> wl_start[2];
-    std::vector<unsigned char> gen_blk[2];
-    int blocks[2] = {0, 0};
     DevBuf<float> wsrc[2];
     // SIBC
     DevBuf<unsigned char> sb_ecomp;
@@ -1935,162 +1914,131 @@ bool build_sibc(cem_sim *s, Device &D) {
            dev_alloc(s, D.sb_y, ns * s->sibc_npole);
 }
 
-// k segments of the H and E kernels: cuts at the z CPML slabs (cells for H,
-// nodes for E) and, for E, at the Debye boxes. `cuts` holds [start, end)
-// pairs; a start is rounded down and an end up to a multiple of 4, so that a
-// slab's segment holds every 4-point group that reaches into it.
-bool make_segments(cem_sim *s, const std::vector<int> &cuts, KSegs &sg) {
-    const Geom &g = s->dev->g;
-    std::vector<int> b{0, g.sj};
-    for (size_t q = 0; q < cuts.size(); q++) {
-        const int c = q % 2 ? (cuts[q] + 3) / 4 * 4 : cuts[q] / 4 * 4;
-        if (c > 0 && c < g.sj) b.push_back(c);
-    }
-    std::sort(b.begin(), b.end());
-    b.erase(std::unique(b.begin(), b.end()), b.end());
-    if ((int)b.size() - 1 > kMaxSegs) {
-        set_error("too many k segments");
-        return false;
-    }
-    sg = KSegs{};
-    sg.n = (int)b.size() - 1;
-    const long long rows = s->n[1] + 1;
-    int blocks = 0;
-    for (int q = 0; q < sg.n; q++) {
-        const long long nk4 = (b[q + 1] - b[q]) / 4;
-        if (rows * nk4 * nk4 >= (1ll << 40) || rows * nk4 >= (1ll << 31)) {
-            set_error("grid too large for the k-segment layout");
-            return false;
-        }
-        sg.k[q] = b[q];
-        sg.blk[q] = blocks;
-        sg.magic[q] = ((1ull << 40) + (unsigned long long)nk4 - 1) / (unsigned long long)nk4;
-        blocks += (int)((rows * nk4 + kBlock - 1) / kBlock);
-    }
-    sg.k[sg.n] = b[sg.n];
-    sg.blk[sg.n] = blocks;
-    return true;
-}
+// blocks of a space
+int space_blocks(const Space &sp) { return (sp.t0[sp.n] + kBlock - 1) / kBlock; }
 
-bool build_segments(cem_sim *s, Device &D) {
-    std::vector<int> ch, ce;
-    if (s->has_pml) {
-        int r[2][2];
-        pml_ranges(s, 2, 0, r);
-        for (int sd = 0; sd < 2; sd++)
-            if (r[sd][1] >= r[sd][0]) { ch.push_back(r[sd][0]); ch.push_back(r[sd][1] + 1); }
-        pml_ranges(s, 2, 1, r);
-        for (int sd = 0; sd < 2; sd++)
-            if (r[sd][1] >= r[sd][0]) { ce.push_back(r[sd][0]); ce.push_back(r[sd][1] + 1); }
-    }
-    for (int c = 0; c < 3; c++)
-        if (D.jbox[c][5] > 0) { ce.push_back(D.jbox[c][2]); ce.push_back(D.jbox[c][2] + D.jbox[c][5]); }
-    return make_segments(s, ch, D.seg_h) && make_segments(s, ce, D.seg_e);
-}
-
-// Which blocks of the update kernels may meet a CPML auxiliary on a
-// derivative axis or (E) a Debye current: a block (node plane i, block b of
-// a k segment, all three components) is general when plane i lies in an x
-// slab, its segment reaches a z slab, one of its rows lies in a y slab, or
-// (E) it overlaps a component's Debye box. The other blocks run the short
-// path only, in kernels compiled without the general one.
-bool build_worklists(cem_sim *s, Device &D) {
-    const int nx = s->n[0], ny = s->n[1], nz = s->n[2];
-    const int rows = ny + 1;
-    auto slab = [&](int a, int is_e, int idx) {
+// The thread spaces of update u (0 H, 1 E) and its general work-list.
+// k is cut at the z CPML slabs (cells for H, nodes for E) and, for E, at the
+// Debye boxes: a slab's start rounded down and its end up to a multiple of
+// 4, so that the slab's k range holds every 4-point group that reaches into
+// it. The rows are cut at the inner edges of the y slabs and, for E, at the
+// boxes' rows. Interior planes: the longest run of node planes outside the
+// x slabs. A rectangle is general when its k range reaches a z slab, its rows
+// a y slab, or (E) it meets a Debye box whose planes meet the interior ones;
+// consecutive row ranges of one class and k range merge.
+bool build_spaces(cem_sim *s, Device &D, int u) {
+    const Geom &g = D.g;
+    const int nx = s->n[0], rows = s->n[1] + 1;
+    const int planes = u ? nx : nx + 1;
+    auto slab = [&](int a, int idx) {
         if (!s->has_pml) return false;
         int r[2][2];
-        pml_ranges(s, a, is_e, r);
-        if (idx >= s->n[a] && !is_e) return false;   // cells end at n-1
+        pml_ranges(s, a, u, r);
+        if (idx >= s->n[a] && !u) return false;   // cells end at n-1
         for (int sd = 0; sd < 2; sd++)
             if (idx >= r[sd][0] && idx <= r[sd][1]) return true;
         return false;
     };
-    for (int u = 0; u < 2; u++) {
-        const KSegs &sg = u ? D.seg_e : D.seg_h;
-        const int planes = u ? nx : nx + 1;
-        const int nb = sg.blk[sg.n];
-        D.blocks[u] = nb;
-        std::vector<unsigned char> gen((size_t)planes * nb, 0);
-        for (int q = 0; q < sg.n; q++) {
-            const int ks = sg.k[q], ke = sg.k[q + 1], nk4 = (ke - ks) / 4;
-            bool zs = false;
-            for (int k = ks; k < ke; k++) zs = zs || slab(2, u, k);
-            for (int b = sg.blk[q]; b < sg.blk[q + 1]; b++) {
-                const long long t0 = (long long)(b - sg.blk[q]) * kBlock;
-                const long long t1 = std::min<long long>(t0 + kBlock, (long long)rows * nk4);
-                const int j0 = (int)(t0 / nk4), j1 = (int)((t1 - 1) / nk4);
-                bool ys = false;
-                for (int j = j0; j <= j1; j++) ys = ys || slab(1, u, j);
-                for (int i = 0; i < planes; i++) {
-                    bool g = zs || ys || slab(0, u, i);
-                    for (int c = 0; u && c < 3 && !g; c++) {
-                        const int *bx = D.jbox[c];
-                        if (bx[3] * bx[4] * bx[5] == 0) continue;
-                        g = i >= bx[0] && i < bx[0] + bx[3] && j1 >= bx[1] && j0 < bx[1] + bx[4] && ke > bx[2] &&
-                            ks < bx[2] + bx[5];
-                    }
-                    gen[(size_t)i * nb + b] = g;
-                }
-            }
-        }
-        // fast planes: the longest run of planes outside the x slabs; fast
-        // blocks: general on none of them; pieces: runs of fast blocks
-        int p0 = 0, p1 = 0;
-        for (int i = 0; i < planes;) {
-            if (slab(0, u, i)) { i++; continue; }
-            int e = i;
-            while (e < planes && !slab(0, u, e)) e++;
-            if (e - i > p1 - p0) { p0 = i; p1 = e; }
-            i = e;
-        }
-        std::vector<unsigned char> fastb(nb, p1 > p0);
-        for (int b = 0; b < nb; b++)
-            for (int i = p0; i < p1 && fastb[b]; i++) fastb[b] = !gen[(size_t)i * nb + b];
-        FastSegs f{};
-        f.p0 = p0;
-        f.p1 = p1;
-        int fb = 0;
-        for (int q = 0; q < sg.n; q++) {
-            const long long nthr = (long long)rows * ((sg.k[q + 1] - sg.k[q]) / 4);
-            for (int b = sg.blk[q]; b < sg.blk[q + 1];) {
-                if (!fastb[b]) { b++; continue; }
-                int e = b;
-                while (e < sg.blk[q + 1] && fastb[e]) e++;
-                if (f.n == kMaxSegs) {   // no room for another piece: these blocks stay general
-                    std::fill(fastb.begin() + b, fastb.begin() + e, 0);
-                } else {
-                    const long long t0 = (long long)(b - sg.blk[q]) * kBlock;
-                    f.ks[f.n] = sg.k[q];
-                    f.ke[f.n] = sg.k[q + 1];
-                    f.t0[f.n] = (int)t0;
-                    f.nt[f.n] = (int)(std::min<long long>((long long)(e - sg.blk[q]) * kBlock, nthr) - t0);
-                    f.magic[f.n] = sg.magic[q];
-                    f.blk[f.n] = fb;
-                    fb += e - b;
-                    f.n++;
-                }
-                b = e;
-            }
-        }
-        f.blk[f.n] = fb;
-        for (int i = 0; i < planes; i++)
-            for (int b = 0; b < nb; b++) gen[(size_t)i * nb + b] = !(i >= p0 && i < p1 && fastb[b]);
-        std::vector<int2> wl;
-        std::vector<int> &st = D.wl_start[u];
-        st.assign(planes + 1, 0);
-        for (int i = 0; i < planes; i++) {
-            st[i] = (int)wl.size();
-            for (int b = 0; b < nb; b++)
-                if (gen[(size_t)i * nb + b])
-                    for (int c = 0; c < 3; c++) wl.push_back(make_int2(i, 3 * b + c));
-        }
-        st[planes] = (int)wl.size();
-        if (!wl.empty() && !dev_upload(s, D.wl[u], wl)) return false;
-        D.fast[u] = f;
-        D.gen_blk[u] = std::move(gen);
+    int p0 = 0, p1 = 0;
+    for (int i = 0; i < planes;) {
+        if (slab(0, i)) { i++; continue; }
+        int e = i;
+        while (e < planes && !slab(0, e)) e++;
+        if (e - i > p1 - p0) { p0 = i; p1 = e; }
+        i = e;
     }
-    return true;
+    // boxes whose planes meet the interior ones
+    std::vector<const int *> boxes;
+    for (int c = 0; u && c < 3; c++) {
+        const int *bx = D.jbox[c];
+        if (bx[3] * bx[4] * bx[5] > 0 && bx[0] < p1 && bx[0] + bx[3] > p0) boxes.push_back(bx);
+    }
+    std::vector<int> kb{0, g.sj}, jb{0, rows};
+    auto kcut = [&](int c) { if (c > 0 && c < g.sj) kb.push_back(c); };
+    auto jcut = [&](int c) { if (c > 0 && c < rows) jb.push_back(c); };
+    if (s->has_pml) {
+        int r[2][2];
+        pml_ranges(s, 2, u, r);
+        for (int sd = 0; sd < 2; sd++)
+            if (r[sd][1] >= r[sd][0]) { kcut(r[sd][0] / 4 * 4); kcut((r[sd][1] + 1 + 3) / 4 * 4); }
+        pml_ranges(s, 1, u, r);
+        if (r[0][1] >= r[0][0]) jcut(r[0][1] + 1);
+        if (r[1][1] >= r[1][0]) jcut(r[1][0]);
+    }
+    for (const int *bx : boxes) {
+        kcut(bx[2] / 4 * 4);
+        kcut((bx[2] + bx[5] + 3) / 4 * 4);
+        jcut(bx[1]);
+        jcut(bx[1] + bx[4]);
+    }
+    for (auto *v : {&kb, &jb}) {
+        std::sort(v->begin(), v->end());
+        v->erase(std::unique(v->begin(), v->end()), v->end());
+    }
+    struct Rect { int ks, ke, js, je; };
+    std::vector<Rect> cls[3];
+    for (size_t q = 0; q + 1 < kb.size(); q++) {
+        const int ks = kb[q], ke = kb[q + 1];
+        bool zs = false;
+        for (int k = ks; k < ke; k++) zs = zs || slab(2, k);
+        cls[kAll].push_back({ks, ke, 0, rows});
+        for (size_t r = 0; r + 1 < jb.size(); r++) {
+            const int js = jb[r], je = jb[r + 1];
+            bool gen = zs;
+            for (int j = js; j < je && !gen; j++) gen = slab(1, j);
+            for (const int *bx : boxes)
+                gen = gen || (ke > bx[2] && ks < bx[2] + bx[5] && je > bx[1] && js < bx[1] + bx[4]);
+            std::vector<Rect> &v = cls[gen ? kGeneral : kFast];
+            if (!v.empty() && v.back().ks == ks && v.back().je == js) v.back().je = je;
+            else v.push_back({ks, ke, js, je});
+        }
+    }
+    if (p1 <= p0 || (int)cls[kFast].size() > kMaxRects || (int)cls[kGeneral].size() > kMaxRects) {
+        cls[kFast].clear();   // no interior planes, or too many rectangles: every block general
+        cls[kGeneral] = cls[kAll];
+    }
+    if ((int)cls[kAll].size() > kMaxRects) {
+        set_error("too many k segments");
+        return false;
+    }
+    for (int c = 0; c < 3; c++) {
+        Space &sp = D.sp[u][c];
+        sp = Space{};
+        long long t = 0;
+        for (const Rect &r : cls[c]) {
+            const long long nk4 = (r.ke - r.ks) / 4, nr = r.je - r.js;
+            if (nr * nk4 * nk4 >= (1ll << 40)) {
+                set_error("grid too large for the update layout");
+                return false;
+            }
+            sp.ks[sp.n] = r.ks;
+            sp.ke[sp.n] = r.ke;
+            sp.js[sp.n] = r.js;
+            sp.t0[sp.n] = (int)t;
+            sp.magic[sp.n] = ((1ull << 40) + (unsigned long long)nk4 - 1) / (unsigned long long)nk4;
+            sp.n++;
+            t += nr * nk4;
+        }
+        if (t >= (1ll << 31) - kBlock) {
+            set_error("grid too large for the update layout");
+            return false;
+        }
+        sp.t0[sp.n] = (int)t;
+    }
+    D.p0[u] = p0;
+    D.p1[u] = p1;
+    // general work-list: the general space on interior planes, every rectangle elsewhere
+    std::vector<int2> wl;
+    std::vector<int> &st = D.wl_start[u];
+    st.assign(planes + 1, 0);
+    const int ng = space_blocks(D.sp[u][kGeneral]), na = space_blocks(D.sp[u][kAll]);
+    for (int i = 0; i < planes; i++) {
+        st[i] = (int)wl.size();
+        const int nb = i >= p0 && i < p1 ? ng : na;
+        for (int b = 0; b < 3 * nb; b++) wl.push_back(make_int2(i, b));
+    }
+    st[planes] = (int)wl.size();
+    return wl.empty() || dev_upload(s, D.wl[u], wl);
 }
 
 bool build_sources(cem_sim *s, Device &D) {
@@ -2112,10 +2060,11 @@ void fill_args_for(cem_sim *s, Device &D, int cur) {
     StepArgs &a = D.sa[cur];
     a = StepArgs{};
     a.g = D.g;
-    a.seg_h = D.seg_h;
-    a.seg_e = D.seg_e;
-    a.fast_h = D.fast[0];
-    a.fast_e = D.fast[1];
+    for (int u = 0; u < 2; u++) {
+        for (int c = 0; c < 3; c++) a.sp[u][c] = D.sp[u][c];
+        a.p0[u] = D.p0[u];
+        a.p1[u] = D.p1[u];
+    }
     for (int c = 0; c < 3; c++) {
         a.E[c] = D.E[cur][c].p;
         a.H[c] = D.H[cur][c].p;
@@ -2290,7 +2239,7 @@ bool create_device_impl(cem_sim *s) {
         if (!dev_upload(s, D.d64[c], s->d[c]) || !dev_upload(s, D.dd64[c], s->dd[c])) return false;
     }
     if (!build_pml(s, D) || !build_tables(s, D) || !build_probes(s, D) || !build_sibc(s, D) || !build_sources(s, D) ||
-        !build_segments(s, D) || !build_worklists(s, D))
+        !build_spaces(s, D, 0) || !build_spaces(s, D, 1))
         return false;
     for (int b = 0; b < 2; b++)
         for (int c = 0; c < 3; c++)
@@ -2607,13 +2556,13 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
         p = D.wl[u].p + st[a];
         return (unsigned)(st[b] - st[a]);
     };
-    // fast pieces of update u on node planes [a, b)
+    // fast rectangles of update u on node planes [a, b)
     auto fast = [&](int u, int a, int b, auto kernel) {
-        const FastSegs &f = D.fast[u];
-        const int c0 = std::max(a, f.p0), c1 = std::min(b, f.p1);
-        if (f.n == 0) return;
+        const int nb = space_blocks(D.sp[u][kFast]);
+        const int c0 = std::max(a, D.p0[u]), c1 = std::min(b, D.p1[u]);
+        if (nb == 0) return;
         for (int c = c0; c < c1; c += kMaxGridY)
-            kernel<<<dim3(3 * f.blk[f.n], std::min(kMaxGridY, c1 - c)), blk, 0, D.stream>>>(D.sa[D.cur], c);
+            kernel<<<dim3(3 * nb, std::min(kMaxGridY, c1 - c)), blk, 0, D.stream>>>(D.sa[D.cur], c);
     };
     // the general blocks go to the side stream (after the work so far on the
     // main one), the fast pieces to the main stream, which then waits for both
@@ -2977,15 +2926,18 @@ bool batch_rebuild(cemx_batch *b) {
     auto add_plane = [&](int x, int i) {
         cem_sim *s = b->members[b->active[x]].s;
         const Device &D = *s->dev;
-        if (i <= s->n[0])
-            for (int bx = 0; bx < 3 * D.blocks[0]; bx++)
-                wh[D.gen_blk[0][(size_t)i * D.blocks[0] + bx / 3]].push_back(make_int4(x, bx, i, 0));
-        if (i < s->n[0])
-            for (int bx = 0; bx < 3 * D.blocks[1]; bx++) {
-                const int4 e = make_int4(x, bx, i, 0);
-                if (D.gen_blk[1][(size_t)i * D.blocks[1] + bx / 3]) we[s->npole].push_back(e);
-                else wef.push_back(e);
-            }
+        // interior planes: the fast and the general space; elsewhere every rectangle
+        auto blocks = [&](int u, int c) { return 3 * space_blocks(D.sp[u][c]); };
+        const bool ih = i >= D.p0[0] && i < D.p1[0], ie = i >= D.p0[1] && i < D.p1[1];
+        if (i <= s->n[0]) {
+            for (int bx = 0; ih && bx < blocks(0, kFast); bx++) wh[0].push_back(make_int4(x, bx, i, 0));
+            for (int bx = 0; bx < blocks(0, ih ? kGeneral : kAll); bx++) wh[1].push_back(make_int4(x, bx, i, 0));
+        }
+        if (i < s->n[0]) {
+            for (int bx = 0; ie && bx < blocks(1, kFast); bx++) wef.push_back(make_int4(x, bx, i, 0));
+            for (int bx = 0; bx < blocks(1, ie ? kGeneral : kAll); bx++)
+                we[s->npole].push_back(make_int4(x, bx, i, 0));
+        }
     };
     if (b->order == 0) {
         for (int x = 0; x < (int)b->active.size(); x++)
@@ -3136,9 +3088,9 @@ int cemx_sizes(const cem_sim *s, long long *out, int n) {
     if (s->dev && s->dev->use_fused) upd = 1;
     else if (s->dev)
         for (int u = 0; u < 2; u++) {
-            const FastSegs &f = s->dev->fast[u];
-            upd -= f.n == 0 || f.p1 <= f.p0;
-            upd -= s->dev->wl_start[u].empty() || s->dev->wl_start[u].back() == 0;
+            const Device &D = *s->dev;
+            upd -= space_blocks(D.sp[u][kFast]) == 0 || D.p1[u] <= D.p0[u];
+            upd -= D.wl_start[u].empty() || D.wl_start[u].back() == 0;
         }
     v[12] = upd + 1 + (s->nsb ? 1 : 0);
     for (int q = 0; q < n && q < 13; q++) out[q] = v[q];
