@@ -1175,6 +1175,8 @@ __device__ __forceinline__ void sibc_edge(const SibcArgs &a, int e) {
     const float4 w4 = __ldg(a.hw + e);
     const uint4 i4 = __ldg(a.hidx + e);
     const uchar4 c4 = __ldg(a.hcomp + e);
+    const unsigned char ec = __ldg(a.ecomp + e);
+    const unsigned ei = __ldg(a.eidx + e);
     float y[kSibcTerms];
 #pragma unroll
     for (int k = 0; k < kSibcTerms; k++)
@@ -1184,7 +1186,7 @@ __device__ __forceinline__ void sibc_edge(const SibcArgs &a, int e) {
     const int hc[4] = {c4.x, c4.y, c4.z, c4.w};
     float h[4];
 #pragma unroll
-    for (int f = 0; f < 4; f++) h[f] = w[f] != 0.f ? a.H[hc[f]][hi[f]] : 0.f;
+    for (int f = 0; f < 4; f++) h[f] = w[f] != 0.f ? __ldg(a.H[hc[f]] + hi[f]) : 0.f;
     // explicit roundings: the same bits in every kernel that inlines this
     float J = 0.f;
 #pragma unroll
@@ -1201,7 +1203,7 @@ __device__ __forceinline__ void sibc_edge(const SibcArgs &a, int e) {
 #pragma unroll
     for (int k = 0; k < kSibcTerms; k++)
         if (k < a.K) a.y[(long long)k * a.ns + e] = y[k];
-    a.E[a.ecomp[e]][a.eidx[e]] = E;
+    a.E[ec][ei] = E;
 }
 
 __global__ void __launch_bounds__(kBlock) k_sibc(const SibcArgs a) {
@@ -1501,6 +1503,8 @@ struct Device {
     DevBuf<float> sb_y;
     // probes
     int nip = 0, nport = 0, nvp = 0, nin = 0, nslot = 0;
+    std::vector<unsigned long long> probe_e;   // (component, index) of the probes' E edges, sorted
+    bool post_beside_sibc = false;             // no probe edge is a surface-impedance edge
     DevBuf<int> off;
     DevBuf<unsigned char> ecomp;
     DevBuf<unsigned> eidx;
@@ -1872,6 +1876,10 @@ bool build_probes(cem_sim *s, Device &D) {
         }
         off.push_back((int)idx.size());
     }
+    D.probe_e.clear();
+    for (size_t e = 0; e < idx.size(); e++)
+        if (comp[e] < 3) D.probe_e.push_back((unsigned long long)comp[e] << 32 | idx[e]);
+    std::sort(D.probe_e.begin(), D.probe_e.end());
     std::vector<double> R;
     for (const LumpedPort &p : s->port) R.push_back(p.R);
     std::vector<double> omega(s->nf);
@@ -1909,6 +1917,11 @@ bool build_sibc(cem_sim *s, Device &D) {
         hidx[e] = make_uint4(q[0], q[1], q[2], q[3]);
         hw[e] = make_float4(w[0], w[1], w[2], w[3]);
     }
+    // the probe pass may run beside the surface impedance when it reads none of its edges
+    D.post_beside_sibc = true;
+    for (size_t e = 0; e < ns && D.post_beside_sibc; e++)
+        D.post_beside_sibc = !std::binary_search(D.probe_e.begin(), D.probe_e.end(),
+                                                  (unsigned long long)ecomp[e] << 32 | eidx[e]);
     return dev_upload(s, D.sb_ecomp, ecomp) && dev_upload(s, D.sb_hcomp, hcomp) && dev_upload(s, D.sb_eidx, eidx) &&
            dev_upload(s, D.sb_hidx, hidx) && dev_upload(s, D.sb_hw, hw) &&
            dev_alloc(s, D.sb_y, ns * s->sibc_npole);
@@ -2524,6 +2537,32 @@ bool end_device_op(cem_sim *s) {
     return true;
 }
 
+// Surface impedance, then the probe pass (probes, ports, sample ring, step
+// count). SIBC writes E only on its own edges and the probes only read, so
+// when no probe edge is a SIBC edge the two run side by side (SIBC on the
+// second stream, joined before the next step); one after the other while
+// kernels are timed one by one.
+void launch_sibc_post(cem_sim *s, Device &D) {
+    PostArgs pa = D.pa[D.cur];
+    pa.advance = 1;
+    const bool beside = s->nsb && D.post_beside_sibc && !g_timer;
+    const unsigned nb = (unsigned)((s->nsb + kBlock - 1) / kBlock);
+    if (beside) {
+        cudaEventRecord(D.fork, D.stream);
+        cudaStreamWaitEvent(D.side, D.fork, 0);
+        k_sibc<<<nb, kBlock, 0, D.side>>>(D.sb[D.cur]);
+        cudaEventRecord(D.join, D.side);
+    } else if (s->nsb) {
+        t_begin(2);
+        k_sibc<<<nb, kBlock, 0, D.stream>>>(D.sb[D.cur]);
+        t_end();
+    }
+    t_begin(3);
+    k_post<<<1, kPostThreads, 0, D.stream>>>(pa);
+    t_end();
+    if (beside) cudaStreamWaitEvent(D.stream, D.join, 0);
+}
+
 // one whole step: the fused H+E pass, then SIBC, probes and the step count
 bool launch_fused_step(cem_sim *s) {
     Device &D = *s->dev;
@@ -2533,12 +2572,7 @@ bool launch_fused_step(cem_sim *s) {
     kFKernels[s->npole]<<<grid, dim3(kFK, kFJ), kFusedSmem, D.stream>>>(D.sa[D.cur], D.fa[D.cur], D.maps[D.cur]);
     t_end();
     D.cur ^= 1;
-    if (s->nsb) { t_begin(2); k_sibc<<<(s->nsb + kBlock - 1) / kBlock, kBlock, 0, D.stream>>>(D.sb[D.cur]); t_end(); }
-    PostArgs pa = D.pa[D.cur];
-    pa.advance = 1;
-    t_begin(3);
-    k_post<<<1, kPostThreads, 0, D.stream>>>(pa);
-    t_end();
+    launch_sibc_post(s, D);
     D.ring_count++;
     s->step++;
     CB2_CHECK(s, cudaGetLastError());
@@ -2610,12 +2644,7 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
     }
     if (phase_mask & 8) {   // surface impedance, probes, step count
         if (D.ring_count == kRing && !flush_dft(s)) return false;
-        if (s->nsb) { t_begin(2); k_sibc<<<(s->nsb + kBlock - 1) / kBlock, blk, 0, D.stream>>>(D.sb[D.cur]); t_end(); }
-        PostArgs pa = D.pa[D.cur];
-        pa.advance = 1;
-        t_begin(3);
-        k_post<<<1, kPostThreads, 0, D.stream>>>(pa);
-        t_end();
+        launch_sibc_post(s, D);
         D.ring_count++;
         s->step++;
     }
@@ -2862,7 +2891,8 @@ struct cemx_batch {
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaStream_t side = nullptr;             // general blocks, beside the fast ones
+    cudaStream_t side = nullptr;             // general blocks beside the fast ones; SIBC beside the probes
+    bool sibc_beside = false;                // no member's probes read a SIBC edge
     cudaEvent_t fork = nullptr, join = nullptr;
     double last_ms = 0;
     long last_steps = 0, last_launches = 0;
@@ -2956,6 +2986,8 @@ bool batch_rebuild(cemx_batch *b) {
         if (!batch_upload(b->work_e[kv.first], kv.second)) return false;
         b->ne[kv.first] = kv.second.size();
     }
+    b->sibc_beside = true;
+    for (int m : b->active) b->sibc_beside = b->sibc_beside && b->members[m].s->dev->post_beside_sibc;
     b->nh[0] = wh[0].size();
     b->nh[1] = wh[1].size();
     b->nef = wef.size();
@@ -2994,8 +3026,14 @@ int batch_step(cemx_batch *b) {
         }
     if (b->nef) { k_batch_e<0, true><<<(unsigned)b->nef, kBlock, 0, b->stream>>>(b->args.p, b->work_ef.p); launches++; }
     if (side) join();
-    if (b->ns) { k_batch_sibc<<<(unsigned)b->ns, kBlock, 0, b->stream>>>(b->sargs.p, b->work_s.p); launches++; }
+    const bool beside = b->ns && b->sibc_beside;
+    if (beside) fork();
+    if (b->ns) {
+        k_batch_sibc<<<(unsigned)b->ns, kBlock, 0, beside ? b->side : b->stream>>>(b->sargs.p, b->work_s.p);
+        launches++;
+    }
     k_batch_post<<<(unsigned)b->active.size(), kPostThreads, 0, b->stream>>>(b->pargs.p);
+    if (beside) join();
     return launches + 1;
 }
 
