@@ -1530,8 +1530,12 @@ struct Device {
     // beside its fast pieces
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
+    // runs of kGraphSteps whole steps replay one captured graph (CEM_B200_GRAPHS=0: never)
+    bool use_graphs = true;
+    cudaGraphExec_t graph = nullptr;
 
     ~Device() {
+        if (graph) cudaGraphExecDestroy(graph);
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
         if (side) cudaStreamDestroy(side);
@@ -2223,6 +2227,7 @@ bool create_device_impl(cem_sim *s) {
     if (g_selected_device >= 0) CB2_CHECK(s, cudaSetDevice(g_selected_device));
     CB2_CHECK(s, cudaGetDevice(&D.device));
     if (const char *e = std::getenv("CEM_B200_FUSED")) D.use_fused = e[0] == '1';
+    if (const char *e = std::getenv("CEM_B200_GRAPHS")) D.use_graphs = e[0] != '0';
     if (s->kernel_choice >= 0) D.use_fused = s->kernel_choice == 1;
     CB2_CHECK(s, cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking));
     CB2_CHECK(s, cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
@@ -2702,11 +2707,59 @@ void engine_host_modified(cem_sim *s, unsigned groups) {
     s->dev_valid &= ~groups;
 }
 
+namespace {
+
+constexpr int kGraphSteps = 32;   // divides kRing: graph runs fill the sample ring exactly
+
+// n whole steps. With graphs on (separate H and E kernels, not while kernels
+// are timed one by one), a run of kGraphSteps steps that needs no DFT flush
+// replays one graph captured from the same launches; the others go one by one.
+// The graph holds the kernels' arguments, which stay fixed for the life of
+// the device state.
+bool run_steps(cem_sim *s, long n) {
+    Device &D = *s->dev;
+    const bool graphs = D.use_graphs && !D.use_fused && !g_timer;
+    for (long it = 0; it < n;) {
+        if (graphs && n - it >= kGraphSteps && D.ring_count + kGraphSteps <= kRing) {
+            if (!D.graph) {
+                const int rc = D.ring_count;
+                const long st = s->step;
+                CB2_CHECK(s, cudaStreamBeginCapture(D.stream, cudaStreamCaptureModeThreadLocal));
+                bool ok = true;
+                for (int q = 0; q < kGraphSteps && ok; q++) ok = launch_step(s, 1 | 4 | 8, 0, s->n[0] + 1);
+                cudaGraph_t g = nullptr;
+                const cudaError_t ec = cudaStreamEndCapture(D.stream, &g);
+                D.ring_count = rc;
+                s->step = st;
+                if (!ok) {
+                    if (g) cudaGraphDestroy(g);
+                    return false;
+                }
+                CB2_CHECK(s, ec);
+                const cudaError_t ei = cudaGraphInstantiate(&D.graph, g, 0);
+                cudaGraphDestroy(g);
+                if (ei != cudaSuccess) D.graph = nullptr;
+                CB2_CHECK(s, ei);
+            }
+            CB2_CHECK(s, cudaGraphLaunch(D.graph, D.stream));
+            D.ring_count += kGraphSteps;
+            s->step += kGraphSteps;
+            it += kGraphSteps;
+        } else {
+            if (!launch_step(s, 1 | 4 | 8, 0, s->n[0] + 1)) return false;
+            it++;
+        }
+    }
+    CB2_CHECK(s, cudaGetLastError());
+    return true;
+}
+
+}  // namespace
+
 int engine_step(cem_sim *s, long n) {
     if (n <= 0) return 0;
     if (!begin_device_op(s)) return -1;
-    for (long it = 0; it < n; it++)
-        if (!launch_step(s, 1 | 4 | 8, 0, s->n[0] + 1)) return -1;
+    if (!run_steps(s, n)) return -1;
     if (!end_device_op(s)) return -1;
     return 0;
 }
@@ -2823,8 +2876,7 @@ bool timed_steps(cem_sim *s, long n, double *ms) {
     CB2_CHECK(s, cudaEventCreate(&e0));
     CB2_CHECK(s, cudaEventCreate(&e1));
     CB2_CHECK(s, cudaEventRecord(e0, D.stream));
-    for (long it = 0; it < n; it++)
-        if (!launch_step(s, 1 | 4 | 8, 0, s->n[0] + 1)) return false;
+    if (!run_steps(s, n)) return false;
     CB2_CHECK(s, cudaEventRecord(e1, D.stream));
     CB2_CHECK(s, cudaEventSynchronize(e1));
     float t = 0;

@@ -166,6 +166,24 @@ def test_phased_stepping_matches_cem_step(lib, fused):
     assert np.array_equal(A.portV(0), B.portV(0))
 
 
+def test_graph_runs_match_single_steps(lib):
+    """cem_step replays runs of 32 steps as one captured graph; stepping 7 at a
+    time never does. Across a DFT ring flush (1024 steps) on the lossy scene
+    (SIBC, Debye, CPML) both give the same bits."""
+    A, meta = scenes.lossy_scene(lib)
+    B, _ = scenes.lossy_scene(lib)
+    A.step(1100)
+    for _ in range(1100 // 7):
+        B.step(7)
+    B.step(1100 % 7)
+    assert A.steps == B.steps == 1100
+    for c in range(6):
+        assert np.array_equal(A.field(c), B.field(c)), c
+    for p in meta["ports"]:
+        assert np.array_equal(A.portV(p), B.portV(p))
+        assert np.array_equal(A.portI(p), B.portI(p))
+
+
 def test_field_initial_condition_and_live_pointer(lib, oracle_lib):
     """Initial E written through cem_field is taken up; the pointer stays live."""
     s, meta = scenes.parity_scene(lib)
