@@ -104,8 +104,6 @@ constexpr int kFast = 0, kGeneral = 1, kAll = 2;
 
 struct StepArgs {
     Geom g;
-    Space sp[2][3];          // [H, E][kFast, kGeneral, kAll]
-    int p0[2], p1[2];        // interior node planes of H and E
     float *E[3], *H[3];
     const float *hc[3];      // dt/mu0 * idh per axis (cells)
     const float *ec[3];      // ide per axis (nodes)
@@ -128,6 +126,9 @@ struct StepArgs {
     const float *wsrc[2];    // mode-source weights of Ey and Ez on plane i_src
     const long long *dstep;
     const float *srcv;       // lumped Vs and modal Vm at this step's H time, FP32 (source_values)
+    // thread spaces last: batched kernels stage the arguments before them
+    Space sp[2][3];          // [H, E][kFast, kGeneral, kAll]
+    int p0[2], p1[2];        // interior node planes of H and E
 };
 
 struct SibcArgs {
@@ -1321,28 +1322,41 @@ __global__ void k_dft(const double *ring, int nslot, int first_e_slot, long long
 // (h_vec, e_vec, sibc_edge, post_block), so every simulation computes the
 // same bits alone and in a batch.
 
-// this simulation's arguments, copied to shared memory by the whole block
+// this simulation's arguments (their first `bytes`), copied to shared memory
+// by the whole block
 template <class T>
-__device__ __forceinline__ const T &stage_args(const T *src, unsigned *buf) {
+__device__ __forceinline__ const T &stage_args(const T *src, unsigned *buf, int bytes = sizeof(T)) {
     static_assert(sizeof(T) % 4 == 0, "arguments copied as 4-byte words");
     const unsigned *s = reinterpret_cast<const unsigned *>(src);
-    for (int q = threadIdx.x; q < (int)(sizeof(T) / 4); q += blockDim.x) buf[q] = s[q];
+    for (int q = threadIdx.x; q < bytes / 4; q += blockDim.x) buf[q] = s[q];
     __syncthreads();
     return *reinterpret_cast<const T *>(buf);
 }
 
+// the update kernels stage the arguments before the thread spaces; a thread
+// reads its position from the spaces in global memory
+constexpr int kStaged = (int)offsetof(StepArgs, sp);
+static_assert(kStaged % 4 == 0, "staged arguments end on a 4-byte boundary");
+
 // work entry: x simulation, y block of the plane (component = y % 3), z node plane
+// FAST: the member's fast rectangles (the lean kernels' code), else its general blocks
 template <bool FAST>
 __global__ void __launch_bounds__(kBlock, FAST ? CB2_HF_MINBLOCKS : CB2_H_MINBLOCKS)
     k_batch_h(const StepArgs *args, const int4 *work) {
     __shared__ unsigned buf[sizeof(StepArgs) / 4];
     const int4 w = work[blockIdx.x];
-    const StepArgs &a = stage_args(args + w.x, buf);
-    const RowPos r = FAST ? space_pos(a.sp[0][kFast], w.y / 3) : general_pos<0>(a, w.z, w.y / 3);
+    const StepArgs &a = stage_args(args + w.x, buf, kStaged);
+    const RowPos r = FAST ? space_pos(args[w.x].sp[0][kFast], w.y / 3) : general_pos<0>(args[w.x], w.z, w.y / 3);
     const int comp = w.y % 3;
-    if (comp == 0) h_vec<0, FAST>(a, w.z, r);
-    else if (comp == 1) h_vec<1, FAST>(a, w.z, r);
-    else h_vec<2, FAST>(a, w.z, r);
+    if (FAST) {
+        if (comp == 0) h_lean<0>(a, w.z, r);
+        else if (comp == 1) h_lean<1>(a, w.z, r);
+        else h_lean<2>(a, w.z, r);
+    } else {
+        if (comp == 0) h_vec<0, false>(a, w.z, r);
+        else if (comp == 1) h_vec<1, false>(a, w.z, r);
+        else h_vec<2, false>(a, w.z, r);
+    }
 }
 
 template <int P, bool FAST>
@@ -1350,13 +1364,19 @@ __global__ void __launch_bounds__(kBlock, FAST ? CB2_EF_MINBLOCKS : CB2_E_MINBLO
     k_batch_e(const StepArgs *args, const int4 *work) {
     __shared__ unsigned buf[sizeof(StepArgs) / 4];
     const int4 w = work[blockIdx.x];
-    const StepArgs &a = stage_args(args + w.x, buf);
-    const RowPos r = FAST ? space_pos(a.sp[1][kFast], w.y / 3) : general_pos<1>(a, w.z, w.y / 3);
+    const StepArgs &a = stage_args(args + w.x, buf, kStaged);
+    const RowPos r = FAST ? space_pos(args[w.x].sp[1][kFast], w.y / 3) : general_pos<1>(args[w.x], w.z, w.y / 3);
     const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
     const int comp = w.y % 3;
-    if (comp == 0) e_vec<0, P, FAST>(a, w.z, r, sv);
-    else if (comp == 1) e_vec<1, P, FAST>(a, w.z, r, sv);
-    else e_vec<2, P, FAST>(a, w.z, r, sv);
+    if (FAST) {
+        if (comp == 0) e_lean<0>(a, w.z, r, sv);
+        else if (comp == 1) e_lean<1>(a, w.z, r, sv);
+        else e_lean<2>(a, w.z, r, sv);
+    } else {
+        if (comp == 0) e_vec<0, P, false>(a, w.z, r, sv);
+        else if (comp == 1) e_vec<1, P, false>(a, w.z, r, sv);
+        else e_vec<2, P, false>(a, w.z, r, sv);
+    }
 }
 
 using BEKernel = void (*)(const StepArgs *, const int4 *);
