@@ -1339,47 +1339,88 @@ constexpr int kStaged = (int)offsetof(StepArgs, sp);
 static_assert(kStaged % 4 == 0, "staged arguments end on a 4-byte boundary");
 
 // work entry: x simulation, y block of the plane (component = y % 3), z node plane
-// FAST: the member's fast rectangles (the lean kernels' code), else its general blocks
+// A batched update block walks kPerBlock consecutive work entries (x
+// member, y block of the plane incl. component, z node plane) and stages a
+// member's arguments only when the member changes: the arguments before the
+// thread spaces, the interior planes and the spaces it walks (the fast one,
+// or the general one and the one of all rectangles), each at its own offset,
+// so the buffer reads as the member's StepArgs.
+constexpr int kPerBlock = 4;
+
+template <int U, bool FAST>
+__device__ __forceinline__ void stage_member(const StepArgs *args, int x, unsigned *buf) {
+    __syncthreads();   // every thread is done with the previous member
+    const unsigned *s = reinterpret_cast<const unsigned *>(args + x);
+    for (int q = threadIdx.x; q < kStaged / 4; q += blockDim.x) buf[q] = s[q];
+    constexpr int sw = (int)(sizeof(Space) / 4);
+    const int c0 = FAST ? kFast : kGeneral;
+    for (int c = c0; c <= (FAST ? kFast : kAll); c++) {
+        const int off = (int)((offsetof(StepArgs, sp) + (U * 3 + c) * sizeof(Space)) / 4);
+        for (int q = threadIdx.x; q < sw; q += blockDim.x) buf[off + q] = s[off + q];
+    }
+    constexpr int po = (int)(offsetof(StepArgs, p0) / 4);
+    if (threadIdx.x < 4) buf[po + threadIdx.x] = s[po + threadIdx.x];   // p0[2], p1[2]
+    __syncthreads();
+}
+
+// FAST: the members' fast rectangles (the lean kernels' code), else their general blocks
 template <bool FAST>
 __global__ void __launch_bounds__(kBlock, FAST ? CB2_HF_MINBLOCKS : CB2_H_MINBLOCKS)
-    k_batch_h(const StepArgs *args, const int4 *work) {
+    k_batch_h(const StepArgs *args, const int4 *work, int n) {
+    static_assert(offsetof(StepArgs, p0) % 4 == 0 && offsetof(StepArgs, p1) == offsetof(StepArgs, p0) + 8, "p0, p1");
     __shared__ unsigned buf[sizeof(StepArgs) / 4];
-    const int4 w = work[blockIdx.x];
-    const StepArgs &a = stage_args(args + w.x, buf, kStaged);
-    const RowPos r = FAST ? space_pos(args[w.x].sp[0][kFast], w.y / 3) : general_pos<0>(args[w.x], w.z, w.y / 3);
-    const int comp = w.y % 3;
-    if (FAST) {
-        if (comp == 0) h_lean<0>(a, w.z, r);
-        else if (comp == 1) h_lean<1>(a, w.z, r);
-        else h_lean<2>(a, w.z, r);
-    } else {
-        if (comp == 0) h_vec<0, false>(a, w.z, r);
-        else if (comp == 1) h_vec<1, false>(a, w.z, r);
-        else h_vec<2, false>(a, w.z, r);
+    const StepArgs &a = *reinterpret_cast<const StepArgs *>(buf);
+    int staged = -1;
+    const int e1 = min(n, (int)(blockIdx.x + 1) * kPerBlock);
+    for (int e = blockIdx.x * kPerBlock; e < e1; e++) {
+        const int4 w = work[e];
+        if (w.x != staged) {
+            stage_member<0, FAST>(args, w.x, buf);
+            staged = w.x;
+        }
+        const RowPos r = FAST ? space_pos(a.sp[0][kFast], w.y / 3) : general_pos<0>(a, w.z, w.y / 3);
+        const int comp = w.y % 3;
+        if (FAST) {
+            if (comp == 0) h_lean<0>(a, w.z, r);
+            else if (comp == 1) h_lean<1>(a, w.z, r);
+            else h_lean<2>(a, w.z, r);
+        } else {
+            if (comp == 0) h_vec<0, false>(a, w.z, r);
+            else if (comp == 1) h_vec<1, false>(a, w.z, r);
+            else h_vec<2, false>(a, w.z, r);
+        }
     }
 }
 
 template <int P, bool FAST>
 __global__ void __launch_bounds__(kBlock, FAST ? CB2_EF_MINBLOCKS : CB2_E_MINBLOCKS)
-    k_batch_e(const StepArgs *args, const int4 *work) {
+    k_batch_e(const StepArgs *args, const int4 *work, int n) {
     __shared__ unsigned buf[sizeof(StepArgs) / 4];
-    const int4 w = work[blockIdx.x];
-    const StepArgs &a = stage_args(args + w.x, buf, kStaged);
-    const RowPos r = FAST ? space_pos(args[w.x].sp[1][kFast], w.y / 3) : general_pos<1>(args[w.x], w.z, w.y / 3);
-    const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
-    const int comp = w.y % 3;
-    if (FAST) {
-        if (comp == 0) e_lean<0>(a, w.z, r, sv);
-        else if (comp == 1) e_lean<1>(a, w.z, r, sv);
-        else e_lean<2>(a, w.z, r, sv);
-    } else {
-        if (comp == 0) e_vec<0, P, false>(a, w.z, r, sv);
-        else if (comp == 1) e_vec<1, P, false>(a, w.z, r, sv);
-        else e_vec<2, P, false>(a, w.z, r, sv);
+    const StepArgs &a = *reinterpret_cast<const StepArgs *>(buf);
+    int staged = -1;
+    const int e1 = min(n, (int)(blockIdx.x + 1) * kPerBlock);
+    for (int e = blockIdx.x * kPerBlock; e < e1; e++) {
+        const int4 w = work[e];
+        if (w.x != staged) {
+            stage_member<1, FAST>(args, w.x, buf);
+            staged = w.x;
+        }
+        const RowPos r = FAST ? space_pos(a.sp[1][kFast], w.y / 3) : general_pos<1>(a, w.z, w.y / 3);
+        const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
+        const int comp = w.y % 3;
+        if (FAST) {
+            if (comp == 0) e_lean<0>(a, w.z, r, sv);
+            else if (comp == 1) e_lean<1>(a, w.z, r, sv);
+            else e_lean<2>(a, w.z, r, sv);
+        } else {
+            if (comp == 0) e_vec<0, P, false>(a, w.z, r, sv);
+            else if (comp == 1) e_vec<1, P, false>(a, w.z, r, sv);
+            else e_vec<2, P, false>(a, w.z, r, sv);
+        }
     }
 }
 
-using BEKernel = void (*)(const StepArgs *, const int4 *);
+using BEKernel = void (*)(const StepArgs *, const int4 *, int);
 #define CB2_BE(p) k_batch_e<p, false>,
 const BEKernel kBEKernels[] = {CB2_BE(0) CB2_BE(1) CB2_BE(2) CB2_BE(3) CB2_BE(4) CB2_BE(5) CB2_BE(6) CB2_BE(7) CB2_BE(8)
                                    CB2_BE(9) CB2_BE(10) CB2_BE(11) CB2_BE(12) CB2_BE(13) CB2_BE(14) CB2_BE(15)
@@ -3068,6 +3109,9 @@ bool batch_rebuild(cemx_batch *b) {
     return true;
 }
 
+// blocks of a batched update launch over n work entries
+unsigned blocks_for(size_t n) { return (unsigned)((n + kPerBlock - 1) / kPerBlock); }
+
 // one batched time step: H (fast, general blocks), E (fast blocks; general
 // blocks one launch per pole count), SIBC, probes
 int batch_step(cemx_batch *b) {
@@ -3083,20 +3127,27 @@ int batch_step(cemx_batch *b) {
     };
     if (b->nh[1]) {
         fork();
-        k_batch_h<false><<<(unsigned)b->nh[1], kBlock, 0, b->side>>>(b->args.p, b->work_h[1].p);
+        k_batch_h<false><<<blocks_for(b->nh[1]), kBlock, 0, b->side>>>(b->args.p, b->work_h[1].p, (int)b->nh[1]);
         launches++;
     }
-    if (b->nh[0]) { k_batch_h<true><<<(unsigned)b->nh[0], kBlock, 0, b->stream>>>(b->args.p, b->work_h[0].p); launches++; }
+    if (b->nh[0]) {
+        k_batch_h<true><<<blocks_for(b->nh[0]), kBlock, 0, b->stream>>>(b->args.p, b->work_h[0].p, (int)b->nh[0]);
+        launches++;
+    }
     if (b->nh[1]) join();
     bool side = false;
     for (auto &kv : b->ne)
         if (kv.second) {
             if (!side) fork();
             side = true;
-            kBEKernels[kv.first]<<<(unsigned)kv.second, kBlock, 0, b->side>>>(b->args.p, b->work_e[kv.first].p);
+            kBEKernels[kv.first]<<<blocks_for(kv.second), kBlock, 0, b->side>>>(b->args.p, b->work_e[kv.first].p,
+                                                                               (int)kv.second);
             launches++;
         }
-    if (b->nef) { k_batch_e<0, true><<<(unsigned)b->nef, kBlock, 0, b->stream>>>(b->args.p, b->work_ef.p); launches++; }
+    if (b->nef) {
+        k_batch_e<0, true><<<blocks_for(b->nef), kBlock, 0, b->stream>>>(b->args.p, b->work_ef.p, (int)b->nef);
+        launches++;
+    }
     if (side) join();
     const bool beside = b->ns && b->sibc_beside;
     if (beside) fork();
