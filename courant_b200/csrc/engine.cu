@@ -31,6 +31,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
+#include <thread>
 #include <map>
 #include <mutex>
 #include <string>
@@ -1737,17 +1739,26 @@ struct TableBuilder {
     }
 };
 
+// Material tables of the three E components, one thread each. Entries are
+// numbered in order of first appearance along (i, j, k); a point whose
+// coefficient row equals the previous point's takes its entry without a
+// lookup. The lumped-source and Debye edges of a component are walked as
+// sorted lists beside the grid loop (reference indices grow with it).
 bool build_tables(cem_sim *s, Device &D) {
     const int P = s->npole;
     const int nfields = 3 + P;
     // per-edge extras: lumped source coefficient (excited port only), Debye beta/dt
-    std::vector<std::unordered_map<size_t, double>> src(3);
+    std::vector<std::vector<std::pair<size_t, double>>> src(3);
     if (s->src_port >= 0) {
         const LumpedPort &pt = s->port[s->src_port];
-        for (size_t e = 0; e < pt.edge.size(); e++) src[pt.axis][pt.edge[e]] = pt.cs[e];
+        for (size_t e = 0; e < pt.edge.size(); e++) src[pt.axis].push_back({pt.edge[e], pt.cs[e]});
     }
-    std::vector<std::unordered_map<size_t, int>> disp(3);
-    for (int e = 0; e < s->ndisp; e++) disp[s->d_comp[e]][s->d_idx[e]] = e;
+    std::vector<std::vector<std::pair<size_t, int>>> disp(3);
+    for (int e = 0; e < s->ndisp; e++) disp[s->d_comp[e]].push_back({s->d_idx[e], e});
+    for (int c = 0; c < 3; c++) {   // stable: of equal indices the last one counts, as a map assignment would
+        std::stable_sort(src[c].begin(), src[c].end(), [](const auto &x, const auto &y) { return x.first < y.first; });
+        std::stable_sort(disp[c].begin(), disp[c].end(), [](const auto &x, const auto &y) { return x.first < y.first; });
+    }
     // mode-source weights of Ey, Ez on the source plane (reference index j*(nz+1)+k)
     int msrc_i = -1;
     std::vector<float> wsrc[2];
@@ -1759,12 +1770,27 @@ bool build_tables(cem_sim *s, Device &D) {
             wsrc[mp.src_comp[e] - 1][mp.src_idx[e] % s->si] += (float)mp.src_w[e];
     }
     const int *n = s->n;
-    for (int c = 0; c < 3; c++) {
-        TableBuilder tb(nfields);
-        std::vector<unsigned short> mat(D.Np, 0);
-        std::vector<float> row(nfields);
-        int box_lo[3] = {n[0], n[1], n[2]}, box_hi[3] = {-1, -1, -1};
-        std::string last_key;
+    struct Built {
+        TableBuilder tb;
+        std::vector<unsigned short> mat;
+        int box_lo[3], box_hi[3];
+        bool overflow = false;
+        explicit Built(int nf) : tb(nf) {}
+    };
+    std::vector<std::unique_ptr<Built>> out;
+    for (int c = 0; c < 3; c++) out.emplace_back(new Built(nfields));
+    auto build = [&](int c) {
+        Built &b = *out[c];
+        TableBuilder &tb = b.tb;
+        std::vector<unsigned short> &mat = b.mat;
+        mat.assign(D.Np, 0);
+        std::vector<float> row(nfields), prev(nfields);
+        unsigned char prev_flag = 0;
+        int prev_id = -1;
+        for (int a = 0; a < 3; a++) { b.box_lo[a] = n[a]; b.box_hi[a] = -1; }
+        const auto &sc = src[c];
+        const auto &dc = disp[c];
+        size_t ss = 0, ds = 0;
         for (int i = 0; i <= n[0]; i++)
             for (int j = 0; j <= n[1]; j++)
                 for (int k = 0; k <= n[2]; k++) {
@@ -1777,28 +1803,53 @@ bool build_tables(cem_sim *s, Device &D) {
                     row[0] = (float)(ca - 1.0);
                     row[1] = (float)cb;
                     unsigned char flag = 0;
-                    auto it = src[c].find(q);
-                    if (it != src[c].end()) { row[2] = (float)it->second; flag |= kFlagSrc; }
+                    while (ss < sc.size() && sc[ss].first < q) ss++;
+                    if (ss < sc.size() && sc[ss].first == q) {
+                        while (ss + 1 < sc.size() && sc[ss + 1].first == q) ss++;
+                        row[2] = (float)sc[ss].second;
+                        flag |= kFlagSrc;
+                    }
                     if (c > 0 && i == msrc_i && wsrc[c - 1][(size_t)j * (n[2] + 1) + k] != 0.f) flag |= kFlagMode;
-                    auto dt_ = disp[c].find(q);
-                    if (dt_ != disp[c].end()) {
+                    while (ds < dc.size() && dc[ds].first < q) ds++;
+                    if (ds < dc.size() && dc[ds].first == q) {
+                        while (ds + 1 < dc.size() && dc[ds + 1].first == q) ds++;
                         flag |= kFlagDisp;
                         for (int p = 0; p < P; p++)
-                            row[3 + p] = (float)(s->d_beta[(size_t)p * s->ndisp + dt_->second] / s->dt);
+                            row[3 + p] = (float)(s->d_beta[(size_t)p * s->ndisp + dc[ds].second] / s->dt);
                         for (int a = 0; a < 3; a++) {
-                            box_lo[a] = std::min(box_lo[a], ijk[a]);
-                            box_hi[a] = std::max(box_hi[a], ijk[a]);
+                            b.box_lo[a] = std::min(b.box_lo[a], ijk[a]);
+                            b.box_hi[a] = std::max(b.box_hi[a], ijk[a]);
                         }
                     }
-                    const int id = tb.add(row.data(), flag, cb);
+                    int id = prev_id;
+                    if (id < 0 || flag != prev_flag || std::memcmp(row.data(), prev.data(), nfields * sizeof(float))) {
+                        id = tb.add(row.data(), flag, cb);
+                        prev = row;
+                        prev_flag = flag;
+                        prev_id = id;
+                    }
                     if (id > 65535) {
-                        set_error("more than 65535 distinct update coefficients on one component");
-                        return false;
+                        b.overflow = true;
+                        return;
                     }
                     mat[(size_t)i * D.g.si + (size_t)j * D.g.sj + k] = (unsigned short)id;
                 }
+    };
+    {
+        std::vector<std::thread> th;
+        for (int c = 0; c < 3; c++) th.emplace_back(build, c);
+        for (auto &x : th) x.join();
+    }
+    for (int c = 0; c < 3; c++) {
+        Built &b = *out[c];
+        if (b.overflow) {
+            set_error("more than 65535 distinct update coefficients on one component");
+            return false;
+        }
+        TableBuilder &tb = b.tb;
+        const int *box_lo = b.box_lo, *box_hi = b.box_hi;
         D.ntab[c] = (int)tb.flags.size();
-        if (!dev_upload(s, D.mat[c], mat)) return false;
+        if (!dev_upload(s, D.mat[c], b.mat)) return false;
         if (!dev_upload(s, D.tab[c], tb.field_major())) return false;
         {
             const size_t ne = tb.flags.size();
