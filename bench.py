@@ -220,8 +220,7 @@ def batch_compare(lib, runs: int, seed: int = 2026) -> dict:
     t0 = time.perf_counter()
     for (s, _), (_, _, n, _) in zip(sims, spec):
         s.step(n)
-    for s, _ in sims:
-        s.synchronize()
+        s.synchronize()   # one at a time: cem_step returns before its device work ends
     t_plain = time.perf_counter() - t0
     plain = [serve.results(s, m)["S21"] for s, m in sims]
     for s, _ in sims:
