@@ -3050,7 +3050,7 @@ struct cemx_batch {
     std::map<int, size_t> ne;
     bool dirty = true;
     int order = 0;                           // work-list order: 0 member-major, 1 plane-interleaved
-    int chunk = 64;                          // steps per graph launch
+    int chunk = 256;                         // steps between the host's checks of budgets and rings
     bool tune = false, tuned = false;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
@@ -3212,24 +3212,30 @@ int batch_step(cemx_batch *b) {
 }
 
 // n batched steps, through the cached graph when n is the chunk length
+// n batched steps: whole runs of kBatchGraph steps replay the graph captured
+// for the current composition (captured once per composition, so a change of
+// members costs one short capture), the rest go step by step
+constexpr int kBatchGraph = 16;
+
 bool batch_launch(cemx_batch *b, int n) {
-    if (n == b->chunk) {
-        if (!b->graph || b->graph_steps != n) {
+    if (n >= kBatchGraph) {
+        if (!b->graph || b->graph_steps != kBatchGraph) {
             batch_drop_graph(b);
             cudaGraph_t g = nullptr;
             CB2_BCHECK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-            for (int q = 0; q < n; q++) batch_step(b);
+            for (int q = 0; q < kBatchGraph; q++) batch_step(b);
             CB2_BCHECK(cudaStreamEndCapture(b->stream, &g));
             const cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) { b->graph = nullptr; return batch_fail("cudaGraphInstantiate", e); }
-            b->graph_steps = n;
+            b->graph_steps = kBatchGraph;
         }
-        CB2_BCHECK(cudaGraphLaunch(b->graph, b->stream));
-        b->last_launches += 1;
-    } else {
-        for (int q = 0; q < n; q++) b->last_launches += batch_step(b);
+        for (int q = 0; q + kBatchGraph <= n; q += kBatchGraph) {
+            CB2_BCHECK(cudaGraphLaunch(b->graph, b->stream));
+            b->last_launches += 1;
+        }
     }
+    for (int q = n / kBatchGraph * kBatchGraph; q < n; q++) b->last_launches += batch_step(b);
     CB2_BCHECK(cudaGetLastError());
     return true;
 }
@@ -3465,7 +3471,7 @@ int cemx_batch_run(cemx_batch *b, long max_steps) {
                 for (int m : b->active) minleft = std::min(minleft, b->members[m].left);
                 float best_ms = 1e30f;
                 for (int order = 0; order < 2; order++)
-                    for (int ch : {16, 64, 256}) {
+                    for (int ch : {64}) {
                         if (2 * ch > minleft) continue;   // one warm-up and one timed chunk
                         if (b->order != order) { b->order = order; if (!batch_rebuild(b)) return -1; }
                         b->chunk = ch;
@@ -3505,7 +3511,6 @@ int cemx_batch_run(cemx_batch *b, long max_steps) {
             }
             b->tuned = true;
             if (b->order != best.second) { b->order = best.second; b->dirty = true; }
-            b->chunk = best.first;
             for (int m : b->active)
                 if (b->members[m].left <= 0) b->dirty = true;
             continue;
@@ -3546,7 +3551,7 @@ int cemx_batch_run(cemx_batch *b, long max_steps) {
 
 int cemx_batch_stats(const cemx_batch *b, double *out, int n) {
     if (!b) return -1;
-    const double v[6] = {b->last_ms, (double)b->last_steps, (double)b->last_launches, (double)b->chunk,
+    const double v[6] = {b->last_ms, (double)b->last_steps, (double)b->last_launches, (double)kBatchGraph,
                          (double)b->order, (double)b->members.size()};
     for (int q = 0; q < n && q < 6; q++) out[q] = v[q];
     return 0;

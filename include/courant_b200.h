@@ -79,7 +79,7 @@ CEM_API int cemx_energy_noalloc(cem_sim *s, double *energy);
 /* Batches (no counterpart in the reference core). A batch advances several
  * finalized simulations on one device together: every batched launch walks a
  * work-list of blocks across all members (H, E, surface impedance, probes),
- * and runs of `chunk` steps replay one captured CUDA graph. Each member
+ * and runs of 16 steps replay one CUDA graph captured per composition. Each member
  * computes the same bits as when stepped alone with cem_step. Members keep
  * their own device state, so results are read with the usual courant.h calls
  * between runs. A simulation belongs to at most one batch and must not be
@@ -106,8 +106,8 @@ CEM_API long cemx_batch_left(const cemx_batch *b, const cem_sim *s);
  * Returns the number of members still short of their budget, or -1. */
 CEM_API int cemx_batch_run(cemx_batch *b, long max_steps);
 
-/* on = 1: the next run picks the graph length (16, 64 or 256 steps) and the
- * work-list order by timing real steps, once per batch composition per
+/* on = 1: the next run picks the work-list order (member-major or plane by
+ * plane across members) by timing real steps, once per batch composition per
  * process. Returns the previous setting. */
 CEM_API int cemx_batch_tune(cemx_batch *b, int on);
 
