@@ -52,9 +52,18 @@ def spectrum_errors(gpu, orc, meta):
     return {k: float(np.max(np.abs(sg[k] - so[k])) / max(np.max(np.abs(so[k])), 1e-300)) for k in sg}
 
 
+def board_scene(lib):
+    """A seeded 4-layer board (three Debye cores at different heights, CPML
+    on five faces, traces, vias, lumped ports): many update rectangles of
+    every class, so a block classed fast by mistake would show here."""
+    from courant_b200 import boards
+    s, meta = boards.seeded_board(lib, 7, 1.2e5, ports="lumped", nf=16, steps=800, excite=1)
+    return s, meta
+
+
 @pytest.mark.parametrize("fused", [False, True], ids=["separate", "fused"])
-@pytest.mark.parametrize("fn", [scenes.parity_scene, scenes.lossy_scene, scenes.modeport_scene],
-                         ids=["parity", "lossy", "modeport"])
+@pytest.mark.parametrize("fn", [scenes.parity_scene, scenes.lossy_scene, scenes.modeport_scene, board_scene],
+                         ids=["parity", "lossy", "modeport", "board"])
 def test_scene_against_oracle(lib, oracle_lib, fn, fused):
     """At step 600 (fields near their peak, the step of the reference's own
     GPU-vs-CPU check) every component is within relative L2 1e-5 of the f64
