@@ -46,7 +46,11 @@
 namespace cb2 {
 
 constexpr int kRing = 1024;          // sample rows kept on the device between DFT flushes
-constexpr int kBlock = 256;
+#ifndef CB2_BLOCK
+#define CB2_BLOCK 128
+#endif
+constexpr int kBlock = CB2_BLOCK;   // threads per block of the update and SIBC kernels
+constexpr int kEnergyBlock = 256;   // threads per block of the energy kernel (one partial per block)
 constexpr int kMaxSlots = 2 * kMaxProbes + kMaxPorts;
 constexpr int kPostThreads = 1024;   // k_post: one block
 constexpr int kMaxGridY = 65535;     // launches over node planes are split into chunks of this many
@@ -882,21 +886,22 @@ __device__ __forceinline__ void e_lean(const StepArgs &a, int i, const RowPos &p
 }
 
 // H over node planes [i0, i0 + gridDim.y) (cem_mt_H and the unfused step)
-// Resident blocks per SM the update kernels are compiled for (register caps
-// of 51 and 64 per thread at the default 5 and 4: occupancy hides the
-// memory latency; the rarer CPML and Debye paths spill a little)
+// Resident blocks (of kBlock threads) per SM the update kernels are
+// compiled for: register caps of 51 and 64 per thread for the general H and
+// E kernels at the default 10 and 8 (the rarer CPML and Debye paths spill a
+// little), 32 and 51 for the lean ones at 16 and 10
 #ifndef CB2_H_MINBLOCKS
-#define CB2_H_MINBLOCKS 5
+#define CB2_H_MINBLOCKS 10
 #endif
 #ifndef CB2_E_MINBLOCKS
-#define CB2_E_MINBLOCKS 4
+#define CB2_E_MINBLOCKS 8
 #endif
 
 #ifndef CB2_HF_MINBLOCKS
-#define CB2_HF_MINBLOCKS 8
+#define CB2_HF_MINBLOCKS 16
 #endif
 #ifndef CB2_EF_MINBLOCKS
-#define CB2_EF_MINBLOCKS 5
+#define CB2_EF_MINBLOCKS 10
 #endif
 
 // H on the fast rectangles of node planes [i0, i0 + gridDim.y); block x:
@@ -1454,10 +1459,10 @@ struct EnergyArgs {
 };
 
 // W = 1/2 sum eps E^2 dV + 1/2 sum mu0 H^2 dV with eps = dt/cb (reference sim.c:970-994)
-__global__ void __launch_bounds__(kBlock) k_energy(const EnergyArgs a, int i0) {
-    __shared__ double red[kBlock / 32];
+__global__ void __launch_bounds__(kEnergyBlock) k_energy(const EnergyArgs a, int i0) {
+    __shared__ double red[kEnergyBlock / 32];
     const int i = i0 + blockIdx.y;
-    const int m = blockIdx.x * kBlock + threadIdx.x;
+    const int m = blockIdx.x * kEnergyBlock + threadIdx.x;
     double acc = 0;
     const int j = (int)(((unsigned long long)m * a.g.sj_magic) >> 40);
     const int k = m - j * a.g.sj;
@@ -1486,7 +1491,7 @@ __global__ void __launch_bounds__(kBlock) k_energy(const EnergyArgs a, int i0) {
     __syncthreads();
     if (threadIdx.x == 0) {
         double s = 0;
-        for (int w = 0; w < kBlock / 32; w++) s += red[w];
+        for (int w = 0; w < kEnergyBlock / 32; w++) s += red[w];
         a.partial[(long long)i * gridDim.x + blockIdx.x] = s;
     }
 }
@@ -2377,7 +2382,7 @@ bool create_device_impl(cem_sim *s) {
                 return false;
     if (!dev_alloc(s, D.error, 1) || !zero_dev(s, D.error.p, 4)) return false;
     CB2_CHECK(s, cudaFuncSetAttribute(kFKernels[s->npole], cudaFuncAttributeMaxDynamicSharedMemorySize, kFusedSmem));
-    const long long nblk = (long long)((g.plane + kBlock - 1) / kBlock) * (s->n[0] + 1);
+    const long long nblk = (long long)((g.plane + kEnergyBlock - 1) / kEnergyBlock) * (s->n[0] + 1);
     if (!dev_alloc(s, D.partial, (size_t)nblk) || !dev_alloc(s, D.scalar, 1)) return false;
     fill_args(s, D);
     return true;
@@ -2890,9 +2895,9 @@ namespace {
 bool energy_on_device(cem_sim *s, double *out) {
     if (!begin_device_op(s)) return false;
     Device &D = *s->dev;
-    const int gx = (D.g.plane + kBlock - 1) / kBlock;
+    const int gx = (D.g.plane + kEnergyBlock - 1) / kEnergyBlock;
     for (int c0 = 0; c0 <= s->n[0]; c0 += kMaxGridY)
-        k_energy<<<dim3(gx, std::min(kMaxGridY, s->n[0] + 1 - c0)), kBlock, 0, D.stream>>>(D.ea[D.cur], c0);
+        k_energy<<<dim3(gx, std::min(kMaxGridY, s->n[0] + 1 - c0)), kEnergyBlock, 0, D.stream>>>(D.ea[D.cur], c0);
     k_sum<<<1, 1024, 0, D.stream>>>(D.partial.p, (long long)gx * (s->n[0] + 1), D.scalar.p);
     CB2_CHECK(s, cudaGetLastError());
     CB2_CHECK(s, cudaMemcpyAsync(out, D.scalar.p, sizeof(double), cudaMemcpyDeviceToHost, D.stream));
@@ -2952,7 +2957,7 @@ bool energy_noalloc(cem_sim *s, double *out) {
         set_error("cemx_energy_noalloc: fields are held or modified on the host; use cem_energy");
         return false;
     }
-    const int gx = (D.g.plane + kBlock - 1) / kBlock;
+    const int gx = (D.g.plane + kEnergyBlock - 1) / kEnergyBlock;
     const long long nblk = (long long)gx * (s->n[0] + 1);
     if (nblk > kNoAllocPartials) {
         char msg[256];
@@ -2968,7 +2973,7 @@ bool energy_noalloc(cem_sim *s, double *out) {
     EnergyArgs ea = D.ea[D.cur];
     ea.partial = scratch;
     for (int c0 = 0; c0 <= s->n[0]; c0 += kMaxGridY)
-        k_energy<<<dim3(gx, std::min(kMaxGridY, s->n[0] + 1 - c0)), kBlock, 0, D.stream>>>(ea, c0);
+        k_energy<<<dim3(gx, std::min(kMaxGridY, s->n[0] + 1 - c0)), kEnergyBlock, 0, D.stream>>>(ea, c0);
     k_sum<<<1, 1024, 0, D.stream>>>(scratch, nblk, scratch + kNoAllocPartials);
     CB2_CHECK(s, cudaGetLastError());
     CB2_CHECK(s, cudaMemcpyAsync(out, scratch + kNoAllocPartials, sizeof(double), cudaMemcpyDeviceToHost, D.stream));
