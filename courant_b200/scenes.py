@@ -186,7 +186,8 @@ def gcpw_line(c: Courant, *, w=0.45e-3, gap=0.2e-3, h=0.254e-3, er=4.3, length=1
     tau = math.sqrt(6.9) / (math.pi * 1.25 * fmax)
     jl, jr = _nearest(Y, -(a + b) / 2), _nearest(Y, (a + b) / 2)
     ja, jb = max(jl, 0), jr - 1
-    meta = {"dims": (nx, ny, nz), "cells": nx * ny * nz, "ip1": ip1, "ip2": ip2, "tau": tau, "steps": steps}
+    meta = {"dims": (nx, ny, nz), "cells": nx * ny * nz, "ip1": ip1, "ip2": ip2, "tau": tau, "steps": steps,
+            "excite": excite}
     if not modeports:
         p1 = s.addLumpedPort(Z, ip1, j0, 0, kh, -1, 50.0)
         p2 = s.addLumpedPort(Z, ip2, j0, 0, kh, -1, 50.0)
@@ -214,6 +215,44 @@ def gcpw_line(c: Courant, *, w=0.45e-3, gap=0.2e-3, h=0.254e-3, er=4.3, length=1
         meta["iprobes"] = [s.addIProbe(X, (ip1 + ip2) // 2, ja, jb, kh - 1, kt)]
     s.finalize(cfl)
     return s, meta
+
+
+# The two GCPW configurations of the benchmark, as gcpw_line keyword sets.
+# c1: lossless GCPW, lumped 50-ohm ports, eps_r 4.3, h 254 um, w 450 um, gap 200 um, 10 mm, graded 25-200 um
+#     (121 x 62 x 40 cells), 20 000 steps, 401 frequencies 0-40 GHz.
+# c2: the same line with 35 um copper, a 20 um eps_r 3.5 mask, a Djordjevic-Sarkar substrate (6 Debye poles), copper
+#     surface impedance with Huray roughness (sphere radius 0.5 um, 2e11 spheres per m^2 of flat area:
+#     K(inf) = 1 + 4 pi a^2 N = 1.63, standing in for Rq = 1 um), 2D eigenmode ports (416 x 161 x 86 cells),
+#     40 000 steps, 400 frequencies 0.1-40 GHz.
+CONFIGS = {
+    "c1": dict(desc="lossless GCPW, lumped 50-ohm ports, er 4.3, h 254um, w 450um, gap 200um, 10 mm",
+               kw=dict(hmin=25e-6, hmax=200e-6, dx=105e-6, zair=4.2e-3, yair=0.9e-3, steps=20000)),
+    "c2": dict(desc="lossy GCPW 2-port: DS substrate (6 Debye poles), 35um Cu + Huray SIBC, 20um mask, mode ports",
+               kw=dict(hmin=10e-6, hmax=30e-6, dx=45e-6, yair=1.2e-3, zair=1.8e-3, tcu=35e-6, mask=20e-6,
+                       debye_poles=6, sigma_cu=5.8e7, huray=(0.5e-6, 2.0e11), modeports=True, steps=40000)),
+}
+
+
+def config_line(c: Courant, name: str, excite: int = 1, **over):
+    """One of the benchmark GCPW configurations (CONFIGS), driven at port `excite`."""
+    return gcpw_line(c, **dict(CONFIGS[name]["kw"], excite=excite, **over))
+
+
+def two_port_s(s, meta: dict) -> dict:
+    """The excited column of the modal or lumped S-matrix: the waves at both
+    ports divided by the incident wave at the driven port. Mode ports use
+    cem_mode_port_waves (a, b at the reference planes, normalised to each port's
+    own Z0); lumped ports use V and I with the 50-ohm port resistance."""
+    e = meta.get("excite", 1) - 1
+    if "modeports" in meta:
+        w = [s.modePortWaves(p) for p in meta["modeports"]]
+        a = w[e]["a"]
+        return {"b": [w[0]["b"] / a, w[1]["b"] / a], "z0": [w[0]["z0"], w[1]["z0"]], "beta": [w[0]["beta"], w[1]["beta"]]}
+    v = [s.portV(p) for p in meta["ports"]]
+    i = [s.portI(p) for p in meta["ports"]]
+    sq = np.sqrt(50.0)
+    a = (v[e] + 50.0 * i[e]) / (2 * sq)
+    return {"b": [(v[q] - 50.0 * i[q]) / (2 * sq) / a for q in range(2)]}
 
 
 def modeport_scene(c: Courant):

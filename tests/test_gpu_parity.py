@@ -246,6 +246,36 @@ def test_gcpw_lumped_sparams(lib, oracle_lib, fused):
     assert cmp["ok"], cmp
 
 
+def test_reference_parity_program_through_the_drop_in():
+    """The reference's known-answer program solver/apps/parity.c, compiled
+    unchanged against libcourant_b200 (oracle/_ref/dropin_parity): its printout
+    matches the reference's own (tests/golden/parity_scene.txt): dt to the
+    bit, energy and every spectrum entry within 1e-5 of the largest entry of
+    its array."""
+    exe = ROOT / "oracle" / "_ref" / "dropin_parity"
+    if not exe.exists():
+        pytest.skip(f"{exe.name} not built (make -C oracle dropin)")
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+    def parse(txt):
+        out = {}
+        for line in txt.splitlines():
+            k, *v = line.split()
+            out[k] = np.array([float(x) for x in v])
+        return out
+
+    got, ref = parse(r.stdout), parse((ROOT / "tests" / "golden" / "parity_scene.txt").read_text())
+    assert set(got) == set(ref)
+    assert got["dt"][0] == ref["dt"][0]
+    assert abs(got["energy"][0] - ref["energy"][0]) / ref["energy"][0] < 1e-5
+    for name in ("V1", "V2", "Vp", "Ip"):
+        keys = [k for k in ref if k.startswith(name + "[")]
+        scale = max(np.hypot(*ref[k]) for k in keys)
+        for k in keys:
+            assert np.hypot(*(got[k] - ref[k])) / scale < SPEC_TOL, (k, got[k], ref[k])
+
+
 @pytest.mark.parametrize("prog", ["test_checkpoint", "test_mode2d", "test_cavity", "test_cpml", "test_sibc"])
 def test_reference_program_links_and_passes(prog):
     """The reference's own known-answer programs, linked unchanged against libcourant_b200."""
