@@ -44,15 +44,18 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-WORKLOADS = {
-    "c2": dict(desc="lossy GCPW 2-port: DS substrate (6 Debye poles), 35um Cu + Huray SIBC, 20um mask, mode ports",
-               kw=dict(hmin=10e-6, hmax=30e-6, dx=45e-6, yair=1.2e-3, zair=1.8e-3, tcu=35e-6, mask=20e-6,
-                       debye_poles=6, sigma_cu=5.8e7, huray=(0.5e-6, 2.0e11), modeports=True, steps=40000)),
-    "c1": dict(desc="lossless GCPW, lumped 50-ohm ports, er 4.3, h 254um, w 450um, gap 200um, 10 mm",
-               kw=dict(hmin=25e-6, hmax=200e-6, dx=100e-6, steps=20000)),
-}
-# Huray: sphere radius 0.5 um, 2e11 spheres per m^2 of flat area (K(inf) = 1 + 4 pi a^2 N = 1.63), standing in
-# for Rq = 1 um
+def _workloads() -> dict:
+    from courant_b200 import scenes
+    w = {k: dict(desc=v["desc"], kw=v["kw"], ref_chunk=200 if k == "c1" else 20) for k, v in scenes.CONFIGS.items()}
+    w["c3"] = dict(desc="seeded 4-layer board, 4-pole Debye cores, 20 traces, 30 vias, mode ports, "
+                        "non-uniform mesh 1500x1014x64",
+                   board=dict(seed=2026, cells=96e6, ports="mode", nf=201, fmax=20e9, steps=30000,
+                              target=(1500, 1000, 64)),
+                   ref_chunk=1, e2e_steps=4000)
+    return w
+
+
+WORKLOADS = _workloads()
 
 
 def log(*a):
@@ -137,9 +140,13 @@ def _oracle():
 
 
 def build_sim(lib, workload: str):
-    from courant_b200 import scenes
+    from courant_b200 import boards, scenes
     t = time.time()
-    s, meta = scenes.gcpw_line(lib, **WORKLOADS[workload]["kw"])
+    w = WORKLOADS[workload]
+    if "board" in w:
+        s, meta = boards.seeded_board(lib, **w["board"])
+    else:
+        s, meta = scenes.gcpw_line(lib, **w["kw"])
     meta["setup_s"] = time.time() - t
     return s, meta
 
@@ -174,7 +181,7 @@ def run_reference(args) -> None:
     from courant_b200.api import Courant
     ref = Courant(oracle.REF_LIB)
     s, meta = build_sim(ref, args.workload)
-    per = args.ref_chunk
+    per = args.ref_chunk or WORKLOADS[args.workload]["ref_chunk"]
     for _ in range(args.warmup):
         s.step(per)
     t = time.perf_counter()
@@ -315,6 +322,30 @@ class Ranks:
             self.dist.destroy_process_group()
 
 
+def spawn_replicas(n: int, cmd: list, env: dict | None = None, timeout: float | None = None) -> int:
+    """Start `cmd` as n ranks of one job on this node (RANK, LOCAL_RANK,
+    WORLD_SIZE, MASTER_ADDR 127.0.0.1 and a free MASTER_PORT set per rank),
+    wait for all of them, and return the worst exit code. Rank 0's output
+    is the job's; the others' stdout is discarded."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    procs = []
+    for r in range(n):
+        e = dict(os.environ if env is None else env, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n),
+                 LOCAL_WORLD_SIZE=str(n), MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen(cmd, env=e, stdout=None if r == 0 else subprocess.DEVNULL))
+    rc = 0
+    for p in procs:
+        try:
+            rc = max(rc, abs(p.wait(timeout=timeout)))
+        except subprocess.TimeoutExpired:
+            p.kill()
+            rc = max(rc, 124)
+    return rc
+
+
 def replica_rate(world: int, cells: int, time_steps: int, max_ms: float) -> float:
     """Whole-job cell-updates/s of `world` replicas that each advanced `cells`
     cells by `time_steps` steps, timed by the slowest rank."""
@@ -331,6 +362,8 @@ def run_b200(args) -> None:
     torch.cuda.set_device(local)
     ranks = Ranks(world)
     barrier, max_over_ranks = ranks.barrier, ranks.max
+    wl = WORKLOADS[args.workload]
+    ref_chunk = args.ref_chunk or wl["ref_chunk"]
 
     lib = Courant()
     lib.selectDevice(local)
@@ -374,7 +407,7 @@ def run_b200(args) -> None:
     e2e = None
     if not args.no_e2e:
         s.releaseDevice()
-        e2e_steps = meta["steps"] if args.e2e_steps is None else args.e2e_steps
+        e2e_steps = args.e2e_steps or min(meta["steps"], wl.get("e2e_steps", meta["steps"]))
         n_chunks = max(1, e2e_steps // chunk)
         ex = s.c.ex
         nvp, nip, nport = ex.cem_plan_nvprobe(s.h), ex.cem_plan_niprobe(s.h), ex.cem_plan_nport(s.h)
@@ -410,7 +443,8 @@ def run_b200(args) -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         oracle = _oracle()
         if oracle.REF_LIB.exists():
-            cpu = cpu_baseline(args.workload, args.ref_chunk, args.ref_samples)
+            s.destroy()   # the reference builds its own host state next (tens of GB for the largest board)
+            cpu = cpu_baseline(args.workload, ref_chunk, args.ref_samples)
 
     if rank == 0:
         launches = z["launches_per_step"] * args.steps * chunk + math.ceil(args.steps * chunk / 1024)
@@ -447,9 +481,10 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c2")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3")
     ap.add_argument("--chunk", type=int, default=500, help="FDTD time steps per benchmark step")
-    ap.add_argument("--ref-chunk", type=int, default=20, help="time steps per step of the CPU reference")
+    ap.add_argument("--ref-chunk", type=int, default=None,
+                    help="time steps per step of the CPU reference (default per workload: c1 200, c2 20, c3 1)")
     ap.add_argument("--ref-samples", type=int, default=10, help="CPU-baseline samples in the b200 arm")
     ap.add_argument("--profile-steps", type=int, default=100)
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -462,6 +497,8 @@ def main() -> None:
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
     if args.impl == "reference":
         run_reference(args)
+    elif args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(spawn_replicas(args.gpus, [sys.executable, str(Path(__file__).resolve()), *sys.argv[1:]]))
     else:
         run_b200(args)
 

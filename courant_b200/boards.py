@@ -1,163 +1,402 @@
 """Seeded synthetic printed-circuit boards over the courant.h ABI.
 
 The generator follows the layered board model of the reference's importer
-(skyhoffert/CourantEM web/src/board/kicad.ts:51-76: a stackup of dielectric
-cores with copper on their faces, traces, vias, planes) and its mesh rules
-(web/src/mesh/mesher.ts:1-12: cells refined where copper is), restated in
-Python since the reference builds boards in TypeScript. A board is four copper
-layers on three cores:
+(skyhoffert/CourantEM web/src/import/kicad.ts:51-76: a stackup of dielectric
+cores with copper on their faces, traces, vias, planes) and the reference's
+board runner (web/src/import/boardsim.ts planBoard :110-209 and buildBoardSim
+:211-331): the geometry is drawn in physical coordinates, each axis is meshed
+by the rule-based mesher (courant_b200.mesher, a restatement of
+web/src/mesh/mesher.ts), CPML cells are added outside, copper is rasterised
+edge by edge on its layer planes, vias become solid PEC cells inside their
+drill radius, and the port trace runs through feed extensions to 2D
+eigenmode (or lumped) ports. The reference builds boards in TypeScript, which
+cannot run here, so this is a restatement in Python.
+
+A board has four copper layers on three cores:
 
 - L1 (z = 0): the bottom ground, the PEC z-low face of the domain;
-- L2 (top of core 1): a ground plane over the whole grid with random
+- L2 (top of core 1): a ground plane over the whole board with random
   rectangular clearances;
 - L3 (top of core 2): stripline traces;
 - L4 (top of core 3): microstrip traces under air;
 
 cores 0.2-1.0 mm thick with eps_r uniform in 3.0-4.5, each a 4-pole
-Djordjevic-Sarkar (tan d 0.02 at 1 GHz) Debye fit sharing one set of poles;
+Djordjevic-Sarkar (tan d 0.02 at 1 GHz) Debye fit sharing one set of poles
+(the pole frequencies depend only on the band, boardsim.ts :231-233);
 traces of width 0.1-0.5 mm running along x with random 45-degree bends
-(staircased on the grid); through-vias as PEC columns; CPML on the open faces.
-Two ports sit at the ends of trace 0 (on L4, over the L2 plane): 2D
-eigenmode ports, or 50-ohm lumped ports. All randomness comes from numpy's PCG64 seeded with `seed`; the
-grid is uniform in x and y and graded in z, sized by `cells`.
+(centres, widths, jogs, clearances and vias on a 50 um routing grid),
+through-vias (L1 to L4) placed clear of the traces. Trace 0 (on L4) is the
+port trace: it runs straight through both port planes, and the board ends
+next to the port planes hold nothing but it and the L2 plane, so the port
+cross-sections are uniform. All randomness comes from numpy's PCG64 seeded
+with `seed`.
+
+Size: the minimum cell and the board's extent are searched so that the mesh
+has about the requested number of cells with the 1500 x 1000 x 64 aspect of
+the large synthetic board (z at least 28 cells: four per core, the air above
+and the CPML).
 """
 from __future__ import annotations
 
 import math
+from dataclasses import dataclass
 
 import numpy as np
 
+from . import mesher
 from .api import Courant
 
 CPML = 1
 X, Y, Z = 0, 1, 2
 
 
-def _dims(cells: float) -> tuple[int, int, int]:
-    """Cell counts with the aspect of the 1500 x 1000 x 64 reference board,
-    z at least 24 cells (layers, air, CPML)."""
-    nz = int(np.clip(round(64 * (cells / 96e6) ** (1 / 3)), 24, 64))
-    nxy = cells / nz
-    ny = max(int(round(math.sqrt(nxy / 1.5))), 24)
-    nx = max(int(round(nxy / ny)), 32)
-    return nx, ny, nz
+@dataclass
+class Layout:
+    """Everything random about a board, drawn once per seed; positions as
+    fractions of the board, widths and radii in metres."""
+    cores: np.ndarray
+    eps: np.ndarray
+    widths: np.ndarray         # per trace
+    rows: np.ndarray           # per trace, fraction of the board's y extent
+    runs: list                 # per trace: [(run fraction of the span, jog fraction of the band), ...]
+    via_uv: np.ndarray         # candidate via positions (fractions)
+    via_r: np.ndarray
+    clear: np.ndarray          # clearances: u0, v0, du, dv (fractions)
+
+
+def draw_layout(seed: int, traces: int, vias: int) -> Layout:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    cores = rng.uniform(0.2e-3, 1.0e-3, 3)
+    eps = rng.uniform(3.0, 4.5, 3)
+    widths = rng.uniform(0.1e-3, 0.5e-3, traces)
+    rows = (np.arange(traces) + 0.5) / traces
+    rows = np.roll(rows, -(traces // 2))         # trace 0 in the middle row
+    runs = []
+    for _ in range(traces):
+        segs, u = [], 0.0
+        while u < 1.0:
+            r = float(rng.uniform(0.04, 0.15))
+            j = float(rng.uniform(-0.8, 0.8))
+            segs.append((r, j))
+            u += r
+        runs.append(segs)
+    via_uv = rng.uniform(0.0, 1.0, (4 * vias, 2))
+    via_r = rng.uniform(0.1e-3, 0.2e-3, 4 * vias)
+    nclr = 6
+    clear = np.column_stack([rng.uniform(0.1, 0.85, nclr), rng.uniform(0.05, 0.9, nclr),
+                             rng.uniform(0.01, 0.05, nclr), rng.uniform(0.01, 0.05, nclr)])
+    return Layout(cores, eps, widths, rows, runs, via_uv, via_r, clear)
+
+
+@dataclass
+class Geometry:
+    """A board in physical coordinates (metres)."""
+    Lx: float
+    Ly: float
+    zl: np.ndarray              # L1..L4 heights
+    eps: np.ndarray
+    traces: list                # (layer 2 or 3, width, [(x, y), ...] polyline)
+    vias: list                  # (x, y, r)
+    clear: list                 # (x0, x1, y0, y1) holes in the L2 plane
+    end: float                  # length at each board end holding only trace 0 and the plane
+    feed: float
+
+
+GRID = 50e-6   # routing grid: trace centres, widths, jogs, clearances and vias snap to it
+
+
+def _snap(v: float) -> float:
+    return round(v / GRID) * GRID
+
+
+def realize(lay: Layout, Lx: float, Ly: float, feed: float) -> Geometry:
+    ntr = len(lay.widths)
+    band = Ly / ntr
+    end = max(0.06 * Lx, 3e-3)
+    zl = np.concatenate([[0.0], np.cumsum(lay.cores)])
+    traces = []
+    for t in range(ntr):
+        w = max(GRID * 2, _snap(float(lay.widths[t])))
+        y0 = _snap(float(lay.rows[t]) * Ly)
+        layer = 3 if t % 2 == 0 else 2
+        if t == 0:
+            traces.append((layer, w, [(-feed - 1.0, y0), (Lx + feed + 1.0, y0)]))
+            continue
+        xa, xb = end + 1e-3, Lx - end - 1e-3
+        if xb <= xa:
+            continue
+        lo, hi = y0 - 0.35 * band + w / 2, y0 + 0.35 * band - w / 2
+        pts = [(xa, y0)]
+        x, y = xa, y0
+        for r, jf in lay.runs[t]:
+            x = min(_snap(x + r * (xb - xa)), xb)
+            pts.append((x, y))
+            if x >= xb:
+                break
+            dy = _snap(float(np.clip(y + jf * 0.35 * band, lo, hi)) - y)
+            if abs(dy) > 1e-9 and x + abs(dy) < xb:
+                x, y = x + abs(dy), y + dy                  # a 45-degree jog
+                pts.append((x, y))
+        if pts[-1][0] < xb:
+            pts.append((xb, y))
+        traces.append((layer, w, pts))
+    clear = [(_snap(u0 * Lx), _snap((u0 + du) * Lx), _snap(v0 * Ly), _snap((v0 + dv) * Ly))
+             for u0, v0, du, dv in lay.clear if u0 * Lx > end and (u0 + du) * Lx < Lx - end]
+    geo = Geometry(Lx, Ly, zl, lay.eps, traces, [], clear, end, feed)
+    return geo
+
+
+def place_vias(geo: Geometry, lay: Layout, count: int) -> None:
+    """The first `count` candidate positions that keep a via clear of every
+    trace (0.2 mm) and of the board ends."""
+    out = []
+    for (u, v), r in zip(lay.via_uv, lay.via_r):
+        if len(out) >= count:
+            break
+        x, y = _snap(geo.end + u * (geo.Lx - 2 * geo.end)), _snap(0.03 * geo.Ly + v * 0.94 * geo.Ly)
+        ok = all(_dist_polyline(x, y, pts) > w / 2 + r + 0.2e-3 for _, w, pts in geo.traces)
+        ok = ok and all(math.hypot(x - a, y - b) > r + q + 0.3e-3 for a, b, q in out)
+        if ok:
+            out.append((float(x), float(y), float(r)))
+    geo.vias = out
+
+
+def _dist_polyline(x, y, pts) -> float:
+    best = math.inf
+    for (x0, y0), (x1, y1) in zip(pts[:-1], pts[1:]):
+        dx, dy = x1 - x0, y1 - y0
+        L2 = dx * dx + dy * dy
+        t = 0.0 if L2 == 0 else min(1.0, max(0.0, ((x - x0) * dx + (y - y0) * dy) / L2))
+        best = min(best, math.hypot(x - x0 - t * dx, y - y0 - t * dy))
+    return best
+
+
+# ------------------------------------------------------------------ meshing
+
+def axis_features(geo: Geometry, fmax: float, hmin: float):
+    """The mesher inputs of the three axes (boardsim.ts planBoard :154-188)."""
+    er_max = float(max(geo.eps))
+    h_air = min(mesher.lambda_over_20(fmax, 1.0), 200e-6)
+    h_diel = mesher.lambda_over_20(fmax, er_max)
+    side = 1e-3
+    # y: trace edges of the x-directed runs, clearance edges, vias
+    yedges = set()
+    xedges = set()
+    for _, w, pts in geo.traces:
+        for (x0, y0), (x1, y1) in zip(pts[:-1], pts[1:]):
+            if abs(y1 - y0) < 1e-12:
+                yedges.add((round(y0 - w / 2, 9), "hi"))
+                yedges.add((round(y0 + w / 2, 9), "lo"))
+        xs = pts[0][0], pts[-1][0]
+        if 0 < xs[0] < geo.Lx:
+            xedges.add((round(xs[0], 9), "hi"))
+        if 0 < xs[1] < geo.Lx:
+            xedges.add((round(xs[1], 9), "lo"))
+    for x0, x1, y0, y1 in geo.clear:
+        yedges |= {(round(y0, 9), "lo"), (round(y1, 9), "hi")}
+        xedges |= {(round(x0, 9), "lo"), (round(x1, 9), "hi")}
+    via_r = min((r for _, _, r in geo.vias), default=0.0)
+    h_via = max(hmin, via_r / 2) if via_r else math.inf
+    fy = mesher.AxisFeatures(lo=-side, hi=geo.Ly + side, sheet_edges=sorted(yedges), planes=[0.0, geo.Ly],
+                             refine=[e for e, _ in yedges] + [y for _, y, _ in geo.vias],
+                             max_cell=[(0.0, geo.Ly, h_diel)] + [(y - r, y + r, h_via) for _, y, r in geo.vias])
+    X0, X1 = -geo.feed, geo.Lx + geo.feed
+    fx = mesher.AxisFeatures(lo=X0, hi=X1, sheet_edges=sorted(xedges), planes=[0.0, geo.Lx],
+                             refine=[e for e, _ in xedges] + [x for x, _, _ in geo.vias],
+                             max_cell=[(X0, X1, min(h_diel, 4 * hmin))] + [(x - r, x + r, h_via) for x, _, r in geo.vias])
+    ztop = float(geo.zl[-1])
+    fz = mesher.AxisFeatures(lo=0.0, hi=ztop + 1.5e-3, planes=[float(v) for v in geo.zl],
+                             spans=[(float(geo.zl[q]), float(geo.zl[q + 1]), 4) for q in range(3)],
+                             max_cell=[(float(geo.zl[q]), float(geo.zl[q + 1]), h_diel) for q in range(3)],
+                             refine=[float(v) for v in geo.zl])
+    return fx, fy, fz, h_air
+
+
+def _mesh_z(geo, fmax, hmin, npml):
+    _, _, fz, h_air = axis_features(geo, fmax, hmin)
+    return mesher.with_pml(mesher.mesh_axis(fz, hmin, h_air), npml, h_air / 2, lo=False, hi=True)
+
+
+def _search(f, lo, hi, target, increasing, iters=18):
+    """Bisection of a monotone integer-valued f for the argument giving `target`."""
+    best = None
+    for _ in range(iters):
+        mid = math.sqrt(lo * hi)
+        v = f(mid)
+        if best is None or abs(v - target) < abs(best[1] - target):
+            best = (mid, v)
+        if (v < target) == increasing:
+            lo = mid
+        else:
+            hi = mid
+    return best[0]
+
+
+def plan_mesh(lay: Layout, cells: float, fmax: float, npml: int, vias: int, feed: float,
+              target: tuple | None = None):
+    """Minimum cell, board extent and node lines for about `cells` cells:
+    hmin sets nz, then Ly sets ny and Lx sets nx (aspect 1.5 : 1)."""
+    if target is None:
+        nz_t = int(np.clip(round(64 * (cells / 96e6) ** (1 / 3)), 28, 64))
+        ny_t = math.sqrt(cells / nz_t / 1.5)
+        target = (1.5 * ny_t, ny_t, nz_t)
+    nx_t, ny_t, nz_t = target
+    probe = realize(lay, 0.1, 0.07, feed)
+    h_air = min(mesher.lambda_over_20(fmax, 1.0), 200e-6)
+    hmin = _search(lambda h: len(_mesh_z(probe, fmax, h, npml)) - 1, 5e-6, h_air, nz_t, increasing=False)
+
+    def ny_of(Ly):
+        geo = realize(lay, 1.5 * Ly, Ly, feed)
+        place_vias(geo, lay, vias)
+        _, fy, _, h_air = axis_features(geo, fmax, hmin)
+        return len(mesher.mesh_axis(fy, hmin, h_air)) - 1 + 2 * npml
+
+    Ly = _search(ny_of, 2e-3, 2.0, ny_t, increasing=True, iters=16)
+
+    def nx_of(Lx):
+        geo = realize(lay, Lx, Ly, feed)
+        place_vias(geo, lay, vias)
+        fx, _, _, h_air = axis_features(geo, fmax, hmin)
+        return len(mesher.mesh_axis(fx, hmin, h_air)) - 1 + 2 * npml
+
+    Lx = _search(nx_of, 3e-3, 3.0, nx_t, increasing=True, iters=16)
+    geo = realize(lay, Lx, Ly, feed)
+    place_vias(geo, lay, vias)
+    fx, fy, fz, h_air = axis_features(geo, fmax, hmin)
+    hp = h_air / 2
+    x = mesher.with_pml(mesher.mesh_axis(fx, hmin, h_air), npml, hp)
+    y = mesher.with_pml(mesher.mesh_axis(fy, hmin, h_air), npml, hp)
+    z = mesher.with_pml(mesher.mesh_axis(fz, hmin, h_air), npml, hp, lo=False, hi=True)
+    return geo, hmin, x, y, z
+
+
+# ------------------------------------------------------------------ rasterising
+
+def _capsule_marks(mask, xs, ys, x0, y0, x1, y1, r):
+    """Mark the points of the grid xs (rows) x ys (columns) within r of segment (x0, y0)-(x1, y1)."""
+    i0, i1 = np.searchsorted(xs, min(x0, x1) - r, "left"), np.searchsorted(xs, max(x0, x1) + r, "right")
+    j0, j1 = np.searchsorted(ys, min(y0, y1) - r, "left"), np.searchsorted(ys, max(y0, y1) + r, "right")
+    if i1 <= i0 or j1 <= j0:
+        return
+    X, Yv = np.meshgrid(xs[i0:i1], ys[j0:j1], indexing="ij")
+    dx, dy = x1 - x0, y1 - y0
+    L2 = dx * dx + dy * dy
+    t = np.zeros_like(X) if L2 == 0 else np.clip(((X - x0) * dx + (Yv - y0) * dy) / L2, 0.0, 1.0)
+    d2 = (X - x0 - t * dx) ** 2 + (Yv - y0 - t * dy) ** 2
+    mask[i0:i1, j0:j1] |= d2 <= r * r * (1 + 1e-12)
+
+
+def _trace_masks(x, y, traces):
+    """Edge masks of a z-normal plane (cem_pec_edges_plane layout: u = x edges
+    nx x (ny+1), v = y edges (nx+1) x ny): an edge is copper when both its
+    nodes and its midpoint are (boardsim.ts :253-265)."""
+    xm, ym = 0.5 * (x[1:] + x[:-1]), 0.5 * (y[1:] + y[:-1])
+    node = np.zeros((len(x), len(y)), bool)
+    midx = np.zeros((len(xm), len(y)), bool)
+    midy = np.zeros((len(x), len(ym)), bool)
+    for w, pts in traces:
+        for (x0, y0), (x1, y1) in zip(pts[:-1], pts[1:]):
+            for m, xs, ys in ((node, x, y), (midx, xm, y), (midy, x, ym)):
+                _capsule_marks(m, xs, ys, x0, y0, x1, y1, w / 2)
+    mu = node[:-1, :] & node[1:, :] & midx
+    mv = node[:, :-1] & node[:, 1:] & midy
+    return mu, mv
+
+
+def _plane_masks(x, y, holes):
+    """Edge masks of a full plane with rectangular holes (open rectangles)."""
+    def inside(X, Yv):
+        m = np.zeros(X.shape, bool)
+        for x0, x1, y0, y1 in holes:
+            m |= (X > x0) & (X < x1) & (Yv > y0) & (Yv < y1)
+        return ~m
+    xm, ym = 0.5 * (x[1:] + x[:-1]), 0.5 * (y[1:] + y[:-1])
+    node = inside(*np.meshgrid(x, y, indexing="ij"))
+    mu = node[:-1, :] & node[1:, :] & inside(*np.meshgrid(xm, y, indexing="ij"))
+    mv = node[:, :-1] & node[:, 1:] & inside(*np.meshgrid(x, ym, indexing="ij"))
+    return mu, mv
+
+
+def _nearest(a, v):
+    return int(np.argmin(np.abs(np.asarray(a) - v)))
+
+
+def hammerstad_neff(w: float, h: float, er: float) -> float:
+    """Quasi-static effective index of a microstrip (Hammerstad), the shift of the port mode solve."""
+    u = w / h
+    e = (er + 1) / 2 + (er - 1) / 2 * (1 + 12 / u) ** -0.5
+    if u < 1:
+        e += (er - 1) / 2 * 0.04 * (1 - u) ** 2
+    return math.sqrt(e)
 
 
 def seeded_board(c: Courant, seed: int, cells: float = 2e6, *, ports: str = "mode", nf: int = 32,
                  fmax: float = 20e9, steps: int | None = None, traces: int = 20, vias: int = 30,
-                 npml: int = 8, cfl: float = 0.99, excite: int = 1):
+                 npml: int = 8, cfl: float = 0.99, excite: int = 1, target: tuple | None = None):
     """Finalized board simulation and its metadata (dims, cells, ports,
-    frequencies, step count). `cells` sets the grid size; `traces` and `vias`
-    scale down for small grids so features stay at least two cells wide;
-    `excite` (1 or 2) picks the driven port, the two excitations of a full
-    2-port measurement."""
-    rng = np.random.Generator(np.random.PCG64(seed))
-    nx, ny, nz = _dims(cells)
-    cores = rng.uniform(0.2e-3, 1.0e-3, 3)
-    eps = rng.uniform(3.0, 4.5, 3)
-    zl = np.concatenate([[0.0], np.cumsum(cores)])          # L1..L4 heights
-    air = 1.5e-3
-    # z: cores split evenly over most cells, air above, CPML cells at the top
-    ncore = max(4, (nz - npml - 6) // 3)
-    zs = [0.0]
-    for q in range(3):
-        zs += list(zl[q] + cores[q] * np.arange(1, ncore + 1) / ncore)
-    nair = nz - 3 * ncore
-    dz_air = air / max(nair - npml, 1)
-    zs += list(zl[3] + dz_air * np.arange(1, nair + 1))
-    z = np.array(zs)
-    kl = [0] + [ncore * (q + 1) for q in range(3)]           # k index of L1..L4
-    # x, y uniform 0.1 mm cells: the board grows with the grid
-    dx = 0.1e-3
-    x = dx * np.arange(nx + 1)
-    y = dx * np.arange(ny + 1)
+    frequencies, step count, mesh report). `cells` sets the grid size (or
+    `target` = (nx, ny, nz) directly); `traces` and `vias` scale down for
+    small boards so features keep a few cells between them; `excite` (1 or
+    2) picks the driven port, the two excitations of a full 2-port
+    measurement."""
+    ntr = max(3, min(traces, int(round((cells / 2e4) ** 0.5))))
+    nvia = max(2, min(vias, int(cells / 1e5)))
+    lay = draw_layout(seed, ntr, 4 * nvia)
+    feed = 4e-3 if ports == "mode" else 0.0
+    geo, hmin, x, y, z = plan_mesh(lay, cells, fmax, npml, nvia, feed, target)
+    nx, ny, nz = len(x) - 1, len(y) - 1, len(z) - 1
     s = c.createSim(x, y, z)
     for f in (0, 1, 2, 3, 5):
         s.setBoundary(f, CPML, npml)
-    fmin = 1e8
-    fits = [c.fitDjordjevicSarkar(float(e), 0.02, 1e9, fmin, fmax, 4) for e in eps]
+    fits = [c.fitDjordjevicSarkar(float(e), 0.02, 1e9, 1e8, fmax, 4) for e in geo.eps]
     s.setDebyePoles(fits[0].fp)
     big = 1.0
+    zl = geo.zl
     for q in range(3):
-        s.materialBoxDebye(-big, big, -big, big, zl[q], zl[q + 1], fits[q])
-    # keep copper away from the CPML, and the x ends (the port cross-sections) clear of all but trace 0
-    i_lo, i_hi = npml + 12, max(nx - npml - 12, npml + 20)
-    j_lo, j_hi = npml + 2, ny - npml - 2
-    xs, ys = x, y
-    # L2 ground plane with clearances
-    nclr = max(1, min(6, (j_hi - j_lo) // 12))
-    clear = []
-    for _ in range(nclr):
-        ci = int(rng.integers(i_lo + 4, max(i_lo + 5, i_hi - 8)))
-        cj = int(rng.integers(j_lo + 2, max(j_lo + 3, j_hi - 6)))
-        clear.append((ci, ci + int(rng.integers(2, 6)), cj, cj + int(rng.integers(2, 5))))
-    # the plane spans the whole grid (uniform cross-sections at the ports), split in y bands at the
-    # clearance edges, each band covered by the x intervals outside its clearances
-    yb = sorted({0, ny} | {a for cl in clear for a in (cl[2], cl[3])})
-    for b0, b1 in zip(yb[:-1], yb[1:]):
-        if b1 <= b0:
-            continue
-        cuts = sorted((cl[0], cl[1]) for cl in clear if cl[2] <= b0 and cl[3] >= b1)
-        a = 0
-        for c0, c1 in cuts:
-            if c0 > a:
-                s.pecSheet(Z, zl[1], xs[a], xs[c0], ys[b0], ys[b1])
-            a = max(a, c1)
-        if a < nx:
-            s.pecSheet(Z, zl[1], xs[a], xs[nx], ys[b0], ys[b1])
-    # traces: x-directed runs with 45-degree staircased jogs; trace 0 on L4 is the port trace
-    ntr = max(1, min(traces, (j_hi - j_lo) // 6))
-    rows = np.linspace(j_lo + 2, j_hi - 4, ntr).astype(int)
-    t0_j, t0_w = None, None
-    for t in range(ntr):
-        layer = 3 if t % 2 == 0 else 2
-        zt = zl[layer]
-        w = int(max(1, round(rng.uniform(0.1e-3, 0.5e-3) / dx)))
-        j = int(rows[t])
-        if t == 0:
-            t0_j, t0_w = j, w
-            s.pecSheet(Z, zt, xs[0] - 1.0, xs[nx] + 1.0, ys[j], ys[j + w])   # straight, through the ports
-            continue
-        i = i_lo
-        while i < i_hi:
-            run = int(rng.integers(6, 20))
-            i1 = min(i + run, i_hi)
-            s.pecSheet(Z, zt, xs[i], xs[i1], ys[j], ys[j + w])
-            i = i1
-            if i >= i_hi:
-                break
-            jog = int(rng.integers(-3, 4))
-            step = 1 if jog > 0 else -1
-            for _ in range(abs(jog)):                        # one cell right and one up per step
-                j2 = j + step
-                if j2 < j_lo or j2 + w > j_hi:
-                    break
-                i2 = min(i + 1, i_hi)
-                s.pecSheet(Z, zt, xs[i], xs[i2], ys[min(j, j2)], ys[max(j, j2) + w])
-                i, j = i2, j2
-    # through-vias (PEC columns of one or two cells), L1 to L4, away from trace 0
-    nv = max(1, min(vias, (i_hi - i_lo) * (j_hi - j_lo) // 200))
-    for _ in range(nv):
-        vi = int(rng.integers(i_lo, i_hi - 2))
-        vj = int(rng.integers(j_lo, j_hi - 2))
-        if t0_j - 2 <= vj <= t0_j + t0_w + 2:
-            continue
-        e = int(rng.integers(1, 3))
-        s.pecBox(xs[vi], xs[vi + e], ys[vj], ys[vj + e], 0.0, zl[3])
+        s.materialBoxDebye(-big, big, -big, big, float(zl[q]), float(zl[q + 1]), fits[q])
+    kl = [_nearest(z, v) for v in zl]
+    # L2 plane with clearances, then the trace layers (the bottom copper is the PEC floor)
+    mu, mv = _plane_masks(x, y, geo.clear)
+    s.pecEdgesPlane(Z, kl[1], mu, mv)
+    for layer in (2, 3):
+        sel = [(w, pts) for ly, w, pts in geo.traces if ly == layer]
+        if sel:
+            mu, mv = _trace_masks(x, y, sel)
+            s.pecEdgesPlane(Z, kl[layer], mu, mv)
+    # via barrels: solid PEC cells inside the drill radius, L1 to L4 (boardsim.ts :281-297)
+    for vx, vy, r in geo.vias:
+        i0, i1 = max(0, _nearest(x, vx - r) - 1), min(nx - 1, _nearest(x, vx + r) + 1)
+        j0, j1 = max(0, _nearest(y, vy - r) - 1), min(ny - 1, _nearest(y, vy + r) + 1)
+        cx = 0.5 * (x[i0:i1 + 1] + x[i0 + 1:i1 + 2])
+        cy = 0.5 * (y[j0:j1 + 1] + y[j0 + 1:j1 + 2])
+        inside = (cx[:, None] - vx) ** 2 + (cy[None, :] - vy) ** 2 <= r * r
+        if inside.any() and kl[3] > 0:
+            s.pecCells(i0, j0, 0, np.repeat(inside[:, :, None], kl[3], axis=2).astype(np.uint8))
     tau = math.sqrt(6.9) / (math.pi * 1.25 * fmax)
     freqs = np.linspace(fmax / nf, fmax, nf)
-    meta = {"seed": seed, "dims": (nx, ny, nz), "cells": nx * ny * nz, "tau": tau, "freqs": freqs, "excite": excite}
-    ktop = kl[3]
+    _, w0, pts0 = geo.traces[0]
+    yc = pts0[0][1]
+    kh = kl[3]
+    meta = {"seed": seed, "dims": (nx, ny, nz), "cells": nx * ny * nz, "tau": tau, "freqs": freqs, "excite": excite,
+            "hmin": hmin, "board_mm": (geo.Lx * 1e3, geo.Ly * 1e3), "traces": len(geo.traces), "vias": len(geo.vias),
+            "mesh": {a: mesher.report(v) for a, v in (("x", x), ("y", y), ("z", z))}}
     if ports == "mode":
-        d = dict(j0=0, j1=ny, k0=0, k1=nz, vj=t0_j, vk0=kl[1], vk1=ktop, vsign=-1, ja=max(t0_j - 1, 0),
-                 jb=t0_j + t0_w, ka=ktop - 1, kb=ktop, f0=0.5 * fmax, neff0=math.sqrt((float(eps[2]) + 1) / 2))
-        p1 = s.addModePort(dict(d, dir=1, iSrc=npml + 2, iMon=npml + 6, xRef=xs[npml + 8]))
-        p2 = s.addModePort(dict(d, dir=-1, iSrc=nx - npml - 2, iMon=nx - npml - 7, xRef=xs[nx - npml - 8]))
+        jl, jr = _nearest(y, yc - w0 / 2), _nearest(y, yc + w0 / 2)
+        ja = max(0, (jl if y[jl] <= yc - w0 / 2 else jl - 1) - 1)
+        jb = min(ny - 1, jr if y[jr] >= yc + w0 / 2 else jr + 1)
+        er_eff = float(np.average(geo.eps[1:], weights=np.diff(zl)[1:]))
+        d = dict(j0=0, j1=ny, k0=0, k1=nz, vj=_nearest(y, yc), vk0=kl[1], vk1=kh, vsign=-1, ja=ja, jb=jb,
+                 ka=kh - 1, kb=kh, f0=0.5 * fmax, neff0=hammerstad_neff(w0, float(zl[3] - zl[1]), er_eff))
+        mon = 2.5e-3
+        i1 = npml + 2
+        i2 = nx - npml - 2
+        p1 = s.addModePort(dict(d, dir=1, iSrc=i1, iMon=_nearest(x, x[i1] + mon), xRef=0.0))
+        p2 = s.addModePort(dict(d, dir=-1, iSrc=i2, iMon=_nearest(x, x[i2] - mon) - 1, xRef=geo.Lx))
         s.setModeExcitation(p1 if excite == 1 else p2, 4.5 * tau, tau)
         meta["modeports"] = [p1, p2]
     else:
-        p1 = s.addLumpedPort(Z, npml + 4, t0_j, kl[1], ktop, -1, 50.0)     # L2 ground to the L4 trace
-        p2 = s.addLumpedPort(Z, nx - npml - 4, t0_j, kl[1], ktop, -1, 50.0)
+        p1 = s.addLumpedPort(Z, npml + 4, _nearest(y, yc), kl[1], kh, -1, 50.0)     # L2 ground to the L4 trace
+        p2 = s.addLumpedPort(Z, nx - npml - 4, _nearest(y, yc), kl[1], kh, -1, 50.0)
         s.setGaussian(p1 if excite == 1 else p2, 1.0, 4.5 * tau, tau)
         meta["ports"] = [p1, p2]
     s.setFrequencies(freqs)

@@ -2920,30 +2920,36 @@ int engine_energy(const cem_sim *cs, double *out) {
 constexpr long long kNoAllocPartials = 65536;   // 512 KiB of block partials
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocPartials + 1];   // + the result
 
-constexpr int kMaxScratchDevices = 64;
-std::mutex g_scratch_mu;
-double *g_scratch_addr[kMaxScratchDevices] = {};
-
-// Address of g_noalloc_scratch on `device`, which must be current. Looked up
-// once per device; later calls only read the cached pointer.
-double *noalloc_scratch(int device) {
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (device < 0 || device >= kMaxScratchDevices) {
-        set_error("cemx_energy_noalloc: device ordinal beyond the 64 this library tracks");
+// Address of g_noalloc_scratch on the current device. In host code the
+// array's name is only a host-side stand-in, so the device address is looked
+// up on every call (cheap once the module is loaded, allocates nothing, and
+// stays right after a cudaDeviceReset tears the module down and reloads it).
+double *noalloc_scratch() {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "cemx_energy_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        set_error(msg);
         return nullptr;
     }
-    if (!g_scratch_addr[device]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) {
-            char msg[256];
-            std::snprintf(msg, sizeof msg, "cemx_energy_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-            set_error(msg);
-            return nullptr;
-        }
-        g_scratch_addr[device] = static_cast<double *>(p);
-    }
-    return g_scratch_addr[device];
+    return static_cast<double *>(p);
+}
+
+bool energy_noalloc_on(cem_sim *s, Device &D, double *out) {
+    const int gx = (D.g.plane + kEnergyBlock - 1) / kEnergyBlock;
+    const long long nblk = (long long)gx * (s->n[0] + 1);
+    double *scratch = noalloc_scratch();
+    if (!scratch) return false;
+    EnergyArgs ea = D.ea[D.cur];
+    ea.partial = scratch;
+    for (int c0 = 0; c0 <= s->n[0]; c0 += kMaxGridY)
+        k_energy<<<dim3(gx, std::min(kMaxGridY, s->n[0] + 1 - c0)), kEnergyBlock, 0, D.stream>>>(ea, c0);
+    k_sum<<<1, 1024, 0, D.stream>>>(scratch, nblk, scratch + kNoAllocPartials);
+    CB2_CHECK(s, cudaGetLastError());
+    CB2_CHECK(s, cudaMemcpyAsync(out, scratch + kNoAllocPartials, sizeof(double), cudaMemcpyDeviceToHost, D.stream));
+    CB2_CHECK(s, cudaStreamSynchronize(D.stream));
+    return true;
 }
 
 bool energy_noalloc(cem_sim *s, double *out) {
@@ -2967,18 +2973,14 @@ bool energy_noalloc(cem_sim *s, double *out) {
         set_error(msg);
         return false;
     }
+    // run on the simulation's device and give the caller back its current device
+    int prev = -1;
+    CB2_CHECK(s, cudaGetDevice(&prev));
     CB2_CHECK(s, cudaSetDevice(D.device));
-    double *scratch = noalloc_scratch(D.device);
-    if (!scratch) return false;
-    EnergyArgs ea = D.ea[D.cur];
-    ea.partial = scratch;
-    for (int c0 = 0; c0 <= s->n[0]; c0 += kMaxGridY)
-        k_energy<<<dim3(gx, std::min(kMaxGridY, s->n[0] + 1 - c0)), kEnergyBlock, 0, D.stream>>>(ea, c0);
-    k_sum<<<1, 1024, 0, D.stream>>>(scratch, nblk, scratch + kNoAllocPartials);
-    CB2_CHECK(s, cudaGetLastError());
-    CB2_CHECK(s, cudaMemcpyAsync(out, scratch + kNoAllocPartials, sizeof(double), cudaMemcpyDeviceToHost, D.stream));
-    CB2_CHECK(s, cudaStreamSynchronize(D.stream));
-    return true;
+    const bool ok = energy_noalloc_on(s, D, out);
+    const cudaError_t e = cudaSetDevice(prev);
+    if (ok && e != cudaSuccess) return fail(s, "cudaSetDevice(previous device)", e);
+    return ok;
 }
 
 }  // namespace cb2
@@ -3060,6 +3062,7 @@ struct cemx_batch {
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t tev0 = nullptr, tev1 = nullptr;   // timing of the tuning chunks
     cudaStream_t side = nullptr;             // general blocks beside the fast ones; SIBC beside the probes
     bool sibc_beside = false;                // no member's probes read a SIBC edge
     cudaEvent_t fork = nullptr, join = nullptr;
@@ -3373,6 +3376,7 @@ cemx_batch *cemx_batch_create(int device) {
     b->device = device;
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaEventCreate(&b->tev0) != cudaSuccess || cudaEventCreate(&b->tev1) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess) {
@@ -3391,6 +3395,8 @@ void cemx_batch_destroy(cemx_batch *b) {
     b->work_e.clear();
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->tev0) cudaEventDestroy(b->tev0);
+    if (b->tev1) cudaEventDestroy(b->tev1);
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->join) cudaEventDestroy(b->join);
     if (b->side) cudaStreamDestroy(b->side);
@@ -3485,21 +3491,19 @@ int cemx_batch_run(cemx_batch *b, long max_steps) {
                             for (int m : b->active) {
                                 Device &D = *b->members[m].s->dev;
                                 if (D.ring_count + ch > kRing) {
-                                    cudaStreamSynchronize(b->stream);
+                                    const cudaError_t e = cudaStreamSynchronize(b->stream);
+                                    if (e != cudaSuccess) { batch_fail("cudaStreamSynchronize", e); return -1; }
                                     if (!flush_dft(b->members[m].s) || cudaStreamSynchronize(D.stream) != cudaSuccess)
                                         return -1;
                                 }
                             }
-                            cudaEvent_t t0, t1;
-                            cudaEventCreate(&t0);
-                            cudaEventCreate(&t1);
-                            cudaEventRecord(t0, b->stream);
+                            cudaError_t e = cudaEventRecord(b->tev0, b->stream);
+                            if (e != cudaSuccess) { batch_fail("cudaEventRecord", e); return -1; }
                             if (!batch_launch(b, ch)) return -1;
-                            cudaEventRecord(t1, b->stream);
-                            cudaEventSynchronize(t1);
-                            cudaEventElapsedTime(&ms, t0, t1);
-                            cudaEventDestroy(t0);
-                            cudaEventDestroy(t1);
+                            if ((e = cudaEventRecord(b->tev1, b->stream)) != cudaSuccess ||
+                                (e = cudaEventSynchronize(b->tev1)) != cudaSuccess ||
+                                (e = cudaEventElapsedTime(&ms, b->tev0, b->tev1)) != cudaSuccess)
+                            { batch_fail("tuning timer", e); return -1; }
                             for (int m : b->active) {
                                 b->members[m].s->step += ch;
                                 b->members[m].s->dev->ring_count += ch;

@@ -78,6 +78,7 @@ class Server:
         self.lib = lib
         self.budget = int(budget_bytes)
         self.chunk = chunk
+        self.tune = tune
         self.batch = lib.createBatch(device)
         self.batch.tune(tune)
         self.incoming: queue.Queue = queue.Queue()
@@ -168,19 +169,59 @@ class Server:
 
     def _gpu_loop(self):
         while not self.stop:
-            self._admit()
-            if not self.members:
-                self.wake.wait(0.01)
-                self.wake.clear()
-                continue
-            self.batch.run(self.chunk)
-            self.gpu_ms += self.batch.stats()["ms"]
-            for h, item in list(self.members.items()):
-                sim = item[1]
-                if self.batch.left(sim) == 0:
-                    self.batch.remove(sim)
-                    del self.members[h]
-                    self.finish_pool.submit(self._finish, item)
+            try:
+                self._gpu_iteration()
+            except Exception as e:   # a failed batched launch or device error: fail its requests, start afresh
+                self._fail_all(f"batch failed: {e}")
+
+    def _gpu_iteration(self):
+        self._admit()
+        if not self.members:
+            self.wake.wait(0.01)
+            self.wake.clear()
+            return
+        self.batch.run(self.chunk)
+        self.gpu_ms += self.batch.stats()["ms"]
+        for h, item in list(self.members.items()):
+            sim = item[1]
+            if self.batch.left(sim) == 0:
+                self.batch.remove(sim)
+                del self.members[h]
+                self.finish_pool.submit(self._finish, item)
+
+    def _fail_all(self, why: str):
+        """Every request on the GPU side (batch members and loaded, not yet
+        added) gets the error; their simulations are freed and their bytes
+        returned to the budget, and the batch is replaced by a new one, so
+        requests still building or queued are served afterwards."""
+        with self.lock:
+            items = list(self.members.values()) + self.loaded
+            self.members, self.loaded = {}, []
+        try:
+            self.batch.destroy()
+        except Exception:
+            pass
+        for r, sim, meta, nbytes in items:
+            r.error = why
+            try:
+                sim.destroy()
+            except Exception:
+                pass
+            with self.lock:
+                self.used -= nbytes
+            r.done = time.perf_counter()
+            r.event.set()
+        try:
+            self.batch = self.lib.createBatch(self.device)
+            self.batch.tune(self.tune)
+        except Exception as e:   # no batch can be made: stop serving, fail what is left
+            self.stop = True
+            with self.lock:
+                rest, self.built = self.built, []
+            for r, sim, meta, nbytes in rest:
+                r.error = f"server stopped: {e}"
+                r.done = time.perf_counter()
+                r.event.set()
 
     def close(self):
         self.stop = True
@@ -223,7 +264,11 @@ def serve_all(server: Server, requests: list[Request], arrivals: list[float]) ->
             time.sleep(at - now)
         out.append(server.submit(r.build, r.steps, r.tag))
     for r in out:
-        r.event.wait()
+        while not r.event.wait(0.5):
+            if not server.thread.is_alive() and not r.event.is_set():   # the GPU thread has stopped
+                r.error = r.error or "server stopped"
+                r.done = time.perf_counter()
+                r.event.set()
     return out
 
 

@@ -67,10 +67,12 @@ CEM_API int cemx_use_fused(cem_sim *s, int on);
  * same kernels, so it returns the same value bit for bit, but keeps its
  * block partials in one static device array per process and device (512 KiB,
  * 65536 partials, about 16.7 million grid points); nothing in it has to
- * start at zero. The first call on a device looks up that array's address
- * (cudaGetSymbolAddress) and should come before any stream capture on that
- * device. Calls for simulations on the same device share the array and must
- * not overlap in time (serialise them across threads).
+ * start at zero. Every call looks up that array's address on the
+ * simulation's device (cudaGetSymbolAddress; the first lookup on a device
+ * loads the module there, so make a first call before any stream capture on
+ * that device) and leaves the caller's current device as it found it. Calls
+ * for simulations on the same device share the array and race if they
+ * overlap on the GPU (serialise them across threads).
  * Fails (-1, cem_last_error() set) when s has no device state yet (step it
  * first), when field pointers handed out by cem_field are live, or when the
  * grid needs more than 65536 partials (use cem_energy). Returns 0 or -1. */

@@ -57,3 +57,17 @@ def test_replica_rate_is_whole_job():
     import bench
     assert bench.replica_rate(1, 1000, 500, 1.0) == pytest.approx(5e8)
     assert bench.replica_rate(4, 1000, 500, 2.0) == pytest.approx(1e9)
+
+
+def test_spawned_replicas_report_the_job(tmp_path):
+    """bench.spawn_replicas, the path `bench.py --gpus N` takes outside
+    torchrun: N ranks with RANK/LOCAL_RANK/WORLD_SIZE/MASTER_* set, here two
+    gloo ranks on the CPU; rank 0 reports n_gpus 2 and the slowest rank."""
+    import json
+    import bench
+    out = tmp_path / "line.json"
+    rc = bench.spawn_replicas(2, [sys.executable, str(ROOT / "tests" / "replica_rank.py"), str(out)], timeout=180)
+    assert rc == 0
+    line = json.loads(out.read_text())
+    assert line["n_gpus"] == 2 and line["max_ms"] == 20.0
+    assert line["value"] == pytest.approx(2 * 24 * 18 * 14 * 1000 / 0.020)

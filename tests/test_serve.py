@@ -54,3 +54,91 @@ def test_request_above_budget_is_refused(lib):
         assert r.error and "budget" in r.error
     finally:
         srv.close()
+
+
+class _FakeSim:
+    """Host stand-in of a finalized simulation (what footprint and the server read)."""
+    _next = 0
+
+    def __init__(self):
+        _FakeSim._next += 1
+        self.h, self.nx, self.ny, self.nz = _FakeSim._next, 8, 8, 8
+        self.destroyed = False
+
+    def sizes(self):
+        return {"psiE": 0, "psiH": 0, "npole": 0, "ndisp": 0, "sibc_terms": 0, "nsibc": 0}
+
+    def prepareDevice(self, device=-1):
+        pass
+
+    def destroy(self):
+        self.destroyed = True
+
+
+class _FakeBatch:
+    """The first batch fails on its first run (as a failed batched launch
+    does); later batches finish every member in one run."""
+    made = 0
+
+    def __init__(self):
+        _FakeBatch.made += 1
+        self.fail = _FakeBatch.made == 1
+        self.left_ = {}
+
+    def tune(self, on=True):
+        return True
+
+    def add(self, sim, steps):
+        self.left_[sim.h] = steps
+
+    def run(self, n):
+        if self.fail:
+            from courant_b200.api import CourantError
+            raise CourantError("batch: a batched launch failed")
+        for h in self.left_:
+            self.left_[h] = 0
+        return 0
+
+    def stats(self):
+        return {"ms": 0.0}
+
+    def left(self, sim):
+        return self.left_[sim.h]
+
+    def remove(self, sim):
+        del self.left_[sim.h]
+
+    def destroy(self):
+        pass
+
+
+class _FakeLib:
+    def createBatch(self, device=-1):
+        return _FakeBatch()
+
+
+def test_failed_batch_fails_its_requests_and_serving_goes_on(monkeypatch):
+    """A batched launch that raises fails the requests on the GPU with the
+    error (their events set, bytes released); the server replaces the batch
+    and serves the next request. Host-only: fake simulations and batches."""
+    sims = []
+
+    def build(c):
+        s = _FakeSim()
+        sims.append(s)
+        return s, {"cells": 512}
+
+    monkeypatch.setattr(serve, "results", lambda sim, meta: {"S11": np.zeros(1), "S21": np.zeros(1)})
+    _FakeBatch.made = 0
+    srv = serve.Server(_FakeLib(), budget_bytes=1e9, chunk=16, builders=1, finishers=1)
+    try:
+        first = srv.submit(build, 10)
+        assert first.event.wait(10)
+        assert first.error and "batched launch failed" in first.error
+        assert sims[0].destroyed
+        second = srv.submit(build, 10)
+        assert second.event.wait(10)
+        assert second.error is None and second.result is not None
+        assert srv.thread.is_alive() and srv.used == 0
+    finally:
+        srv.close()

@@ -60,3 +60,24 @@ def test_noalloc_rejects_grids_beyond_the_scratch(lib):
         assert s.steps == 2
     finally:
         s.destroy()
+
+
+@pytest.mark.gpu
+def test_noalloc_at_the_exact_capacity(lib):
+    """65535 x-cells of a 2x2 cross-section need exactly 65536 block partials,
+    the size of the static array, and two energy launches (grid y is split at
+    65535 planes): accepted, and bit-equal to cem_energy on two calls in a row."""
+    nx = 65535
+    x = np.arange(nx + 1) * 1e-4
+    y = np.arange(3) * 1e-4
+    s = lib.createSim(x, y, y)
+    try:
+        p = s.addLumpedPort(2, 100, 1, 0, 2, -1, 50.0)
+        s.setGaussian(p, 1.0, 8e-12, 2e-12)
+        s.finalize()
+        s.step(60)
+        ref = s.energy()
+        assert ref > 0 and math.isfinite(ref)
+        assert s.energyNoAlloc() == ref and s.energyNoAlloc() == ref
+    finally:
+        s.destroy()
