@@ -106,7 +106,9 @@ struct Space {
     int t0[kMaxRects + 1];                  // t0[n]: threads of the space
     unsigned long long magic[kMaxRects];    // row in its rectangle of thread t - t0: ((t - t0) * magic) >> 40
 };
-constexpr int kFast = 0, kGeneral = 1, kAll = 2;
+// E only: kDebye, the interior rectangles that meet a Debye box but no CPML
+// slab (the lean Debye kernel's space; general otherwise).
+constexpr int kFast = 0, kGeneral = 1, kAll = 2, kDebye = 3, kSpaces = 4;
 
 struct StepArgs {
     Geom g;
@@ -120,6 +122,8 @@ struct StepArgs {
     const unsigned short *mat[3];
     const float *tab[3];          // field-major: ca-1, cb, cs, beta_p/dt (p = 0..P-1)
     const float4 *tab4[3];        // packed per entry: ca-1, cb, cs, flags (bit pattern)
+    const float4 *beta4[3];       // per entry: beta_p/dt of the P poles, nb4 float4 (zero beyond P)
+    int nb4;
     int ntab[3];
     int npole;
     float omk[kMaxPoles], hk[kMaxPoles];
@@ -133,7 +137,7 @@ struct StepArgs {
     const long long *dstep;
     const float *srcv;       // lumped Vs and modal Vm at this step's H time, FP32 (source_values)
     // thread spaces last: batched kernels stage the arguments before them
-    Space sp[2][3];          // [H, E][kFast, kGeneral, kAll]
+    Space sp[2][4];          // [H, E][kFast, kGeneral, kAll, kDebye]
     int p0[2], p1[2];        // interior node planes of H and E
 };
 
@@ -349,11 +353,16 @@ __device__ __forceinline__ float debye_term(const StepArgs &a, int p, float jp, 
     return __fmaf_rn(a.hk[p], jp, acc);
 }
 
-// Debye current update of pole p of a dispersive edge with table index mi
-// (reference dispersive.c:105-112): J_p += -(1-k_p) J_p + beta_p/dt (E_new - E_old)
+// beta_p/dt of pole p for table entry mi of component C (packed table)
 template <int C>
-__device__ __forceinline__ float debye_next(const StepArgs &a, int p, int mi, float de, float jp) {
-    const float bidt = __ldg(a.tab[C] + (3 + p) * a.ntab[C] + mi);
+__device__ __forceinline__ float beta_at(const StepArgs &a, int mi, int p) {
+    return __ldg(reinterpret_cast<const float *>(a.beta4[C] + mi * a.nb4) + p);
+}
+
+// Debye current update of pole p of a dispersive edge (reference
+// dispersive.c:105-112): J_p += -(1-k_p) J_p + beta_p/dt (E_new - E_old),
+// bidt = beta_p/dt of the edge's table entry
+__device__ __forceinline__ float debye_next(const StepArgs &a, int p, float bidt, float de, float jp) {
     return __fmaf_rn(bidt, de, __fmaf_rn(-a.omk[p], jp, jp));
 }
 
@@ -421,7 +430,7 @@ __device__ __forceinline__ float e_comp(const StepArgs &a, int i, int j, int k, 
 #pragma unroll
         for (int p = 0; p < P; p++) {
             float *jp = a.J[C] + p * jvol + jo;
-            *jp = debye_next<C>(a, p, mi, de, *jp);
+            *jp = debye_next(a, p, beta_at<C>(a, mi, p), de, *jp);
         }
     }
     return r;
@@ -756,7 +765,7 @@ __device__ __forceinline__ void e_points(const StepArgs &a, int i, int j, int k4
             float4 jv = ld4(jp);
 #pragma unroll
             for (int e = 0; e < 4; e++)
-                if (disp[e]) set4(jv, e, debye_next<C>(a, p, mi[e], de[e], lane4(jv, e)));
+                if (disp[e]) set4(jv, e, debye_next(a, p, beta_at<C>(a, mi[e], p), de[e], lane4(jv, e)));
             st4(jp, jv);
         }
     }
@@ -885,6 +894,88 @@ __device__ __forceinline__ void e_lean(const StepArgs &a, int i, const RowPos &p
     st4(E + q, r);
 }
 
+// E component C at points k4 .. k4+3 of row (i, j) of a Debye piece: no
+// CPML auxiliary on a derivative axis, the points in or beside the
+// component's Debye box. The P pole currents of the four points are read
+// once as float4 and kept in registers for both sum_p hk_p J_p and their own
+// update, then written once; beta_p/dt comes packed per table entry. Every
+// rounding is that of e_points.
+template <int C, int P>
+__device__ __forceinline__ void e_debye(const StepArgs &a, int i, const RowPos &p, const float2 sv) {
+    constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    constexpr int NB = (P + 3) / 4;
+    const int ny = a.g.n[1], nz = a.g.n[2];
+    const int j = p.j, k4 = p.k4;
+    const bool row = p.act && (C == 0 || i >= 1) && (C == 1 ? j < ny : (j >= 1 && j < ny));
+    const int q = i * (int)a.g.si + j * a.g.sj + k4;
+    const float *__restrict__ H2 = a.H[A2];
+    const float *__restrict__ H1 = a.H[A1];
+    float *__restrict__ E = a.E[C];
+    float *__restrict__ Jc = a.J[C];
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 h2 = z4, h1 = z4, ev = z4, h2m = z4, h1m = z4;
+    uint2 mv = make_uint2(0, 0);
+    // the four points' offset in the Debye box (k extent aligned to four: all in or all out)
+    const int *bx = a.jbox[C];
+    const int jo4 = row && k4 >= bx[2] && k4 < bx[2] + bx[5] ? jbox_at<C>(a, i, j, k4) : -1;
+    const int jvol = jbox_volume<C>(a);
+    float4 J[P > 0 ? P : 1];
+    if (row) {
+        h2 = ldg4(H2 + q);
+        h1 = ldg4(H1 + q);
+        ev = ld4(E + q);
+        mv = __ldg(reinterpret_cast<const uint2 *>(a.mat[C] + q));
+        if (A1 != 2) h2m = ldg4(H2 + q - stride_of<A1>(a));
+        if (A2 != 2) h1m = ldg4(H1 + q - stride_of<A2>(a));
+    }
+#pragma unroll
+    for (int pp = 0; pp < P; pp++) J[pp] = jo4 >= 0 ? ld4(Jc + pp * jvol + jo4) : z4;
+    const bool first = (threadIdx.x & 31) == 0 || k4 == p.ks;
+    if (A1 == 2) h2m = prev_k(h2, H2 + q, row && k4 > 0, first);
+    if (A2 == 2) h1m = prev_k(h1, H1 + q, row && k4 > 0, first);
+    if (!row) return;
+    const float ci = __ldg(a.ec[0] + i), cj = __ldg(a.ec[1] + j);
+    const float4 ck = ldg4(a.ec[2] + k4);
+    const int mi[4] = {(int)(mv.x & 0xffffu), (int)(mv.x >> 16), (int)(mv.y & 0xffffu), (int)(mv.y >> 16)};
+    float s = 0.f;
+    float4 r = ev;
+    float de[4];
+    bool disp[4];
+    bool any = false;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int k = k4 + e;
+        const float4 t = __ldg(a.tab4[C] + mi[e]);
+        float jsum = 0.f;
+#pragma unroll
+        for (int pp = 0; pp < P; pp++) jsum = debye_term(a, pp, lane4(J[pp], e), jsum);
+        const float c[3] = {ci, cj, lane4(ck, e)};
+        const float v = e_value<C>(a, t, i, j, k, sv, lane4(ev, e), __fsub_rn(lane4(h2, e), lane4(h2m, e)),
+                                   __fsub_rn(lane4(h1, e), lane4(h1m, e)), c[A1], c[A2], false, false, s, s, jsum);
+        const bool own = C == 2 ? k < nz : (k >= 1 && k < nz);
+        if (own) set4(r, e, v);
+        disp[e] = own && jo4 >= 0 && (__float_as_uint(t.w) & kFlagDisp);
+        de[e] = __fsub_rn(v, lane4(ev, e));
+        any = any || disp[e];
+    }
+    st4(E + q, r);
+    if (!any) return;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        if (!disp[e]) continue;
+        float b[4 * (NB > 0 ? NB : 1)];
+#pragma unroll
+        for (int h = 0; h < NB; h++) {
+            const float4 v = __ldg(a.beta4[C] + mi[e] * NB + h);
+            b[4 * h] = v.x; b[4 * h + 1] = v.y; b[4 * h + 2] = v.z; b[4 * h + 3] = v.w;
+        }
+#pragma unroll
+        for (int pp = 0; pp < P; pp++) set4(J[pp], e, debye_next(a, pp, b[pp], de[e], lane4(J[pp], e)));
+    }
+#pragma unroll
+    for (int pp = 0; pp < P; pp++) st4(Jc + pp * jvol + jo4, J[pp]);
+}
+
 // H over node planes [i0, i0 + gridDim.y) (cem_mt_H and the unfused step)
 // Resident blocks (of kBlock threads) per SM the update kernels are
 // compiled for: register caps of 51 and 64 per thread for the general H and
@@ -924,6 +1015,22 @@ __global__ void __launch_bounds__(kBlock, CB2_EF_MINBLOCKS) k_update_e_fast(cons
     if (comp == 0) e_lean<0>(a, i, p, sv);
     else if (comp == 1) e_lean<1>(a, i, p, sv);
     else e_lean<2>(a, i, p, sv);
+}
+
+#ifndef CB2_ED_MINBLOCKS
+#define CB2_ED_MINBLOCKS 6
+#endif
+
+// E on the Debye rectangles of node planes [i0, i0 + gridDim.y) (P poles)
+template <int P>
+__global__ void __launch_bounds__(kBlock, CB2_ED_MINBLOCKS) k_update_e_debye(const StepArgs a, int i0) {
+    const int comp = blockIdx.x % 3;
+    const RowPos p = space_pos(a.sp[1][kDebye], blockIdx.x / 3);
+    const int i = i0 + blockIdx.y;
+    const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
+    if (comp == 0) e_debye<0, P>(a, i, p, sv);
+    else if (comp == 1) e_debye<1, P>(a, i, p, sv);
+    else e_debye<2, P>(a, i, p, sv);
 }
 
 // Position in the general space of update U: the general rectangles on an
@@ -1167,10 +1274,13 @@ using FKernel = void (*)(StepArgs, FusedArgs, TmaMaps);
 #define CB2_POLES(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
 #define CB2_EK(p) k_update_e<p>,
 #define CB2_FK(p) k_step_fused<p>,
+#define CB2_DK(p) k_update_e_debye<p>,
 const EKernel kEKernels[] = {CB2_POLES(CB2_EK)};
 const FKernel kFKernels[] = {CB2_POLES(CB2_FK)};
+const HKernel kEDKernels[] = {CB2_POLES(CB2_DK)};
 #undef CB2_EK
 #undef CB2_FK
+#undef CB2_DK
 #undef CB2_POLES
 
 // ------------------------------------------------------------------- SIBC
@@ -1361,8 +1471,8 @@ __device__ __forceinline__ void stage_member(const StepArgs *args, int x, unsign
     for (int q = threadIdx.x; q < kStaged / 4; q += blockDim.x) buf[q] = s[q];
     constexpr int sw = (int)(sizeof(Space) / 4);
     const int c0 = FAST ? kFast : kGeneral;
-    for (int c = c0; c <= (FAST ? kFast : kAll); c++) {
-        const int off = (int)((offsetof(StepArgs, sp) + (U * 3 + c) * sizeof(Space)) / 4);
+    for (int c = c0; c < (FAST ? kFast + 1 : kSpaces); c++) {
+        const int off = (int)((offsetof(StepArgs, sp) + (U * kSpaces + c) * sizeof(Space)) / 4);
         for (int q = threadIdx.x; q < sw; q += blockDim.x) buf[off + q] = s[off + q];
     }
     constexpr int po = (int)(offsetof(StepArgs, p0) / 4);
@@ -1412,7 +1522,9 @@ __global__ void __launch_bounds__(kBlock, FAST ? CB2_EF_MINBLOCKS : CB2_E_MINBLO
             stage_member<1, FAST>(args, w.x, buf);
             staged = w.x;
         }
-        const RowPos r = FAST ? space_pos(a.sp[1][kFast], w.y / 3) : general_pos<1>(a, w.z, w.y / 3);
+        // general entries: w.w = 1 for blocks of the Debye space (general code, the same bits)
+        const RowPos r = FAST ? space_pos(a.sp[1][kFast], w.y / 3)
+                              : (w.w ? space_pos(a.sp[1][kDebye], w.y / 3) : general_pos<1>(a, w.z, w.y / 3));
         const float2 sv = *reinterpret_cast<const float2 *>(a.srcv);
         const int comp = w.y % 3;
         if (FAST) {
@@ -1549,6 +1661,7 @@ struct Device {
     DevBuf<unsigned short> mat[3];
     DevBuf<float> tab[3];
     DevBuf<float4> tab4[3];
+    DevBuf<float4> beta4[3];   // beta_p/dt per table entry, (P + 3) / 4 float4 each
     DevBuf<double> cb64[3];
     int ntab[3] = {0, 0, 0};
     DevBuf<float> J[3];
@@ -1557,7 +1670,7 @@ struct Device {
     // interior node planes [p0, p1), and the work-list of the general blocks
     // (entries: node plane, block of the plane's general space incl.
     // component) in plane order; wl_start[u][i] is the first entry of plane i.
-    Space sp[2][3]{};
+    Space sp[2][kSpaces]{};
     int p0[2] = {0, 0}, p1[2] = {0, 0};
     DevBuf<int2> wl[2];
     std::vector<int> wl_start[2];
@@ -1866,6 +1979,14 @@ bool build_tables(cem_sim *s, Device &D) {
                 packed[e] = make_float4(tb.rows[e * nfields], tb.rows[e * nfields + 1], tb.rows[e * nfields + 2], fbits);
             }
             if (!dev_upload(s, D.tab4[c], packed)) return false;
+            const int nb4 = (P + 3) / 4;
+            if (nb4) {
+                std::vector<float4> beta(ne * nb4, make_float4(0.f, 0.f, 0.f, 0.f));
+                for (size_t e = 0; e < ne; e++)
+                    for (int p = 0; p < P; p++)
+                        reinterpret_cast<float *>(&beta[e * nb4])[p] = tb.rows[e * nfields + 3 + p];
+                if (!dev_upload(s, D.beta4[c], beta)) return false;
+            }
         }
         if (!dev_upload(s, D.cb64[c], tb.cb64)) return false;
         if (box_hi[0] >= 0) {
@@ -2110,7 +2231,7 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
         v->erase(std::unique(v->begin(), v->end()), v->end());
     }
     struct Rect { int ks, ke, js, je; };
-    std::vector<Rect> cls[3];
+    std::vector<Rect> cls[kSpaces];
     for (size_t q = 0; q + 1 < kb.size(); q++) {
         const int ks = kb[q], ke = kb[q + 1];
         bool zs = false;
@@ -2118,24 +2239,26 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
         cls[kAll].push_back({ks, ke, 0, rows});
         for (size_t r = 0; r + 1 < jb.size(); r++) {
             const int js = jb[r], je = jb[r + 1];
-            bool gen = zs;
-            for (int j = js; j < je && !gen; j++) gen = slab(1, j);
+            bool pml = zs, deb = false;
+            for (int j = js; j < je && !pml; j++) pml = slab(1, j);
             for (const int *bx : boxes)
-                gen = gen || (ke > bx[2] && ks < bx[2] + bx[5] && je > bx[1] && js < bx[1] + bx[4]);
-            std::vector<Rect> &v = cls[gen ? kGeneral : kFast];
+                deb = deb || (ke > bx[2] && ks < bx[2] + bx[5] && je > bx[1] && js < bx[1] + bx[4]);
+            std::vector<Rect> &v = cls[pml ? kGeneral : (deb ? kDebye : kFast)];
             if (!v.empty() && v.back().ks == ks && v.back().je == js) v.back().je = je;
             else v.push_back({ks, ke, js, je});
         }
     }
-    if (p1 <= p0 || (int)cls[kFast].size() > kMaxRects || (int)cls[kGeneral].size() > kMaxRects) {
+    if (p1 <= p0 || (int)cls[kFast].size() > kMaxRects || (int)cls[kGeneral].size() > kMaxRects ||
+        (int)cls[kDebye].size() > kMaxRects) {
         cls[kFast].clear();   // no interior planes, or too many rectangles: every block general
+        cls[kDebye].clear();
         cls[kGeneral] = cls[kAll];
     }
     if ((int)cls[kAll].size() > kMaxRects) {
         set_error("too many k segments");
         return false;
     }
-    for (int c = 0; c < 3; c++) {
+    for (int c = 0; c < kSpaces; c++) {
         Space &sp = D.sp[u][c];
         sp = Space{};
         long long t = 0;
@@ -2195,7 +2318,7 @@ void fill_args_for(cem_sim *s, Device &D, int cur) {
     a = StepArgs{};
     a.g = D.g;
     for (int u = 0; u < 2; u++) {
-        for (int c = 0; c < 3; c++) a.sp[u][c] = D.sp[u][c];
+        for (int c = 0; c < kSpaces; c++) a.sp[u][c] = D.sp[u][c];
         a.p0[u] = D.p0[u];
         a.p1[u] = D.p1[u];
     }
@@ -2213,6 +2336,7 @@ void fill_args_for(cem_sim *s, Device &D, int cur) {
         a.mat[c] = D.mat[c].p;
         a.tab[c] = D.tab[c].p;
         a.tab4[c] = D.tab4[c].p;
+        a.beta4[c] = D.beta4[c].p;
         a.ntab[c] = D.ntab[c];
         a.J[c] = D.J[c].p;
         for (int q = 0; q < 6; q++) a.jbox[c][q] = D.jbox[c][q];
@@ -2220,6 +2344,7 @@ void fill_args_for(cem_sim *s, Device &D, int cur) {
     a.dth = (float)(s->dt / CEM_MU0);
     a.has_pml = s->has_pml;
     a.npole = s->npole;
+    a.nb4 = (s->npole + 3) / 4;
     for (int p = 0; p < s->npole; p++) {
         const double tau = 1.0 / (2 * M_PI * s->pole_f[p]);
         const double r = s->dt / (2 * tau);
@@ -2712,9 +2837,9 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
         p = D.wl[u].p + st[a];
         return (unsigned)(st[b] - st[a]);
     };
-    // fast rectangles of update u on node planes [a, b)
-    auto fast = [&](int u, int a, int b, auto kernel) {
-        const int nb = space_blocks(D.sp[u][kFast]);
+    // fast (or Debye) rectangles of update u on node planes [a, b)
+    auto fast = [&](int u, int a, int b, auto kernel, int cls = kFast) {
+        const int nb = space_blocks(D.sp[u][cls]);
         const int c0 = std::max(a, D.p0[u]), c1 = std::min(b, D.p1[u]);
         if (nb == 0) return;
         for (int c = c0; c < c1; c += kMaxGridY)
@@ -2760,6 +2885,7 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
                 cudaEventRecord(D.join, D.side);
             }
             fast(1, a, b, k_update_e_fast);
+            fast(1, a, b, kEDKernels[s->npole], kDebye);
             if (n) join();
             t_end();
         }
@@ -3139,6 +3265,7 @@ bool batch_rebuild(cemx_batch *b) {
             for (int bx = 0; ie && bx < blocks(1, kFast); bx++) wef.push_back(make_int4(x, bx, i, 0));
             for (int bx = 0; bx < blocks(1, ie ? kGeneral : kAll); bx++)
                 we[s->npole].push_back(make_int4(x, bx, i, 0));
+            for (int bx = 0; ie && bx < blocks(1, kDebye); bx++) we[s->npole].push_back(make_int4(x, bx, i, 1));
         }
     };
     if (b->order == 0) {
