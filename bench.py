@@ -385,7 +385,7 @@ def run_b200(args) -> None:
     value = replica_rate(world, cells, chunk * args.steps, gpu_ms)
 
     # per-kernel device time (event pair per launch) for the roofline
-    prof = s.profileSteps(args.profile_steps)
+    prof = s.profileSteps(max(args.profile_steps, 1))
     ab = algorithmic_bytes(z)
     kern = {k: v for k, v in prof.items() if v["launches"]}
     dominant = max(kern, key=lambda k: kern[k]["ms"])

@@ -34,6 +34,7 @@
 #include <memory>
 #include <thread>
 #include <map>
+#include <chrono>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -2498,8 +2499,21 @@ bool create_device_impl(cem_sim *s) {
         if (!dev_upload(s, D.hc[c], to_f32(hc)) || !dev_upload(s, D.ec[c], to_f32(ec))) return false;
         if (!dev_upload(s, D.d64[c], s->d[c]) || !dev_upload(s, D.dd64[c], s->dd[c])) return false;
     }
-    if (!build_pml(s, D) || !build_tables(s, D) || !build_probes(s, D) || !build_sibc(s, D) || !build_sources(s, D) ||
-        !build_spaces(s, D, 0) || !build_spaces(s, D, 1))
+    // CEM_B200_TRACE=1: the host time of each set-up phase on stderr
+    static const bool trace = [] { const char *e = std::getenv("CEM_B200_TRACE"); return e && e[0] == '1'; }();
+    auto t0 = std::chrono::steady_clock::now();
+    auto phase = [&](const char *name, bool ok) {
+        if (trace) {
+            const auto t1 = std::chrono::steady_clock::now();
+            std::fprintf(stderr, "courant-b200: device set-up %-8s %8.3f s\n", name,
+                         std::chrono::duration<double>(t1 - t0).count());
+            t0 = t1;
+        }
+        return ok;
+    };
+    if (!phase("fields", true) || !phase("pml", build_pml(s, D)) || !phase("tables", build_tables(s, D)) ||
+        !phase("probes", build_probes(s, D)) || !phase("sibc", build_sibc(s, D)) ||
+        !phase("sources", build_sources(s, D)) || !phase("spaces", build_spaces(s, D, 0) && build_spaces(s, D, 1)))
         return false;
     for (int b = 0; b < 2; b++)
         for (int c = 0; c < 3; c++)
