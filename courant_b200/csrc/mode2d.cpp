@@ -1,23 +1,38 @@
 // 2D full-wave eigenmode solver on a Yee cross-section (FP64, host).
 //
-// Propagation along +x with fields ~ exp(-j beta x); transverse unknowns
-//   E_u = Ey(j+1/2,k)  E_v = Ez(j,k+1/2)  E_w = Ex(j,k)
-//   H_u = Hy(j,k+1/2)  H_v = Hz(j+1/2,k)  H_w = Hx(j+1/2,k+1/2)
-// with beta e = P h, beta h = Q e, i.e. beta^2 e = (P Q) e. Complex arithmetic
-// carries the stretched-coordinate PML (s = kappa + sigma/(alpha + j w eps0)),
-// conductivity and Debye dispersion. P Q is applied matrix-free, assembled in
-// band storage by probing with coloured unit vectors, factorised by a banded
-// LU with partial pivoting, and the eigenpair nearest (k0 n_guess)^2 is found
-// by shifted inverse iteration.
+// The physics is the reference's mode formulation (skyhoffert/CourantEM
+// solver/src/mode2d.c:1-20), which the 3D mode ports must reproduce: fields
+// ~ exp(-j beta x) along +x on the transverse Yee cell
+//   E_u = Ey(j+1/2, k)   E_v = Ez(j, k+1/2)   E_w = Ex(j, k)
+//   H_u = Hy(j, k+1/2)   H_v = Hz(j+1/2, k)   H_w = Hx(j+1/2, k+1/2)
+// with beta e = P h, beta h = Q e, so beta^2 is an eigenvalue of A = P Q acting
+// on the transverse E unknowns. Derivatives carry the stretched-coordinate PML
+// factor 1/(s d), s = kappa + sigma/(alpha + j w eps0), and media are complex
+// (eps - j sigma/w, Debye poles). The window's outer boundary is PEC.
 //
-// The formulation, unknown ordering, probing pattern, shift and start vector
-// are those of the reference solver (skyhoffert/CourantEM solver/src/mode2d.c),
-// because the 3D mode-port results must match the oracle; std::complex<double>
-// under GCC performs the same IEEE complex operations as C99 double complex.
+// The solver is this library's own:
+//  * A is assembled in closed form. Writing Q and P out, the longitudinal
+//    field is E_w = w iw div_t(eps E_t) (the curl terms of H_u, H_v cancel in
+//    the divergence), so each row of A is
+//        w^2 mu0 eps E  -  curl_t curl_t E  +  grad_t(iw div_t(eps E_t))
+//    with at most 15 couplings (E_u: k +- 1, j +- 1 and the four E_v around
+//    it), computed directly instead of by applying the operator to probe
+//    vectors.
+//  * Unknowns on metal (and on the PEC window boundary) are not part of the
+//    system at all; the rest are numbered j-major, then k, E_u before E_v, so
+//    the band half-width is about 2 nz + 2.
+//  * The band is factorised by LU with partial pivoting in row-major storage
+//    (each row holds its band plus the pivoting fill), with the complex
+//    arithmetic written out so the update loops vectorise.
+//  * The eigenpair nearest sigma = (k0 n_guess)^2 comes from shifted inverse
+//    iteration: converged when the eigenvalue estimate sigma + 1/<x, y> changes
+//    by less than tol relatively and the phase-aligned iterate by less than
+//    1e-10, the reference's stopping rule.
 #include "sim.hpp"
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <vector>
 
@@ -29,190 +44,261 @@ using cb2::cplx;
 
 struct cem_mode2d {
     int ny = 0, nz = 0;
-    std::vector<double> y, z, dy, dz, ddy, ddz;
-    std::vector<double> er_u, er_v, er_w, sg_u, sg_v, sg_w;
-    std::vector<uint8_t> pec_u, pec_v, pec_w;
+    std::vector<double> y, z;
+    std::vector<double> hy, hz;    // cell sizes
+    std::vector<double> gy, gz;    // dual sizes at the nodes (half cells at the ends)
+    // media at the three E locations (u, v, w): relative permittivity,
+    // conductivity, metal flag, Debye pole strengths (npole blocks)
+    struct Media {
+        std::vector<double> eps, sig, deps;
+        std::vector<uint8_t> metal;
+    } med[3];
     int npole = 0;
     double pole_f[cb2::kMaxPoles] = {};
-    std::vector<double> dp_u, dp_v, dp_w;   // npole blocks
-    std::vector<double> ps[4], pk[4], pa[4];   // PML sigma/kappa/alpha: y cells, y nodes, z cells, z nodes
+    // stretching profiles: [0] y cells, [1] y nodes, [2] z cells, [3] z nodes
+    std::vector<double> pml_s[4], pml_k[4], pml_a[4];
     double freq = 0;
     cplx beta = 0;
-    std::vector<cplx> eu, ev, hu, hv;
+    std::vector<cplx> eu, ev, hu, hv;   // last mode (API layout: E_u/H_v at j*(nz+1)+k, E_v/H_u at j*nz+k)
 
-    // flat indices: E_u and H_v (j<ny, k<=nz), E_v and H_u (j<=ny, k<nz), nodes, cells
-    int iu(int j, int k) const { return j * (nz + 1) + k; }
-    int iv(int j, int k) const { return j * nz + k; }
-    int in(int j, int k) const { return j * (nz + 1) + k; }
-    int ic(int j, int k) const { return j * nz + k; }
-    int nu() const { return ny * (nz + 1); }
-    int nv() const { return (ny + 1) * nz; }
-    int nn() const { return (ny + 1) * (nz + 1); }
+    int at_u(int j, int k) const { return j * (nz + 1) + k; }   // E_u, H_v: j < ny, k <= nz
+    int at_v(int j, int k) const { return j * nz + k; }         // E_v, H_u: j <= ny, k < nz
+    int at_n(int j, int k) const { return j * (nz + 1) + k; }   // nodes
+    int count(int which) const { return which == 0 ? ny * (nz + 1) : (which == 1 ? (ny + 1) * nz : (ny + 1) * (nz + 1)); }
 };
 
 namespace {
 
-// Coefficients for one angular frequency.
-struct Coef {
-    std::vector<cplx> iyc, iyn, izc, izn;   // 1/(s d) at y cells, y nodes, z cells, z nodes
-    std::vector<cplx> eu, ev, iw;           // complex permittivity of E_u, E_v; 1/eps at E_w (0 on PEC)
+constexpr int U = 0, V = 1, W = 2;
+
+// Coefficients of one angular frequency: 1/(s d) per grid line, absolute
+// complex permittivity of E_u and E_v, and 1/eps at the E_w nodes (0 on metal).
+struct Coeffs {
+    std::vector<cplx> ryc, ryn, rzc, rzn;
+    std::vector<cplx> eps_u, eps_v, inv_w;
 };
 
-Coef make_coef(const cem_mode2d &m, double w) {
-    const int ny = m.ny, nz = m.nz;
-    Coef c;
-    const cplx jw = cplx(0.0, 1.0) * w * CEM_EPS0;
-    auto stretch = [&](int a, int i) { return m.pk[a][i] + m.ps[a][i] / (m.pa[a][i] + jw); };
-    c.iyc.resize(ny); c.iyn.resize(ny + 1); c.izc.resize(nz); c.izn.resize(nz + 1);
-    for (int j = 0; j < ny; j++) c.iyc[j] = 1.0 / (stretch(0, j) * m.dy[j]);
-    for (int j = 0; j <= ny; j++) c.iyn[j] = 1.0 / (stretch(1, j) * m.ddy[j]);
-    for (int k = 0; k < nz; k++) c.izc[k] = 1.0 / (stretch(2, k) * m.dz[k]);
-    for (int k = 0; k <= nz; k++) c.izn[k] = 1.0 / (stretch(3, k) * m.ddz[k]);
-    cplx dfac[cb2::kMaxPoles];
-    for (int p = 0; p < m.npole; p++) dfac[p] = 1.0 / (1.0 + cplx(0.0, 1.0) * w / (2 * M_PI * m.pole_f[p]));
-    const cplx jay(0.0, 1.0);
-    auto permittivity = [&](double er, const std::vector<double> &dp, size_t stride, size_t q, double sg) {
-        cplx e = er;
-        for (int p = 0; p < m.npole; p++) e += dp[(size_t)p * stride + q] * dfac[p];
-        return e * CEM_EPS0 - jay * sg / w;
+Coeffs coefficients(const cem_mode2d &m, double w) {
+    Coeffs c;
+    const cplx jwe0(0.0, w * CEM_EPS0);
+    auto inv_stretched = [&](int prof, int i, double d) {
+        return 1.0 / ((m.pml_k[prof][i] + m.pml_s[prof][i] / (m.pml_a[prof][i] + jwe0)) * d);
     };
-    const int nu = m.nu(), nv = m.nv(), nn = m.nn();
-    c.eu.resize(nu); c.ev.resize(nv); c.iw.resize(nn);
-    for (int q = 0; q < nu; q++) c.eu[q] = permittivity(m.er_u[q], m.dp_u, nu, q, m.sg_u[q]);
-    for (int q = 0; q < nv; q++) c.ev[q] = permittivity(m.er_v[q], m.dp_v, nv, q, m.sg_v[q]);
-    for (int q = 0; q < nn; q++)
-        c.iw[q] = m.pec_w[q] ? cplx(0) : 1.0 / permittivity(m.er_w[q], m.dp_w, nn, q, m.sg_w[q]);
+    for (int j = 0; j < m.ny; j++) c.ryc.push_back(inv_stretched(0, j, m.hy[j]));
+    for (int j = 0; j <= m.ny; j++) c.ryn.push_back(inv_stretched(1, j, m.gy[j]));
+    for (int k = 0; k < m.nz; k++) c.rzc.push_back(inv_stretched(2, k, m.hz[k]));
+    for (int k = 0; k <= m.nz; k++) c.rzn.push_back(inv_stretched(3, k, m.gz[k]));
+    cplx relax[cb2::kMaxPoles];
+    for (int p = 0; p < m.npole; p++) relax[p] = 1.0 / cplx(1.0, w / (2 * M_PI * m.pole_f[p]));
+    auto permittivity = [&](int which, int q) {
+        const cem_mode2d::Media &md = m.med[which];
+        cplx e = md.eps[q];
+        const int n = m.count(which);
+        for (int p = 0; p < m.npole; p++) e += md.deps[(size_t)p * n + q] * relax[p];
+        return e * CEM_EPS0 - cplx(0.0, md.sig[q] / w);
+    };
+    for (int q = 0; q < m.count(U); q++) c.eps_u.push_back(permittivity(U, q));
+    for (int q = 0; q < m.count(V); q++) c.eps_v.push_back(permittivity(V, q));
+    for (int q = 0; q < m.count(W); q++) c.inv_w.push_back(m.med[W].metal[q] ? cplx(0.0) : 1.0 / permittivity(W, q));
     return c;
 }
 
-// h = Q e (curl of E and Faraday's law); hw: work array over cells
-void apply_q(const cem_mode2d &m, const Coef &c, double w, const cplx *eu, const cplx *ev, cplx *hu, cplx *hv,
-             cplx *hw) {
-    const int ny = m.ny, nz = m.nz;
-    for (int j = 0; j < ny; j++)
-        for (int k = 0; k < nz; k++)
-            hw[m.ic(j, k)] = (ev[m.iv(j + 1, k)] - ev[m.iv(j, k)]) * c.iyc[j] - (eu[m.iu(j, k + 1)] - eu[m.iu(j, k)]) * c.izc[k];
-    const double cc = 1.0 / (w * CEM_MU0);
-    for (int j = 0; j <= ny; j++)
-        for (int k = 0; k < nz; k++) {
-            const cplx r = (j < ny ? hw[m.ic(j, k)] : 0.0) - (j > 0 ? hw[m.ic(j - 1, k)] : 0.0);
-            hu[m.iv(j, k)] = -w * c.ev[m.iv(j, k)] * ev[m.iv(j, k)] - cc * r * c.iyn[j];
-        }
-    for (int j = 0; j < ny; j++)
-        for (int k = 0; k <= nz; k++) {
-            const cplx r = (k < nz ? hw[m.ic(j, k)] : 0.0) - (k > 0 ? hw[m.ic(j, k - 1)] : 0.0);
-            hv[m.iu(j, k)] = w * c.eu[m.iu(j, k)] * eu[m.iu(j, k)] - cc * r * c.izn[k];
-        }
-}
-
-// e = P h (Ampere's law with the longitudinal E eliminated); ew: work array over nodes
-void apply_p(const cem_mode2d &m, const Coef &c, double w, const cplx *hu, const cplx *hv, cplx *eu, cplx *ev,
-             cplx *ew) {
-    const int ny = m.ny, nz = m.nz;
-    for (int j = 0; j <= ny; j++)
-        for (int k = 0; k <= nz; k++) {
-            const cplx du = ((j < ny ? hv[m.iu(j, k)] : 0.0) - (j > 0 ? hv[m.iu(j - 1, k)] : 0.0)) * c.iyn[j];
-            const cplx dv = ((k < nz ? hu[m.iv(j, k)] : 0.0) - (k > 0 ? hu[m.iv(j, k - 1)] : 0.0)) * c.izn[k];
-            ew[m.in(j, k)] = (du - dv) * c.iw[m.in(j, k)];
-        }
-    const double cc = 1.0 / w;
-    for (int j = 0; j < ny; j++)
-        for (int k = 0; k <= nz; k++)
-            eu[m.iu(j, k)] = w * CEM_MU0 * hv[m.iu(j, k)] + cc * (ew[m.in(j + 1, k)] - ew[m.in(j, k)]) * c.iyc[j];
-    for (int j = 0; j <= ny; j++)
-        for (int k = 0; k < nz; k++)
-            ev[m.iv(j, k)] = -w * CEM_MU0 * hu[m.iv(j, k)] + cc * (ew[m.in(j, k + 1)] - ew[m.in(j, k)]) * c.izc[k];
-}
-
-// Unknown ordering: j outer, k inner, E_u and E_v interleaved, which keeps the
-// half-bandwidth near 2 (nz + 2).
-struct Unknowns {
-    std::vector<int> kind, idx;   // kind 0: E_u, 1: E_v
+// Unknown numbering of the field points off metal: j-major, k, E_u before E_v.
+struct Numbering {
+    std::vector<int> of_u, of_v;    // system index of each E_u / E_v point, -1 on metal
+    std::vector<int> where;         // per system index: 2 * point + (0 for E_u, 1 for E_v)
     int n = 0;
 };
 
-Unknowns make_unknowns(const cem_mode2d &m) {
-    Unknowns o;
+Numbering number_unknowns(const cem_mode2d &m) {
+    Numbering o;
+    o.of_u.assign(m.count(U), -1);
+    o.of_v.assign(m.count(V), -1);
     for (int j = 0; j <= m.ny; j++)
         for (int k = 0; k <= m.nz; k++) {
-            if (j < m.ny) { o.kind.push_back(0); o.idx.push_back(m.iu(j, k)); }
-            if (k < m.nz) { o.kind.push_back(1); o.idx.push_back(m.iv(j, k)); }
+            if (j < m.ny && !m.med[U].metal[m.at_u(j, k)]) {
+                o.of_u[m.at_u(j, k)] = o.n++;
+                o.where.push_back(2 * m.at_u(j, k));
+            }
+            if (k < m.nz && !m.med[V].metal[m.at_v(j, k)]) {
+                o.of_v[m.at_v(j, k)] = o.n++;
+                o.where.push_back(2 * m.at_v(j, k) + 1);
+            }
         }
-    o.n = (int)o.kind.size();
     return o;
 }
 
-bool unknown_is_pec(const cem_mode2d &m, const Unknowns &o, int g) {
-    return o.kind[g] == 0 ? m.pec_u[o.idx[g]] != 0 : m.pec_v[o.idx[g]] != 0;
+// One assembled row: up to 16 (column, value) couplings.
+struct Row {
+    int n = 0;
+    int col[16];
+    cplx val[16];
+    void add(int c, cplx v) {
+        if (c < 0) return;
+        for (int q = 0; q < n; q++)
+            if (col[q] == c) { val[q] += v; return; }
+        col[n] = c;
+        val[n++] = v;
+    }
+};
+
+// Row of A for E_u(j, k) or E_v(j, k) (which = U or V), every term of
+//   w^2 mu0 eps E - curl curl E + grad(iw div(eps E)).
+Row assemble_row(const cem_mode2d &m, const Coeffs &c, const Numbering &o, double w, int which, int j, int k) {
+    const int ny = m.ny, nz = m.nz;
+    const double wwm = w * w * CEM_MU0;
+    Row r;
+    auto u = [&](int jj, int kk) { return (jj >= 0 && jj < ny && kk >= 0 && kk <= nz) ? o.of_u[m.at_u(jj, kk)] : -1; };
+    auto v = [&](int jj, int kk) { return (jj >= 0 && jj <= ny && kk >= 0 && kk < nz) ? o.of_v[m.at_v(jj, kk)] : -1; };
+    auto eu = [&](int jj, int kk) { return c.eps_u[m.at_u(jj, kk)]; };
+    auto ev = [&](int jj, int kk) { return c.eps_v[m.at_v(jj, kk)]; };
+    // h_w(jc, kc) = ryc (E_v(jc+1) - E_v(jc)) - rzc (E_u(kc+1) - E_u(kc)), scaled by s
+    auto hw = [&](int jc, int kc, cplx s) {
+        const cplx a = s * c.ryc[jc], b = s * c.rzc[kc];
+        r.add(v(jc + 1, kc), a);
+        r.add(v(jc, kc), -a);
+        r.add(u(jc, kc + 1), -b);
+        r.add(u(jc, kc), b);
+    };
+    // iw div(eps E) at node (jn, kn), scaled by s
+    auto div = [&](int jn, int kn, cplx s) {
+        const cplx t = s * c.inv_w[m.at_n(jn, kn)];
+        if (t == 0.0) return;
+        const cplx ty = t * c.ryn[jn], tz = t * c.rzn[kn];
+        if (jn < ny) r.add(u(jn, kn), ty * eu(jn, kn));
+        if (jn > 0) r.add(u(jn - 1, kn), -ty * eu(jn - 1, kn));
+        if (kn < nz) r.add(v(jn, kn), tz * ev(jn, kn));
+        if (kn > 0) r.add(v(jn, kn - 1), -tz * ev(jn, kn - 1));
+    };
+    if (which == U) {
+        r.add(u(j, k), wwm * eu(j, k));
+        // - d/dz of h_w across the node line k (cells k-1, k)
+        if (k < nz) hw(j, k, -c.rzn[k]);
+        if (k > 0) hw(j, k - 1, c.rzn[k]);
+        // d/dy of the divergence between nodes j and j+1
+        div(j + 1, k, c.ryc[j]);
+        div(j, k, -c.ryc[j]);
+    } else {
+        r.add(v(j, k), wwm * ev(j, k));
+        // + d/dy of h_w across the node line j (cells j-1, j)
+        if (j < ny) hw(j, k, c.ryn[j]);
+        if (j > 0) hw(j - 1, k, -c.ryn[j]);
+        div(j, k + 1, c.rzc[k]);
+        div(j, k, -c.rzc[k]);
+    }
+    return r;
 }
 
-// Complex band matrix in LAPACK gbtrf layout: element (i, j) at
-// ab[j*ldab + kl + ku + i - j], kl rows of fill kept above the band for pivoting.
+// Complex band matrix in row-major storage: row r keeps columns
+// [r - kl, r + kl + ku] (the upper kl diagonals receive the pivoting fill),
+// as interleaved (re, im) doubles.
 struct Band {
-    int n, kl, ku, ldab;
-    std::vector<cplx> ab;
-    std::vector<int> ipiv;
-    Band(int n_, int bw) : n(n_), kl(bw), ku(bw), ldab(3 * bw + 1), ab((size_t)(3 * bw + 1) * n_), ipiv(n_) {}
-    cplx &at(int i, int j) { return ab[(size_t)j * ldab + (kl + ku + i - j)]; }
-
-    int factor() {
-        const int kv = ku + kl;
-        for (int j = 0; j < n; j++) {
-            const int last = std::min(j + kl, n - 1);
-            int p = j;
-            double best = std::abs(at(j, j));
-            for (int i = j + 1; i <= last; i++) {
-                const double v = std::abs(at(i, j));
-                if (v > best) { best = v; p = i; }
-            }
-            ipiv[j] = p;
-            if (best == 0) return -1;
-            const int jmax = std::min(j + kv, n - 1);
-            if (p != j)
-                for (int c = j; c <= jmax; c++) std::swap(at(j, c), at(p, c));
-            const cplx piv = at(j, j);
-            for (int i = j + 1; i <= last; i++) {
-                at(i, j) /= piv;
-                const cplx l = at(i, j);
-                if (l == 0.0) continue;
-                for (int c = j + 1; c <= jmax; c++) at(i, c) -= l * at(j, c);
-            }
-        }
-        return 0;
-    }
-
-    void solve(cplx *x) {
-        const int kv = ku + kl;
-        for (int j = 0; j < n; j++) {
-            const int p = ipiv[j];
-            if (p != j) std::swap(x[j], x[p]);
-            const int last = std::min(j + kl, n - 1);
-            for (int i = j + 1; i <= last; i++) x[i] -= at(i, j) * x[j];
-        }
-        for (int j = n - 1; j >= 0; j--) {
-            x[j] /= at(j, j);
-            const int first = std::max(j - kv, 0);
-            for (int i = first; i < j; i++) x[i] -= at(i, j) * x[j];
-        }
-    }
+    int n = 0, kl = 0, ku = 0, width = 0;
+    std::vector<double> a;
+    std::vector<int> piv;
+    double *at(int r, int c) { return &a[((size_t)r * width + (size_t)(c - r + kl)) * 2]; }
 };
 
-struct Work {
-    std::vector<cplx> eu, ev, hu, hv, wk;
-    explicit Work(const cem_mode2d &m) : eu(m.nu()), ev(m.nv()), hu(m.nv()), hv(m.nu()), wk(m.nn()) {}
-};
-
-void apply_a(const cem_mode2d &m, const Coef &c, const Unknowns &o, double w, const cplx *x, cplx *y, Work &W) {
-    std::fill(W.eu.begin(), W.eu.end(), cplx(0));
-    std::fill(W.ev.begin(), W.ev.end(), cplx(0));
-    for (int g = 0; g < o.n; g++) {
-        if (unknown_is_pec(m, o, g)) continue;
-        (o.kind[g] == 0 ? W.eu : W.ev)[o.idx[g]] = x[g];
+// LU with partial pivoting, column by column; multipliers stay in the rows
+// they were computed for (interchanges apply from their step on).
+bool band_factor(Band &B) {
+    const int n = B.n, kl = B.kl, reach = B.kl + B.ku;
+    B.piv.assign(n, 0);
+    for (int j = 0; j < n; j++) {
+        const int last = std::min(n - 1, j + kl), cmax = std::min(n - 1, j + reach);
+        int p = j;
+        double best = -1;
+        for (int i = j; i <= last; i++) {
+            const double *x = B.at(i, j);
+            const double mag = std::hypot(x[0], x[1]);
+            if (mag > best) { best = mag; p = i; }
+        }
+        B.piv[j] = p;
+        if (!(best > 0)) return false;
+        if (p != j) {
+            double *rj = B.at(j, j), *rp = B.at(p, j);
+            for (int q = 0; q < 2 * (cmax - j + 1); q++) std::swap(rj[q], rp[q]);
+        }
+        const double *pr = B.at(j, j);
+        const double den = pr[0] * pr[0] + pr[1] * pr[1];
+        const double ir = pr[0] / den, ii = -pr[1] / den;   // 1 / pivot
+        const int len = cmax - j;
+        for (int i = j + 1; i <= last; i++) {
+            double *ri = B.at(i, j);
+            const double lr = ri[0] * ir - ri[1] * ii, li = ri[0] * ii + ri[1] * ir;
+            ri[0] = lr;
+            ri[1] = li;
+            if (lr == 0 && li == 0) continue;
+            double *__restrict__ dst = ri + 2;
+            const double *__restrict__ src = pr + 2;
+            for (int q = 0; q < len; q++) {
+                const double sr = src[2 * q], si = src[2 * q + 1];
+                dst[2 * q] -= lr * sr - li * si;
+                dst[2 * q + 1] -= lr * si + li * sr;
+            }
+        }
     }
-    apply_q(m, c, w, W.eu.data(), W.ev.data(), W.hu.data(), W.hv.data(), W.wk.data());
-    apply_p(m, c, w, W.hu.data(), W.hv.data(), W.eu.data(), W.ev.data(), W.wk.data());
-    for (int g = 0; g < o.n; g++)
-        y[g] = unknown_is_pec(m, o, g) ? cplx(0) : (o.kind[g] == 0 ? W.eu : W.ev)[o.idx[g]];
+    return true;
+}
+
+// x <- (L U)^-1 P x
+void band_solve(Band &B, std::vector<cplx> &x) {
+    const int n = B.n, kl = B.kl, reach = B.kl + B.ku;
+    for (int j = 0; j < n; j++) {
+        if (B.piv[j] != j) std::swap(x[j], x[B.piv[j]]);
+        const cplx xj = x[j];
+        if (xj == 0.0) continue;
+        for (int i = j + 1; i <= std::min(n - 1, j + kl); i++) {
+            const double *l = B.at(i, j);
+            x[i] -= cplx(l[0], l[1]) * xj;
+        }
+    }
+    for (int j = n - 1; j >= 0; j--) {
+        const int cmax = std::min(n - 1, j + reach);
+        const double *row = B.at(j, j);
+        double sr = x[j].real(), si = x[j].imag();
+        for (int q = 1; q <= cmax - j; q++) {
+            const double ar = row[2 * q], ai = row[2 * q + 1];
+            const double xr = x[j + q].real(), xi = x[j + q].imag();
+            sr -= ar * xr - ai * xi;
+            si -= ar * xi + ai * xr;
+        }
+        const double den = row[0] * row[0] + row[1] * row[1];
+        x[j] = cplx((sr * row[0] + si * row[1]) / den, (si * row[0] - sr * row[1]) / den);
+    }
+}
+
+double norm2(const std::vector<cplx> &x) {
+    double s = 0;
+    for (const cplx &v : x) s += std::norm(v);
+    return std::sqrt(s);
+}
+
+cplx inner(const std::vector<cplx> &a, const std::vector<cplx> &b) {   // sum conj(a) b
+    cplx s = 0;
+    for (size_t q = 0; q < a.size(); q++) s += std::conj(a[q]) * b[q];
+    return s;
+}
+
+// h = Q e / beta for the API's H_u, H_v arrays
+void magnetic_field(cem_mode2d &m, const Coeffs &c, double w) {
+    const int ny = m.ny, nz = m.nz;
+    std::vector<cplx> hw((size_t)ny * nz);
+    for (int j = 0; j < ny; j++)
+        for (int k = 0; k < nz; k++)
+            hw[(size_t)j * nz + k] = (m.ev[m.at_v(j + 1, k)] - m.ev[m.at_v(j, k)]) * c.ryc[j] -
+                                     (m.eu[m.at_u(j, k + 1)] - m.eu[m.at_u(j, k)]) * c.rzc[k];
+    const double g = 1.0 / (w * CEM_MU0);
+    for (int j = 0; j <= ny; j++)
+        for (int k = 0; k < nz; k++) {
+            const cplx d = (j < ny ? hw[(size_t)j * nz + k] : 0.0) - (j > 0 ? hw[(size_t)(j - 1) * nz + k] : 0.0);
+            m.hu[m.at_v(j, k)] = (-w * c.eps_v[m.at_v(j, k)] * m.ev[m.at_v(j, k)] - g * d * c.ryn[j]) / m.beta;
+        }
+    for (int j = 0; j < ny; j++)
+        for (int k = 0; k <= nz; k++) {
+            const cplx d = (k < nz ? hw[(size_t)j * nz + k] : 0.0) - (k > 0 ? hw[(size_t)j * nz + k - 1] : 0.0);
+            m.hv[m.at_u(j, k)] = (w * c.eps_u[m.at_u(j, k)] * m.eu[m.at_u(j, k)] - g * d * c.rzn[k]) / m.beta;
+        }
 }
 
 }  // namespace
@@ -225,31 +311,44 @@ extern "C" {
 
 cem_mode2d *cem_mode2d_create(int ny, int nz, const double *y, const double *z) {
     cem_mode2d *m = new cem_mode2d;
-    m->ny = ny; m->nz = nz;
+    m->ny = ny;
+    m->nz = nz;
     m->y.assign(y, y + ny + 1);
     m->z.assign(z, z + nz + 1);
-    m->dy.resize(ny); m->dz.resize(nz);
-    m->ddy.assign(ny + 1, 0.0); m->ddz.assign(nz + 1, 0.0);
-    // dual spacings accumulated half-cell by half-cell (reference mode2d.c:64-65)
-    for (int j = 0; j < ny; j++) { m->dy[j] = y[j + 1] - y[j]; m->ddy[j] += m->dy[j] / 2; m->ddy[j + 1] += m->dy[j] / 2; }
-    for (int k = 0; k < nz; k++) { m->dz[k] = z[k + 1] - z[k]; m->ddz[k] += m->dz[k] / 2; m->ddz[k + 1] += m->dz[k] / 2; }
-    const int nu = m->nu(), nv = m->nv(), nn = m->nn();
-    m->er_u.assign(nu, 1.0); m->er_v.assign(nv, 1.0); m->er_w.assign(nn, 1.0);
-    m->sg_u.assign(nu, 0.0); m->sg_v.assign(nv, 0.0); m->sg_w.assign(nn, 0.0);
-    m->pec_u.assign(nu, 0); m->pec_v.assign(nv, 0); m->pec_w.assign(nn, 0);
+    // dual sizes: half of each neighbouring cell
+    m->gy.assign(ny + 1, 0.0);
+    m->gz.assign(nz + 1, 0.0);
+    for (int j = 0; j < ny; j++) {
+        m->hy.push_back(y[j + 1] - y[j]);
+        m->gy[j] += m->hy[j] / 2;
+        m->gy[j + 1] += m->hy[j] / 2;
+    }
+    for (int k = 0; k < nz; k++) {
+        m->hz.push_back(z[k + 1] - z[k]);
+        m->gz[k] += m->hz[k] / 2;
+        m->gz[k + 1] += m->hz[k] / 2;
+    }
+    for (int which = 0; which < 3; which++) {
+        cem_mode2d::Media &md = m->med[which];
+        md.eps.assign(m->count(which), 1.0);
+        md.sig.assign(m->count(which), 0.0);
+        md.metal.assign(m->count(which), 0);
+    }
     const int len[4] = {ny, ny + 1, nz, nz + 1};
     for (int a = 0; a < 4; a++) {
-        m->ps[a].assign(len[a], 0.0);
-        m->pk[a].assign(len[a], 1.0);
-        m->pa[a].assign(len[a], 0.0);
+        m->pml_s[a].assign(len[a], 0.0);
+        m->pml_k[a].assign(len[a], 1.0);
+        m->pml_a[a].assign(len[a], 0.0);
     }
-    // the window's outer boundary is PEC
-    for (int j = 0; j < ny; j++) m->pec_u[m->iu(j, 0)] = m->pec_u[m->iu(j, nz)] = 1;
-    for (int k = 0; k < nz; k++) m->pec_v[m->iv(0, k)] = m->pec_v[m->iv(ny, k)] = 1;
-    for (int j = 0; j <= ny; j++) m->pec_w[m->in(j, 0)] = m->pec_w[m->in(j, nz)] = 1;
-    for (int k = 0; k <= nz; k++) m->pec_w[m->in(0, k)] = m->pec_w[m->in(ny, k)] = 1;
-    m->eu.assign(nu, cplx(0)); m->ev.assign(nv, cplx(0));
-    m->hu.assign(nv, cplx(0)); m->hv.assign(nu, cplx(0));
+    // the window's outer boundary is a perfect conductor
+    for (int j = 0; j < ny; j++) m->med[U].metal[m->at_u(j, 0)] = m->med[U].metal[m->at_u(j, nz)] = 1;
+    for (int k = 0; k < nz; k++) m->med[V].metal[m->at_v(0, k)] = m->med[V].metal[m->at_v(ny, k)] = 1;
+    for (int j = 0; j <= ny; j++) m->med[W].metal[m->at_n(j, 0)] = m->med[W].metal[m->at_n(j, nz)] = 1;
+    for (int k = 0; k <= nz; k++) m->med[W].metal[m->at_n(0, k)] = m->med[W].metal[m->at_n(ny, k)] = 1;
+    m->eu.assign(m->count(U), cplx(0));
+    m->ev.assign(m->count(V), cplx(0));
+    m->hu.assign(m->count(V), cplx(0));
+    m->hv.assign(m->count(U), cplx(0));
     return m;
 }
 
@@ -257,206 +356,214 @@ void cem_mode2d_destroy(cem_mode2d *m) { delete m; }
 
 void cem_mode2d_set_debye(cem_mode2d *m, int npole, const double *f_p, const double *deps_u, const double *deps_v,
                           const double *deps_w) {
-    if (npole > cb2::kMaxPoles) npole = cb2::kMaxPoles;
+    npole = std::min(npole, cb2::kMaxPoles);
     m->npole = npole;
-    std::memcpy(m->pole_f, f_p, npole * sizeof(double));
-    m->dp_u.assign(deps_u, deps_u + (size_t)npole * m->nu());
-    m->dp_v.assign(deps_v, deps_v + (size_t)npole * m->nv());
-    m->dp_w.assign(deps_w, deps_w + (size_t)npole * m->nn());
+    std::copy(f_p, f_p + npole, m->pole_f);
+    const double *src[3] = {deps_u, deps_v, deps_w};
+    for (int which = 0; which < 3; which++)
+        m->med[which].deps.assign(src[which], src[which] + (size_t)npole * m->count(which));
 }
 
 void cem_mode2d_set_media(cem_mode2d *m, const double *epsr_u, const double *epsr_v, const double *epsr_w,
                           const unsigned char *pec_u, const unsigned char *pec_v, const unsigned char *pec_w) {
-    for (int q = 0; q < m->nu(); q++) { m->er_u[q] = epsr_u[q]; m->pec_u[q] |= pec_u[q]; }
-    for (int q = 0; q < m->nv(); q++) { m->er_v[q] = epsr_v[q]; m->pec_v[q] |= pec_v[q]; }
-    for (int q = 0; q < m->nn(); q++) { m->er_w[q] = epsr_w[q]; m->pec_w[q] |= pec_w[q]; }
+    const double *eps[3] = {epsr_u, epsr_v, epsr_w};
+    const unsigned char *pec[3] = {pec_u, pec_v, pec_w};
+    for (int which = 0; which < 3; which++) {
+        cem_mode2d::Media &md = m->med[which];
+        for (int q = 0; q < m->count(which); q++) {
+            md.eps[q] = eps[which][q];
+            md.metal[q] |= pec[which][q];   // the boundary stays metal
+        }
+    }
 }
 
 void cem_mode2d_set_loss(cem_mode2d *m, const double *sig_u, const double *sig_v, const double *sig_w) {
-    m->sg_u.assign(sig_u, sig_u + m->nu());
-    m->sg_v.assign(sig_v, sig_v + m->nv());
-    m->sg_w.assign(sig_w, sig_w + m->nn());
+    const double *sig[3] = {sig_u, sig_v, sig_w};
+    for (int which = 0; which < 3; which++) m->med[which].sig.assign(sig[which], sig[which] + m->count(which));
 }
 
 void cem_mode2d_set_pml(cem_mode2d *m, int which, const double *sigma, const double *kappa, const double *alpha) {
     if (which < 0 || which > 3) return;
-    const int len[4] = {m->ny, m->ny + 1, m->nz, m->nz + 1};
-    m->ps[which].assign(sigma, sigma + len[which]);
-    m->pk[which].assign(kappa, kappa + len[which]);
-    m->pa[which].assign(alpha, alpha + len[which]);
+    const int len = (which < 2 ? m->ny : m->nz) + (which & 1);
+    m->pml_s[which].assign(sigma, sigma + len);
+    m->pml_k[which].assign(kappa, kappa + len);
+    m->pml_a[which].assign(alpha, alpha + len);
 }
 
+// 0: converged; 1: not within maxit iterations (the last iterate is kept); -1: singular
 int cem_mode2d_solve(cem_mode2d *m, double f, double neff_guess, const double *start, int maxit, double tol) {
     const int ny = m->ny, nz = m->nz;
     const double w = 2 * M_PI * f, k0 = w / CEM_C0;
-    const cplx shift = k0 * k0 * neff_guess * neff_guess;
-    const Coef c = make_coef(*m, w);
-    const Unknowns o = make_unknowns(*m);
-    const int n = o.n, bw = 2 * (nz + 2) + 2;
-    Band B(n, bw);
-    std::vector<cplx> x(n), y(n);
-    Work W(*m);
-
-    // assemble the band by probing: unknowns Wc apart never share a band column
-    const int Wc = 2 * bw + 1;
-    for (int col = 0; col < Wc; col++) {
-        std::fill(x.begin(), x.end(), cplx(0));
-        for (int g = col; g < n; g += Wc) x[g] = 1.0;
-        apply_a(*m, c, o, w, x.data(), y.data(), W);
-        for (int g = col; g < n; g += Wc) {
-            const int lo = std::max(g - bw, 0), hi = std::min(g + bw, n - 1);
-            for (int r = lo; r <= hi; r++) B.at(r, g) = y[r];
-        }
-    }
-    // PEC unknowns are pushed far from the shift so they never attract the iteration
-    const double big = -1e6 * (std::abs(shift) + 1.0);
+    const cplx sigma = k0 * k0 * neff_guess * neff_guess;
+    const Coeffs c = coefficients(*m, w);
+    const Numbering o = number_unknowns(*m);
+    const int n = o.n;
+    if (n == 0) return -1;
+    // rows of A - sigma I and the band they need
+    std::vector<Row> rows(n);
+    int half = 0;
     for (int g = 0; g < n; g++) {
-        if (unknown_is_pec(*m, o, g)) B.at(g, g) = big;
-        B.at(g, g) -= shift;
+        const int pt = o.where[g] >> 1, which = o.where[g] & 1;
+        const int j = which == U ? pt / (nz + 1) : pt / nz, k = which == U ? pt % (nz + 1) : pt % nz;
+        rows[g] = assemble_row(*m, c, o, w, which, j, k);
+        rows[g].add(g, -sigma);
+        for (int q = 0; q < rows[g].n; q++) half = std::max(half, std::abs(rows[g].col[q] - g));
     }
-    if (B.factor()) return -1;
+    Band B;
+    B.n = n;
+    B.kl = B.ku = half;
+    B.width = 2 * half + half + 1;
+    B.a.assign((size_t)n * B.width * 2, 0.0);
+    for (int g = 0; g < n; g++)
+        for (int q = 0; q < rows[g].n; q++) {
+            double *e = B.at(g, rows[g].col[q]);
+            e[0] += rows[g].val[q].real();
+            e[1] += rows[g].val[q].imag();
+        }
+    rows.clear();
+    rows.shrink_to_fit();
+    if (!band_factor(B)) return -1;
 
+    // start vector: the given field (API layout: E_u then E_v, complex) or a fixed pseudo-random one
+    std::vector<cplx> x(n), y(n);
     if (start) {
         const cplx *st = reinterpret_cast<const cplx *>(start);
-        for (int g = 0; g < n; g++) x[g] = o.kind[g] == 0 ? st[o.idx[g]] : st[ny * (nz + 1) + o.idx[g]];
-    } else {
-        unsigned lcg = 12345u;
         for (int g = 0; g < n; g++) {
-            lcg = lcg * 1103515245u + 12345u;
-            x[g] = ((lcg >> 8) & 0xffff) / 65536.0 - 0.5;
+            const int pt = o.where[g] >> 1;
+            x[g] = (o.where[g] & 1) ? st[m->count(U) + pt] : st[pt];
+        }
+    } else {
+        uint64_t s = 0x9e3779b97f4a7c15ull;
+        for (int g = 0; g < n; g++) {
+            s ^= s << 13; s ^= s >> 7; s ^= s << 17;   // xorshift64
+            x[g] = (double)(s >> 11) * 0x1.0p-53 - 0.5;
         }
     }
-    cplx lam = shift, lam_old = 0;
-    std::vector<cplx> xo(n, cplx(0));
+    double nx = norm2(x);
+    if (!(nx > 0)) return -1;
+    for (cplx &v : x) v /= nx;
+    cplx lam = sigma, lam_prev = 0;
     int rc = 1;
     for (int it = 0; it < maxit; it++) {
-        double nx2 = 0;
-        for (int g = 0; g < n; g++) nx2 += std::real(x[g] * std::conj(x[g]));
-        const double inv = 1 / std::sqrt(nx2);
-        for (int g = 0; g < n; g++) x[g] *= inv;
-        // converge the phase-aligned vector as well as lambda: the source
-        // profile comes from the vector
-        cplx ph = 0;
-        for (int g = 0; g < n; g++) ph += std::conj(xo[g]) * x[g];
-        double dv = 0;
-        if (std::abs(ph) > 0) {
-            ph = std::conj(ph) / std::abs(ph);
-            for (int g = 0; g < n; g++) {
-                const cplx d = x[g] * ph - xo[g];
-                dv += std::real(d * std::conj(d));
-            }
-        } else {
-            dv = 1;
-        }
-        xo = x;
         y = x;
-        B.solve(y.data());
-        cplx mu = 0;
-        for (int g = 0; g < n; g++) mu += std::conj(x[g]) * y[g];
-        lam = shift + 1.0 / mu;
-        x = y;
-        if (it > 2 && std::abs(lam - lam_old) < tol * std::abs(lam) && std::sqrt(dv) < 1e-10) { rc = 0; break; }
-        lam_old = lam;
+        band_solve(B, y);
+        const cplx mu = inner(x, y);
+        lam = sigma + 1.0 / mu;
+        const double ny2 = norm2(y);
+        for (cplx &v : y) v /= ny2;
+        // change of the iterate with its global phase aligned to the previous one
+        const cplx ph = inner(y, x);
+        const cplx rot = std::abs(ph) > 0 ? ph / std::abs(ph) : cplx(1.0);
+        double d = 0;
+        for (int g = 0; g < n; g++) d += std::norm(y[g] * rot - x[g]);
+        x.swap(y);
+        if (it >= 2 && std::abs(lam - lam_prev) < tol * std::abs(lam) && std::sqrt(d) < 1e-10) {
+            rc = 0;
+            break;
+        }
+        lam_prev = lam;
     }
-    // normalise and make the largest component real
-    double nx2 = 0, amax = 0;
-    cplx ph = 1;
-    for (int g = 0; g < n; g++) {
-        nx2 += std::real(x[g] * std::conj(x[g]));
-        if (std::abs(x[g]) > amax) { amax = std::abs(x[g]); ph = std::conj(x[g]) / amax; }
-    }
-    const double inv = 1 / std::sqrt(nx2);
+    // largest component real and positive; scatter into the API arrays
+    int imax = 0;
+    for (int g = 1; g < n; g++)
+        if (std::abs(x[g]) > std::abs(x[imax])) imax = g;
+    const cplx fix = std::conj(x[imax]) / std::abs(x[imax]);
     std::fill(m->eu.begin(), m->eu.end(), cplx(0));
     std::fill(m->ev.begin(), m->ev.end(), cplx(0));
     for (int g = 0; g < n; g++) {
-        if (unknown_is_pec(*m, o, g)) continue;
-        (o.kind[g] == 0 ? m->eu : m->ev)[o.idx[g]] = x[g] * inv * ph;
+        const int pt = o.where[g] >> 1;
+        ((o.where[g] & 1) ? m->ev : m->eu)[pt] = x[g] * fix;
     }
     cplx bt = std::sqrt(lam);
-    if (std::real(bt) < 0) bt = -bt;
+    if (bt.real() < 0) bt = -bt;
     m->beta = bt;
     m->freq = f;
-    apply_q(*m, c, w, m->eu.data(), m->ev.data(), m->hu.data(), m->hv.data(), W.wk.data());
-    for (cplx &v : m->hu) v /= bt;
-    for (cplx &v : m->hv) v /= bt;
+    magnetic_field(*m, c, w);
     return rc;
 }
 
-double cem_mode2d_beta(const cem_mode2d *m) { return std::real(m->beta); }
-double cem_mode2d_alpha(const cem_mode2d *m) { return -std::imag(m->beta); }
+double cem_mode2d_beta(const cem_mode2d *m) { return m->beta.real(); }
+double cem_mode2d_alpha(const cem_mode2d *m) { return -m->beta.imag(); }
 const double *cem_mode2d_eu(const cem_mode2d *m) { return reinterpret_cast<const double *>(m->eu.data()); }
 const double *cem_mode2d_ev(const cem_mode2d *m) { return reinterpret_cast<const double *>(m->ev.data()); }
 const double *cem_mode2d_hu(const cem_mode2d *m) { return reinterpret_cast<const double *>(m->hu.data()); }
 const double *cem_mode2d_hv(const cem_mode2d *m) { return reinterpret_cast<const double *>(m->hv.data()); }
 
-// Real part of the complex power 1/2 sum (Eu Hv* - Ev Hu*) dA.
+// Real part of the complex power flow 1/2 integral (E_t x H_t*) . x dA.
 double cem_mode2d_power(const cem_mode2d *m) {
-    const int ny = m->ny, nz = m->nz;
-    cplx P = 0;
-    for (int j = 0; j < ny; j++)
-        for (int k = 0; k <= nz; k++) P += m->eu[m->iu(j, k)] * std::conj(m->hv[m->iu(j, k)]) * m->dy[j] * m->ddz[k];
-    for (int j = 0; j <= ny; j++)
-        for (int k = 0; k < nz; k++) P -= m->ev[m->iv(j, k)] * std::conj(m->hu[m->iv(j, k)]) * m->ddy[j] * m->dz[k];
-    return 0.5 * std::real(P);
+    double p = 0;
+    for (int j = 0; j < m->ny; j++)
+        for (int k = 0; k <= m->nz; k++) {
+            const int q = m->at_u(j, k);
+            p += (m->eu[q] * std::conj(m->hv[q])).real() * m->hy[j] * m->gz[k];
+        }
+    for (int j = 0; j <= m->ny; j++)
+        for (int k = 0; k < m->nz; k++) {
+            const int q = m->at_v(j, k);
+            p -= (m->ev[q] * std::conj(m->hu[q])).real() * m->gy[j] * m->hz[k];
+        }
+    return 0.5 * p;
 }
 
-// V = -sum Ez dz on node column j0, k0..k1; I = circulation of H around the
-// dual rectangle (ja+1/2..jb+1/2) x (ka+1/2..kb+1/2), current in +x.
+// V = -integral of Ez from k0 to k1 on node column j0; I = circulation of H
+// (+x current) around the dual rectangle (ja+1/2 .. jb+1/2) x (ka+1/2 .. kb+1/2).
 void cem_mode2d_vi(const cem_mode2d *m, int j0, int k0, int k1, int ja, int jb, int ka, int kb, double *V,
                    double *Iout) {
-    cplx v = 0, c = 0;
-    for (int k = k0; k < k1; k++) v -= m->ev[m->iv(j0, k)] * m->dz[k];
-    for (int j = ja + 1; j <= jb; j++) c += (m->hu[m->iv(j, ka)] - m->hu[m->iv(j, kb)]) * m->ddy[j];
-    for (int k = ka + 1; k <= kb; k++) c += (m->hv[m->iu(jb, k)] - m->hv[m->iu(ja, k)]) * m->ddz[k];
-    V[0] = std::real(v); V[1] = std::imag(v);
-    Iout[0] = std::real(c); Iout[1] = std::imag(c);
+    cplx v = 0, i = 0;
+    for (int k = k0; k < k1; k++) v -= m->ev[m->at_v(j0, k)] * m->hz[k];
+    for (int j = ja + 1; j <= jb; j++) i += (m->hu[m->at_v(j, ka)] - m->hu[m->at_v(j, kb)]) * m->gy[j];
+    for (int k = ka + 1; k <= kb; k++) i += (m->hv[m->at_u(jb, k)] - m->hv[m->at_u(ja, k)]) * m->gz[k];
+    V[0] = v.real();
+    V[1] = v.imag();
+    Iout[0] = i.real();
+    Iout[1] = i.imag();
 }
 
-// Conductor attenuation by perturbation: P_loss = Rs/2 sum |n x H|^2 dl over
-// metal surfaces facing a field cell, alpha_c = P_loss / (2 P).
-// (reference mode2d.c:444-498)
+// Conductor attenuation of the last mode by perturbation (the reference's
+// definition, solver/src/mode2d.c:444-498): every metal segment of the
+// section that faces a field cell outside the PML loses Rs/2 |J|^2 per unit
+// length, with the transverse surface current |H_w| = |curl_w E| / (w mu0) on
+// the segment and the longitudinal one from the transverse H at its two end
+// points (half a segment each); alpha_c = P_loss / (2 P).
 double cem_mode2d_conductor_alpha(const cem_mode2d *m, double Rs) {
     const int ny = m->ny, nz = m->nz;
-    auto solid = [&](int j, int k) {
-        return j >= 0 && j < ny && k >= 0 && k < nz && m->pec_u[m->iu(j, k)] && m->pec_u[m->iu(j, k + 1)] &&
-               m->pec_v[m->iv(j, k)] && m->pec_v[m->iv(j + 1, k)];
+    const cem_mode2d::Media &mu = m->med[U], &mv = m->med[V];
+    auto solid = [&](int j, int k) {   // cell (j, k) enclosed by metal on all four sides
+        return j >= 0 && j < ny && k >= 0 && k < nz && mu.metal[m->at_u(j, k)] && mu.metal[m->at_u(j, k + 1)] &&
+               mv.metal[m->at_v(j, k)] && mv.metal[m->at_v(j + 1, k)];
     };
-    const double w = 2 * M_PI * m->freq;
-    auto curl_w = [&](int j, int k) {
-        return (m->ev[m->iv(j + 1, k)] - m->ev[m->iv(j, k)]) / m->dy[j] - (m->eu[m->iu(j, k + 1)] - m->eu[m->iu(j, k)]) / m->dz[k];
+    const double wm = 2 * M_PI * m->freq * CEM_MU0;
+    auto hw_mag = [&](int j, int k) {
+        const cplx cw = (m->ev[m->at_v(j + 1, k)] - m->ev[m->at_v(j, k)]) / m->hy[j] -
+                        (m->eu[m->at_u(j, k + 1)] - m->eu[m->at_u(j, k)]) / m->hz[k];
+        return std::abs(cw) / wm;
     };
     double loss = 0;
-    for (int j = 0; j < ny; j++)
+    for (int j = 0; j < ny; j++)   // y-directed segments (E_u points on metal)
         for (int k = 0; k <= nz; k++) {
-            if (!m->pec_u[m->iu(j, k)]) continue;
-            if (m->ps[0][j] > 0 || m->ps[3][k] > 0) continue;   // metal inside the PML is not the device
-            for (int side = 0; side < 2; side++) {
-                const int kc = side == 0 ? k : k - 1;
+            if (!mu.metal[m->at_u(j, k)] || m->pml_s[0][j] > 0 || m->pml_s[3][k] > 0) continue;
+            for (int kc : {k, k - 1}) {
                 if (kc < 0 || kc >= nz || solid(j, kc)) continue;
-                const double hw = std::abs(curl_w(j, kc)) / (w * CEM_MU0);
-                loss += 0.5 * Rs * hw * hw * m->dy[j];
-                for (int e = 0; e < 2; e++) {
-                    const int jn = j + e;
-                    if (m->pec_v[m->iv(jn, kc)]) continue;
-                    const double hu = std::abs(m->hu[m->iv(jn, kc)]);
-                    loss += 0.5 * Rs * hu * hu * 0.5 * m->dy[j];
+                const double h = hw_mag(j, kc);
+                loss += 0.5 * Rs * h * h * m->hy[j];
+                for (int jn : {j, j + 1}) {
+                    if (mv.metal[m->at_v(jn, kc)]) continue;
+                    const double t = std::abs(m->hu[m->at_v(jn, kc)]);
+                    loss += 0.25 * Rs * t * t * m->hy[j];
                 }
             }
         }
-    for (int j = 0; j <= ny; j++)
+    for (int j = 0; j <= ny; j++)   // z-directed segments (E_v points on metal)
         for (int k = 0; k < nz; k++) {
-            if (!m->pec_v[m->iv(j, k)]) continue;
-            if (m->ps[1][j] > 0 || m->ps[2][k] > 0) continue;
-            for (int side = 0; side < 2; side++) {
-                const int jc = side == 0 ? j : j - 1;
+            if (!mv.metal[m->at_v(j, k)] || m->pml_s[1][j] > 0 || m->pml_s[2][k] > 0) continue;
+            for (int jc : {j, j - 1}) {
                 if (jc < 0 || jc >= ny || solid(jc, k)) continue;
-                const double hw = std::abs(curl_w(jc, k)) / (w * CEM_MU0);
-                loss += 0.5 * Rs * hw * hw * m->dz[k];
-                for (int e = 0; e < 2; e++) {
-                    const int kn = k + e;
-                    if (m->pec_u[m->iu(jc, kn)]) continue;
-                    const double hv = std::abs(m->hv[m->iu(jc, kn)]);
-                    loss += 0.5 * Rs * hv * hv * 0.5 * m->dz[k];
+                const double h = hw_mag(jc, k);
+                loss += 0.5 * Rs * h * h * m->hz[k];
+                for (int kn : {k, k + 1}) {
+                    if (mu.metal[m->at_u(jc, kn)]) continue;
+                    const double t = std::abs(m->hv[m->at_u(jc, kn)]);
+                    loss += 0.25 * Rs * t * t * m->hz[k];
                 }
             }
         }

@@ -24,11 +24,13 @@ def plan_digest(plan: dict) -> dict:
     return out
 
 
-def cmp_plans(x, y, path=""):
+def cmp_plans(x, y, path="", skip=()):
+    """Paths where two plans differ (bit for bit); keys in `skip` are left out."""
     bad = []
     if isinstance(x, dict):
         for k in x:
-            bad += cmp_plans(x[k], y[k], f"{path}.{k}")
+            if k not in skip:
+                bad += cmp_plans(x[k], y[k], f"{path}.{k}")
     elif isinstance(x, list):
         if len(x) != len(y):
             return [path]
@@ -52,3 +54,14 @@ def db_deg(s_test, s_ref):
     d_db = np.abs(20 * np.log10(np.abs(s_test)) - 20 * np.log10(np.abs(s_ref)))
     d_deg = np.abs(np.angle(s_test / s_ref, deg=True))
     return d_db, d_deg
+
+
+def mode_source_diff(a: dict, b: dict) -> float:
+    """Largest difference of two mode-source tables (global E index -> weight,
+    missing entries zero), relative to the largest weight of `a`."""
+    wa = dict(zip(a["idx"].tolist(), a["w"].tolist()))
+    wb = dict(zip(b["idx"].tolist(), b["w"].tolist()))
+    scale = max((abs(v) for v in wa.values()), default=0.0)
+    if scale == 0:
+        return 0.0 if not wb else float("inf")
+    return max(abs(wa.get(k, 0.0) - wb.get(k, 0.0)) for k in set(wa) | set(wb)) / scale
