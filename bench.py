@@ -51,7 +51,7 @@ def _workloads() -> dict:
                         "non-uniform mesh 1500x1014x64",
                    board=dict(seed=2026, cells=96e6, ports="mode", nf=201, fmax=20e9, steps=30000,
                               target=(1500, 1000, 64)),
-                   ref_chunk=1, e2e_steps=4000)
+                   ref_chunk=1, e2e_steps=10000)
     return w
 
 

@@ -34,6 +34,7 @@
 #include <memory>
 #include <thread>
 #include <map>
+#include <atomic>
 #include <chrono>
 #include <mutex>
 #include <string>
@@ -1858,7 +1859,7 @@ struct TableBuilder {
     }
 };
 
-// Material tables of the three E components, one thread each. Entries are
+// Material tables of the three E components. Entries are
 // numbered in order of first appearance along (i, j, k); a point whose
 // coefficient row equals the previous point's takes its entry without a
 // lookup. The lumped-source and Debye edges of a component are walked as
@@ -1889,6 +1890,16 @@ bool build_tables(cem_sim *s, Device &D) {
             wsrc[mp.src_comp[e] - 1][mp.src_idx[e] % s->si] += (float)mp.src_w[e];
     }
     const int *n = s->n;
+    // Each component's node planes are cut into slabs that build tables of
+    // their own in parallel; the slabs' tables then merge in slab order, so
+    // entries keep their numbering by first appearance along (i, j, k), and the
+    // slabs' indices are renumbered.
+    struct Slab {
+        std::unique_ptr<TableBuilder> tb;
+        int box_lo[3], box_hi[3];
+        bool overflow = false;
+        int i0 = 0, i1 = 0;
+    };
     struct Built {
         TableBuilder tb;
         std::vector<unsigned short> mat;
@@ -1897,20 +1908,43 @@ bool build_tables(cem_sim *s, Device &D) {
         explicit Built(int nf) : tb(nf) {}
     };
     std::vector<std::unique_ptr<Built>> out;
-    for (int c = 0; c < 3; c++) out.emplace_back(new Built(nfields));
-    auto build = [&](int c) {
-        Built &b = *out[c];
-        TableBuilder &tb = b.tb;
-        std::vector<unsigned short> &mat = b.mat;
-        mat.assign(D.Np, 0);
+    for (int c = 0; c < 3; c++) {
+        out.emplace_back(new Built(nfields));
+        out[c]->mat.assign(D.Np, 0);
+    }
+    const int nthreads = (int)std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
+    const int nslab = std::max(1, std::min(n[0] + 1, nthreads));
+    std::vector<Slab> slabs(3 * (size_t)nslab);
+    auto run_parallel = [&](int ntask, auto f) {
+        std::atomic<int> next{0};
+        std::vector<std::thread> th;
+        for (int w = 0; w < std::min(ntask, nthreads); w++)
+            th.emplace_back([&] {
+                for (int t = next++; t < ntask; t = next++) f(t);
+            });
+        for (auto &x : th) x.join();
+    };
+    auto build = [&](int t) {
+        const int c = t / nslab, sl = t % nslab;
+        Slab &b = slabs[t];
+        b.tb.reset(new TableBuilder(nfields));
+        TableBuilder &tb = *b.tb;
+        std::vector<unsigned short> &mat = out[c]->mat;
+        b.i0 = (int)((long long)(n[0] + 1) * sl / nslab);
+        b.i1 = (int)((long long)(n[0] + 1) * (sl + 1) / nslab);
         std::vector<float> row(nfields), prev(nfields);
         unsigned char prev_flag = 0;
         int prev_id = -1;
         for (int a = 0; a < 3; a++) { b.box_lo[a] = n[a]; b.box_hi[a] = -1; }
         const auto &sc = src[c];
         const auto &dc = disp[c];
-        size_t ss = 0, ds = 0;
-        for (int i = 0; i <= n[0]; i++)
+        const size_t q0 = idx3(s, b.i0, 0, 0);
+        auto first_at = [q0](const auto &v) {
+            return (size_t)(std::lower_bound(v.begin(), v.end(), q0, [](const auto &x, size_t q) { return x.first < q; }) -
+                            v.begin());
+        };
+        size_t ss = first_at(sc), ds = first_at(dc);
+        for (int i = b.i0; i < b.i1; i++)
             for (int j = 0; j <= n[1]; j++)
                 for (int k = 0; k <= n[2]; k++) {
                     const int ijk[3] = {i, j, k};
@@ -1954,11 +1988,36 @@ bool build_tables(cem_sim *s, Device &D) {
                     mat[(size_t)i * D.g.si + (size_t)j * D.g.sj + k] = (unsigned short)id;
                 }
     };
-    {
-        std::vector<std::thread> th;
-        for (int c = 0; c < 3; c++) th.emplace_back(build, c);
-        for (auto &x : th) x.join();
+    run_parallel(3 * nslab, build);
+    // merge: the slabs' entries join each component's table in slab order
+    std::vector<std::vector<int>> remap(slabs.size());
+    for (int c = 0; c < 3; c++) {
+        Built &b = *out[c];
+        for (int a = 0; a < 3; a++) { b.box_lo[a] = n[a]; b.box_hi[a] = -1; }
+        for (int sl = 0; sl < nslab && !b.overflow; sl++) {
+            Slab &x = slabs[(size_t)c * nslab + sl];
+            if (x.overflow) { b.overflow = true; break; }
+            const TableBuilder &t = *x.tb;
+            std::vector<int> &rm = remap[(size_t)c * nslab + sl];
+            rm.resize(t.flags.size());
+            for (size_t l = 0; l < t.flags.size(); l++) {
+                rm[l] = b.tb.add(&t.rows[l * nfields], t.flags[l], t.cb64[l]);
+                if (rm[l] > 65535) { b.overflow = true; break; }
+            }
+            for (int a = 0; a < 3; a++) {
+                b.box_lo[a] = std::min(b.box_lo[a], x.box_lo[a]);
+                b.box_hi[a] = std::max(b.box_hi[a], x.box_hi[a]);
+            }
+        }
     }
+    run_parallel(3 * nslab, [&](int t) {
+        const int c = t / nslab;
+        if (out[c]->overflow) return;
+        const Slab &x = slabs[t];
+        const std::vector<int> &rm = remap[t];
+        unsigned short *m = out[c]->mat.data();
+        for (size_t q = (size_t)x.i0 * D.g.si; q < (size_t)x.i1 * D.g.si; q++) m[q] = (unsigned short)rm[m[q]];
+    });
     for (int c = 0; c < 3; c++) {
         Built &b = *out[c];
         if (b.overflow) {

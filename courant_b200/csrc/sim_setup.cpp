@@ -12,6 +12,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
+#include <thread>
 
 #ifndef M_PI
 #define M_PI 3.14159265358979323846
@@ -483,6 +485,34 @@ namespace {
 // CPML grading on one axis: polynomial (m = 3) sigma and kappa, linear alpha,
 // recursive-convolution b/c at nodes (E) and cells (H), and the kappa-scaled
 // inverse spacings used by the bulk update. (reference sim.c:369-425)
+// host threads for the whole-grid loops of finalize
+int plane_threads() {
+    const unsigned h = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(h ? h : 1u, 32u));
+}
+
+// f(t) for t in [0, n) on up to plane_threads() threads
+template <class F>
+void parallel_tasks(int n, F f) {
+    const int nt = std::min(n, plane_threads());
+    std::atomic<int> next{0};
+    std::vector<std::thread> th;
+    for (int w = 0; w < nt; w++)
+        th.emplace_back([&] {
+            for (int t = next++; t < n; t = next++) f(t);
+        });
+    for (auto &x : th) x.join();
+}
+
+// f(i0, i1) over slabs of the node planes [0, n)
+template <class F>
+void parallel_planes(int n, F f) {
+    const int ns = std::max(1, std::min(n, 4 * plane_threads()));
+    parallel_tasks(ns, [&](int sl) {
+        f((int)((long long)n * sl / ns), (int)((long long)n * (sl + 1) / ns));
+    });
+}
+
 void setup_pml_axis(cem_sim *s, int a) {
     const int n = s->n[a];
     s->ide[a].assign(n + 1, 0.0);
@@ -562,25 +592,28 @@ int cem_finalize(cem_sim *s, double cfl) {
 
         const int nx = s->n[0], ny = s->n[1], nz = s->n[2];
         // per-edge coefficients, lossy dielectric by the semi-implicit average
-        // (reference sim.c:450-465)
+        // (reference sim.c:450-465); every edge on its own, node planes in parallel
         for (int c = 0; c < 3; c++) {
             s->ca[c].assign(s->N, 0.0);
             s->cb[c].assign(s->N, 0.0);
-            for (int i = 0; i <= nx; i++)
-                for (int j = 0; j <= ny; j++)
-                    for (int k = 0; k <= nz; k++) {
-                        const int ijk[3] = {i, j, k};
-                        if (ijk[c] >= s->n[c]) continue;
-                        const size_t q = idx3(s, i, j, k);
-                        double er, sg;
-                        int pec;
-                        edge_material(s, c, i, j, k, &er, &sg, &pec);
-                        if (pec || s->edge_pec[c][q]) continue;   // ca = cb = 0
-                        const double eps = er * CEM_EPS0, h = sg * s->dt / (2 * eps);
-                        s->ca[c][q] = (1 - h) / (1 + h);
-                        s->cb[c][q] = (s->dt / eps) / (1 + h);
-                    }
         }
+        parallel_planes(nx + 1, [&](int i0, int i1) {
+            for (int c = 0; c < 3; c++)
+                for (int i = i0; i < i1; i++)
+                    for (int j = 0; j <= ny; j++)
+                        for (int k = 0; k <= nz; k++) {
+                            const int ijk[3] = {i, j, k};
+                            if (ijk[c] >= s->n[c]) continue;
+                            const size_t q = idx3(s, i, j, k);
+                            double er, sg;
+                            int pec;
+                            edge_material(s, c, i, j, k, &er, &sg, &pec);
+                            if (pec || s->edge_pec[c][q]) continue;   // ca = cb = 0
+                            const double eps = er * CEM_EPS0, h = sg * s->dt / (2 * eps);
+                            s->ca[c][q] = (1 - h) / (1 + h);
+                            s->cb[c][q] = (s->dt / eps) / (1 + h);
+                        }
+        });
 
         // lumped ports: resistive voltage source spread over the column's edges
         // (reference sim.c:468-492)
@@ -618,13 +651,23 @@ int cem_finalize(cem_sim *s, double cfl) {
         // Debye edges: eps -> eps_inf eps0 + sum beta_p / 2 in ca/cb, ADE tables.
         // Lumped-port edges keep their own coefficients. (reference sim.c:501-549)
         if (s->npole) {
-            double dep[kMaxPoles];
-            std::vector<int> comp;
-            std::vector<size_t> idx;
-            std::vector<double> cbv;
-            std::vector<std::vector<double>> beta(s->npole);
-            for (int c = 0; c < 3; c++)
-                for (int i = 0; i <= nx; i++)
+            // each (component, slab of node planes) lists its Debye edges on its own;
+            // the lists join in component, then plane order: the reference's edge order
+            struct Part {
+                std::vector<int> comp;
+                std::vector<size_t> idx;
+                std::vector<double> cbv;
+                std::vector<std::vector<double>> beta;
+            };
+            const int nslab = std::max(1, std::min(nx + 1, 4 * plane_threads()));
+            std::vector<Part> parts(3 * (size_t)nslab);
+            parallel_tasks((int)parts.size(), [&](int t) {
+                const int c = t / nslab, sl = t % nslab;
+                const int i0 = (int)((long long)(nx + 1) * sl / nslab), i1 = (int)((long long)(nx + 1) * (sl + 1) / nslab);
+                Part &pt = parts[t];
+                pt.beta.resize(s->npole);
+                double dep[kMaxPoles];
+                for (int i = i0; i < i1; i++)
                     for (int j = 0; j <= ny; j++)
                         for (int k = 0; k <= nz; k++) {
                             const int ijk[3] = {i, j, k};
@@ -639,23 +682,36 @@ int cem_finalize(cem_sim *s, double cfl) {
                             for (int p = 0; p < s->npole; p++) {
                                 const double tau = 1.0 / (2 * M_PI * s->pole_f[p]);
                                 const double bt = CEM_EPS0 * dep[p] * s->dt / (tau * (1 + s->dt / (2 * tau)));
-                                beta[p].push_back(bt);
+                                pt.beta[p].push_back(bt);
                                 einst += 0.5 * bt;
                             }
                             const double h = sg * s->dt / (2 * einst);
                             s->ca[c][q] = (1 - h) / (1 + h);
                             s->cb[c][q] = (s->dt / einst) / (1 + h);
-                            comp.push_back(c);
-                            idx.push_back(q);
-                            cbv.push_back(s->cb[c][q]);
+                            pt.comp.push_back(c);
+                            pt.idx.push_back(q);
+                            pt.cbv.push_back(s->cb[c][q]);
                         }
-            s->ndisp = (int)idx.size();
-            s->d_comp = std::move(comp);
-            s->d_idx = std::move(idx);
-            s->d_cb = std::move(cbv);
+            });
+            size_t total = 0;
+            for (const Part &pt : parts) total += pt.idx.size();
+            s->ndisp = (int)total;
+            s->d_comp.clear();
+            s->d_idx.clear();
+            s->d_cb.clear();
+            s->d_comp.reserve(total);
+            s->d_idx.reserve(total);
+            s->d_cb.reserve(total);
             s->d_beta.assign((size_t)s->npole * s->ndisp, 0.0);
-            for (int p = 0; p < s->npole; p++)
-                std::copy(beta[p].begin(), beta[p].end(), s->d_beta.begin() + (size_t)p * s->ndisp);
+            size_t at = 0;
+            for (const Part &pt : parts) {
+                s->d_comp.insert(s->d_comp.end(), pt.comp.begin(), pt.comp.end());
+                s->d_idx.insert(s->d_idx.end(), pt.idx.begin(), pt.idx.end());
+                s->d_cb.insert(s->d_cb.end(), pt.cbv.begin(), pt.cbv.end());
+                for (int p = 0; p < s->npole; p++)
+                    std::copy(pt.beta[p].begin(), pt.beta[p].end(), s->d_beta.begin() + (size_t)p * s->ndisp + at);
+                at += pt.idx.size();
+            }
             for (int p = 0; p < s->npole; p++) {
                 const double tau = 1.0 / (2 * M_PI * s->pole_f[p]);
                 s->d_k[p] = (1 - s->dt / (2 * tau)) / (1 + s->dt / (2 * tau));
