@@ -52,6 +52,9 @@ def _workloads() -> dict:
                    board=dict(seed=2026, cells=96e6, ports="mode", nf=201, fmax=20e9, steps=30000,
                               target=(1500, 1000, 64)),
                    ref_chunk=1, e2e_steps=10000)
+    # the same generator at 8 M cells: a case of the large board's kernels small enough to profile
+    w["c3s"] = dict(desc="seeded 4-layer board as c3 at 8 M cells", board=dict(w["c3"]["board"], cells=8e6, target=None,
+                                                                               steps=30000), ref_chunk=5, e2e_steps=10000)
     return w
 
 

@@ -404,6 +404,23 @@ __device__ __forceinline__ int jbox_volume(const StepArgs &a) {
     return a.jbox[C][3] * a.jbox[C][4] * a.jbox[C][5];
 }
 
+// Element of pole p's current at offset o of a Debye box of `vol` points
+// with P poles. CB2_JLAYOUT 0: one box-sized plane per pole; 1: the P poles
+// of each four-point group side by side (one thread's currents are P
+// consecutive float4).
+#ifndef CB2_JLAYOUT
+#define CB2_JLAYOUT 0
+#endif
+__host__ __device__ __forceinline__ size_t jaddr(int P, size_t vol, int p, size_t o) {
+#if CB2_JLAYOUT
+    (void)vol;
+    return ((o >> 2) * (size_t)P + (size_t)p) * 4 + (o & 3);
+#else
+    (void)P;
+    return (size_t)p * vol + o;
+#endif
+}
+
 // E value with auxiliaries and Debye currents read and written in place
 // (fused step; p1, p2: CPML planes as for h_comp; mi: table index)
 template <int C, int P>
@@ -422,7 +439,7 @@ __device__ __forceinline__ float e_comp(const StepArgs &a, int i, int j, int k, 
     if (disp) {
         jo = jbox_at<C>(a, i, j, k);
 #pragma unroll
-        for (int p = 0; p < P; p++) jsum = debye_term(a, p, a.J[C][p * jvol + jo], jsum);
+        for (int p = 0; p < P; p++) jsum = debye_term(a, p, a.J[C][jaddr(P, jvol, p, jo)], jsum);
     }
     const float r = e_value<C>(a, t, i, j, k, sv, e, d1, d2, c1, c2, p1 >= 0, p2 >= 0, s1, s2, jsum);
     if (p1 >= 0) a.psiE[C][0][x1] = s1;
@@ -431,7 +448,7 @@ __device__ __forceinline__ float e_comp(const StepArgs &a, int i, int j, int k, 
         const float de = __fsub_rn(r, e);
 #pragma unroll
         for (int p = 0; p < P; p++) {
-            float *jp = a.J[C] + p * jvol + jo;
+            float *jp = a.J[C] + jaddr(P, jvol, p, jo);
             *jp = debye_next(a, p, beta_at<C>(a, mi, p), de, *jp);
         }
     }
@@ -730,7 +747,7 @@ __device__ __forceinline__ void e_points(const StepArgs &a, int i, int j, int k4
     if (P > 0 && box) {
 #pragma unroll
         for (int p = 0; p < (P > 0 ? P : 1); p++) {
-            const float4 jp = ld4(a.J[C] + p * jvol + jo4);
+            const float4 jp = ld4(a.J[C] + jaddr(P, jvol, p, jo4));
 #pragma unroll
             for (int e = 0; e < 4; e++) jsum[e] = debye_term(a, p, lane4(jp, e), jsum[e]);
         }
@@ -763,7 +780,7 @@ __device__ __forceinline__ void e_points(const StepArgs &a, int i, int j, int k4
         }
 #pragma unroll
         for (int p = 0; p < (P > 0 ? P : 1); p++) {
-            float *jp = a.J[C] + p * jvol + jo4;
+            float *jp = a.J[C] + jaddr(P, jvol, p, jo4);
             float4 jv = ld4(jp);
 #pragma unroll
             for (int e = 0; e < 4; e++)
@@ -931,7 +948,7 @@ __device__ __forceinline__ void e_debye(const StepArgs &a, int i, const RowPos &
         if (A2 != 2) h1m = ldg4(H1 + q - stride_of<A2>(a));
     }
 #pragma unroll
-    for (int pp = 0; pp < P; pp++) J[pp] = jo4 >= 0 ? ld4(Jc + pp * jvol + jo4) : z4;
+    for (int pp = 0; pp < P; pp++) J[pp] = jo4 >= 0 ? ld4(Jc + jaddr(P, jvol, pp, jo4)) : z4;
     const bool first = (threadIdx.x & 31) == 0 || k4 == p.ks;
     if (A1 == 2) h2m = prev_k(h2, H2 + q, row && k4 > 0, first);
     if (A2 == 2) h1m = prev_k(h1, H1 + q, row && k4 > 0, first);
@@ -975,7 +992,7 @@ __device__ __forceinline__ void e_debye(const StepArgs &a, int i, const RowPos &
         for (int pp = 0; pp < P; pp++) set4(J[pp], e, debye_next(a, pp, b[pp], de[e], lane4(J[pp], e)));
     }
 #pragma unroll
-    for (int pp = 0; pp < P; pp++) st4(Jc + pp * jvol + jo4, J[pp]);
+    for (int pp = 0; pp < P; pp++) st4(Jc + jaddr(P, jvol, pp, jo4), J[pp]);
 }
 
 // H over node planes [i0, i0 + gridDim.y) (cem_mt_H and the unfused step)
@@ -2727,7 +2744,7 @@ bool upload_group(cem_sim *s, unsigned g, bool from_host) {
                 const size_t q = s->d_idx[e];
                 const int i = (int)(q / s->si), j = (int)((q % s->si) / s->sj), k = (int)(q % s->sj);
                 const size_t o = ((size_t)(i - bx[0]) * bx[4] + (j - bx[1])) * bx[5] + (k - bx[2]);
-                for (int p = 0; p < s->npole; p++) box[p * vol + o] = (float)s->d_J[(size_t)p * s->ndisp + e];
+                for (int p = 0; p < s->npole; p++) box[jaddr(s->npole, vol, p, o)] = (float)s->d_J[(size_t)p * s->ndisp + e];
             }
             if (!h2d(s, D.J[c].p, box.data(), box.size() * 4)) return false;
         }
@@ -2784,7 +2801,7 @@ bool download_group(cem_sim *s, unsigned g) {
                 const size_t q = s->d_idx[e];
                 const int i = (int)(q / s->si), j = (int)((q % s->si) / s->sj), k = (int)(q % s->sj);
                 const size_t o = ((size_t)(i - bx[0]) * bx[4] + (j - bx[1])) * bx[5] + (k - bx[2]);
-                for (int p = 0; p < s->npole; p++) s->d_J[(size_t)p * s->ndisp + e] = box[p * vol + o];
+                for (int p = 0; p < s->npole; p++) s->d_J[(size_t)p * s->ndisp + e] = box[jaddr(s->npole, vol, p, o)];
             }
         }
     }
