@@ -17,6 +17,8 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIBDIR = PKG / "lib"
 LIB = LIBDIR / "libcourant_b200.so"
+NAPI = PKG / "napi"
+SHIM_LIB = LIBDIR / "libcourant_napi_core.so"   # the Node shim's call translation behind a C ABI (node-free)
 INCLUDE = PKG.parent / "include"
 VERSION = "20261017.0-b200"
 
@@ -43,8 +45,15 @@ def sources() -> list[Path]:
     return sorted(CSRC.glob("*.cpp")) + sorted(CSRC.glob("*.cu"))
 
 
+def shim_sources() -> list[Path]:
+    return [NAPI / n for n in ("arena.cpp", "shim.cpp", "shim_exports.cpp", "shim_capi.cpp")]
+
+
 def needs_build() -> bool:
-    if not LIB.exists():
+    if not LIB.exists() or not SHIM_LIB.exists():
+        return True
+    ts = SHIM_LIB.stat().st_mtime
+    if any(p.stat().st_mtime > ts for p in shim_sources() + list(NAPI.glob("*.hpp")) + list(NAPI.glob("*.inc"))):
         return True
     t = LIB.stat().st_mtime
     deps = sources() + [CSRC / "exports.map"] + list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.cuh")) + [INCLUDE / "courant.h", Path(__file__)]
@@ -71,6 +80,11 @@ def build(force: bool = False, verbose: bool = False) -> Path:
               "-lpthread", "-Wl,--exclude-libs,ALL", "-Wl,-Bsymbolic",
               f"-Wl,--version-script={CSRC / 'exports.map'}"], log)
         os.replace(tmp, LIB)
+        # the Node shim's translation layer (the N-API module itself builds with node-gyp: napi/binding.gyp)
+        tmp = SHIM_LIB.with_suffix(".so.tmp")
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-fvisibility=hidden", "-Wall", "-Wextra",
+              *[str(p) for p in shim_sources()], "-ldl", "-o", str(tmp)], log)
+        os.replace(tmp, SHIM_LIB)
     if verbose:
         print((obj / "build.log").read_text())
     return LIB
