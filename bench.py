@@ -53,8 +53,9 @@ def _workloads() -> dict:
                               target=(1500, 1000, 64)),
                    ref_chunk=1, e2e_steps=10000)
     # the same generator at 8 M cells: a case of the large board's kernels small enough to profile
-    w["c3s"] = dict(desc="seeded 4-layer board as c3 at 8 M cells", board=dict(w["c3"]["board"], cells=8e6, target=None,
-                                                                               steps=30000), ref_chunk=5, e2e_steps=10000)
+    w["c3s"] = dict(desc="seeded 4-layer board as c3 at 500x330x64 cells",
+                    board=dict(w["c3"]["board"], cells=10.6e6, target=(500, 330, 64), steps=30000), ref_chunk=5,
+                    e2e_steps=10000)
     return w
 
 

@@ -484,10 +484,11 @@ class Sim:
         return {k: {"ms": float(ms[q]), "launches": int(cnt[q])} for q, k in enumerate(names)}
 
     def sizes(self) -> dict:
-        out = (C.c_longlong * 13)()
-        self._check(self.c.ex.cemx_sizes(self.h, out, 13), "sizes")
+        out = (C.c_longlong * 19)()
+        self._check(self.c.ex.cemx_sizes(self.h, out, 19), "sizes")
         keys = ["cells", "points", "psiE", "psiH", "ndisp", "npole", "nsibc", "sibc_terms", "tab_x", "tab_y", "tab_z",
-                "device_bytes", "launches_per_step"]
+                "device_bytes", "launches_per_step", "h_fast_pts", "h_general_pts", "e_fast_pts", "e_general_pts",
+                "e_debye_pts", "jbox_points"]
         return dict(zip(keys, [int(v) for v in out]))
 
     def useFused(self, on: bool = True) -> bool:

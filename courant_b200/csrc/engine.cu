@@ -2285,8 +2285,10 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
         const int *bx = D.jbox[c];
         if (bx[3] * bx[4] * bx[5] > 0 && bx[0] < p1 && bx[0] + bx[3] > p0) boxes.push_back(bx);
     }
-    std::vector<int> kb{0, g.sj}, jb{0, rows};
-    auto kcut = [&](int c) { if (c > 0 && c < g.sj) kb.push_back(c); };
+    // k groups up to the last node (nz); the row padding beyond is never touched
+    const int kmax = (s->n[2] + 1 + 3) / 4 * 4;
+    std::vector<int> kb{0, kmax}, jb{0, rows};
+    auto kcut = [&](int c) { if (c > 0 && c < kmax) kb.push_back(c); };
     auto jcut = [&](int c) { if (c > 0 && c < rows) jb.push_back(c); };
     if (s->has_pml) {
         int r[2][2];
@@ -2306,6 +2308,35 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
     for (auto *v : {&kb, &jb}) {
         std::sort(v->begin(), v->end());
         v->erase(std::unique(v->begin(), v->end()), v->end());
+    }
+    // A k segment thinner than four groups leaves most lanes of a warp on
+    // different rows; it joins a neighbour (its class then follows from the
+    // joined range): preferably one that meets a Debye box (the lean Debye
+    // kernel handles points outside the box too), then a plain one, last a z
+    // CPML slab (the general kernel).
+    {
+        auto rank = [&](int ks, int ke) {
+            for (int k = ks; k < ke; k++)
+                if (slab(2, k)) return 2;
+            for (const int *bx : boxes)
+                if (ke > bx[2] && ks < bx[2] + bx[5]) return 1;
+            return 0;
+        };
+        constexpr int kThin = 16;
+        for (bool changed = true; changed && kb.size() > 2;) {
+            changed = false;
+            for (size_t q = 0; q + 1 < kb.size(); q++) {
+                if (kb[q + 1] - kb[q] >= kThin) continue;
+                static const int cost[3] = {1, 0, 2};   // by rank: plain, box, slab
+                const int left = q > 0 ? cost[rank(kb[q - 1], kb[q])] : 99;
+                const int right = q + 2 < kb.size() ? cost[rank(kb[q + 1], kb[q + 2])] : 99;
+                if (left == 99 && right == 99) break;
+                if (left <= right) kb.erase(kb.begin() + q);   // join the left neighbour
+                else kb.erase(kb.begin() + q + 1);
+                changed = true;
+                break;
+            }
+        }
     }
     struct Rect { int ks, ke, js, je; };
     std::vector<Rect> cls[kSpaces];
@@ -3500,7 +3531,7 @@ int cemx_profile_steps(cem_sim *s, long n, double *kernel_ms, long *launches) {
 
 int cemx_sizes(const cem_sim *s, long long *out, int n) {
     if (!s->finalized) { set_error("not finalized"); return -1; }
-    long long v[13] = {0};
+    long long v[19] = {0};
     v[0] = (long long)s->n[0] * s->n[1] * s->n[2];
     v[1] = (long long)s->N;
     for (int c = 0; c < 3; c++)
@@ -3534,9 +3565,27 @@ int cemx_sizes(const cem_sim *s, long long *out, int n) {
             const Device &D = *s->dev;
             upd -= space_blocks(D.sp[u][kFast]) == 0 || D.p1[u] <= D.p0[u];
             upd -= D.wl_start[u].empty() || D.wl_start[u].back() == 0;
+            upd += u == 1 && space_blocks(D.sp[u][kDebye]) > 0 && D.p1[u] > D.p0[u];
         }
     v[12] = upd + 1 + (s->nsb ? 1 : 0);
-    for (int q = 0; q < n && q < 13; q++) out[q] = v[q];
+    // point-components each update class covers per step (4 points per thread,
+    // 3 components): H fast, H general, E fast, E general, E Debye; and the
+    // Debye boxes' points (pole currents move for all of them)
+    if (s->dev) {
+        const Device &D = *s->dev;
+        for (int u = 0; u < 2; u++) {
+            const long long inner = std::max(0, D.p1[u] - D.p0[u]), planes = u ? s->n[0] : s->n[0] + 1;
+            auto pts = [&](int c) { return 12LL * D.sp[u][c].t0[D.sp[u][c].n]; };
+            const bool split = space_blocks(D.sp[u][kFast]) + space_blocks(D.sp[u][kDebye]) > 0 && inner > 0;
+            const long long fast = split ? pts(kFast) * inner : 0, deb = split ? pts(kDebye) * inner : 0;
+            const long long gen = split ? pts(kGeneral) * inner + pts(kAll) * (planes - inner) : pts(kAll) * planes;
+            v[13 + 2 * u] = fast;
+            v[14 + 2 * u] = gen;
+            if (u == 1) v[17] = deb;
+        }
+        for (int c = 0; c < 3; c++) v[18] += (long long)D.jbox[c][3] * D.jbox[c][4] * D.jbox[c][5];
+    }
+    for (int q = 0; q < n && q < 19; q++) out[q] = v[q];
     return 0;
 }
 

@@ -32,7 +32,10 @@ CEM_API int cemx_profile_steps(cem_sim *s, long n, double *kernel_ms, long *laun
  *   0 cells nx*ny*nz, 1 points N, 2 CPML E auxiliaries, 3 CPML H auxiliaries,
  *   4 Debye edges, 5 Debye poles, 6 surface-impedance edges, 7 their terms,
  *   8..10 coefficient-table entries of Ex/Ey/Ez (0 before the first step),
- *   11 device bytes held (0 before the first step), 12 kernel launches per step.
+ *   11 device bytes held (0 before the first step), 12 kernel launches per step,
+ *   13-17 point-components the update classes cover per step (H fast, H
+ *   general, E fast, E general, E Debye; 0 before the first step),
+ *   18 points of the Debye boxes (all three components).
  * Returns 0 or -1. */
 CEM_API int cemx_sizes(const cem_sim *s, long long *out, int n);
 

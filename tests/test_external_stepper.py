@@ -103,7 +103,7 @@ def test_state_arrays_round_trip_on_device(lib, ref_lib):
     neighbouring points, or one point before and after its update - so their
     FP32 rounding is larger than the fields'); the reference's
     arrays written into the engine's through the same pointers are taken up,
-    and 300 more steps on both keep the fields within 1e-5."""
+    and 300 more steps on both keep the E and H fields within relative L2 1e-5."""
     G, _ = scenes.lossy_scene(lib)
     R, _ = scenes.lossy_scene(ref_lib)
     G.step(600)
@@ -122,5 +122,7 @@ def test_state_arrays_round_trip_on_device(lib, ref_lib):
         G.fieldView(c)[:] = R.field(c)
     G.step(300)
     R.step(300)
-    for c in range(6):
-        assert rel_l2(G.field(c), R.field(c)) < 1e-5, c
+    for fam in (range(3), range(3, 6)):   # relative to the family's norm (the longitudinal Ex is small)
+        num = np.sqrt(sum(np.linalg.norm(G.field(c) - R.field(c)) ** 2 for c in fam))
+        den = np.sqrt(sum(np.linalg.norm(R.field(c)) ** 2 for c in fam))
+        assert num / den < 1e-5, list(fam)
