@@ -123,3 +123,26 @@ def test_c2_full_run_sparams(lib, excite):
     errs = column_errors(col, ref, excite)
     print("c2 excite", excite, errs)
     check(errs)
+
+
+@pytest.mark.parametrize("excite", [1, 2])
+def test_large_board_generator_scaled_against_reference(lib, ref_lib, excite):
+    """A board from the large configuration's generator (4-layer stackup with
+    4-pole Debye cores, traces with 45-degree jogs, vias, plane clearances,
+    rule-based non-uniform mesh, 2D mode ports) at 2.5e5 cells, 5 000 steps,
+    16 frequencies, both excitations: the modal S-matrix columns against the
+    reference core run on the same plan beside it, within the gate."""
+    from courant_b200 import boards
+    kw = dict(seed=31, cells=2.5e5, ports="mode", nf=16, steps=5000, excite=excite)
+    s, meta = boards.seeded_board(lib, **kw)
+    r, mr = boards.seeded_board(ref_lib, **kw)
+    assert meta["dims"] == mr["dims"] and meta["cells"] >= 2e5
+    assert meta["mesh"]["y"]["max_cell"] > 1.3 * meta["mesh"]["y"]["min_cell"]   # non-uniform
+    s.step(meta["steps"])
+    r.step(meta["steps"])
+    col, rcol = scenes.two_port_s(s, meta), scenes.two_port_s(r, mr)
+    ref = {"freqs": list(meta["freqs"]),
+           "S": [[[complex(v).real, complex(v).imag] for v in b] for b in rcol["b"]]}
+    errs = column_errors(col, ref, excite)
+    print("board excite", excite, meta["dims"], errs)
+    check(errs)
