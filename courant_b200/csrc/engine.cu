@@ -20,6 +20,7 @@
 // stored as their difference from 1 (ca-1, b-1, 1-k, 1-e) so FP32 keeps the
 // decay rates accurate over tens of thousands of steps.
 #include "sim.hpp"
+#include "spaces.hpp"
 #include "../../include/courant_b200.h"
 
 #include <cuda.h>
@@ -2309,35 +2310,14 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
         std::sort(v->begin(), v->end());
         v->erase(std::unique(v->begin(), v->end()), v->end());
     }
-    // A k segment thinner than four groups leaves most lanes of a warp on
-    // different rows; it joins a neighbour (its class then follows from the
-    // joined range): preferably one that meets a Debye box (the lean Debye
-    // kernel handles points outside the box too), then a plain one, last a z
-    // CPML slab (the general kernel).
-    {
-        auto rank = [&](int ks, int ke) {
-            for (int k = ks; k < ke; k++)
-                if (slab(2, k)) return 2;
-            for (const int *bx : boxes)
-                if (ke > bx[2] && ks < bx[2] + bx[5]) return 1;
-            return 0;
-        };
-        constexpr int kThin = 16;
-        for (bool changed = true; changed && kb.size() > 2;) {
-            changed = false;
-            for (size_t q = 0; q + 1 < kb.size(); q++) {
-                if (kb[q + 1] - kb[q] >= kThin) continue;
-                static const int cost[3] = {1, 0, 2};   // by rank: plain, box, slab
-                const int left = q > 0 ? cost[rank(kb[q - 1], kb[q])] : 99;
-                const int right = q + 2 < kb.size() ? cost[rank(kb[q + 1], kb[q + 2])] : 99;
-                if (left == 99 && right == 99) break;
-                if (left <= right) kb.erase(kb.begin() + q);   // join the left neighbour
-                else kb.erase(kb.begin() + q + 1);
-                changed = true;
-                break;
-            }
-        }
-    }
+    // thin k segments join a neighbour (spaces.hpp)
+    merge_thin_segments(kb, [&](int ks, int ke) {
+        for (int k = ks; k < ke; k++)
+            if (slab(2, k)) return 2;
+        for (const int *bx : boxes)
+            if (ke > bx[2] && ks < bx[2] + bx[5]) return 1;
+        return 0;
+    });
     struct Rect { int ks, ke, js, je; };
     std::vector<Rect> cls[kSpaces];
     for (size_t q = 0; q + 1 < kb.size(); q++) {

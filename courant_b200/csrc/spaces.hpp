@@ -1,0 +1,49 @@
+// Host-side layout rule of the update kernels' thread spaces (engine.cu
+// build_spaces), kept apart so that it can be tested on its own.
+#pragma once
+
+#include <vector>
+
+namespace cb2 {
+
+// The k axis of a node plane is cut into segments at `kb` (sorted, first 0,
+// last the end of the k range); one thread moves four consecutive k, and the
+// threads of a segment's rows follow one another. A segment thinner than four
+// groups (16 points) leaves most lanes of a warp on different rows, so it
+// joins a neighbour, whose class the joined range then takes. rank(ks, ke):
+// 2 when [ks, ke) reaches a z CPML slab (general kernel), 1 when it meets a
+// Debye box (lean Debye kernel, which also handles points outside the box),
+// 0 otherwise (lean kernel). The preferred neighbour is a Debye one, then a
+// plain one, then a CPML one (the thinner on a tie); a thin CPML segment never
+// joins a thick CPML-free neighbour, which would turn the whole thick segment
+// general, and then stays as it is.
+template <class Rank>
+void merge_thin_segments(std::vector<int> &kb, Rank rank) {
+    constexpr int kThin = 16;
+    static const int cost[3] = {1, 0, 2};   // by rank: plain, box, slab
+    for (bool changed = true; changed && kb.size() > 2;) {
+        changed = false;
+        for (size_t q = 0; q + 1 < kb.size(); q++) {
+            if (kb[q + 1] - kb[q] >= kThin) continue;
+            const int r = rank(kb[q], kb[q + 1]);
+            int best = -1, best_cost = 99, best_w = 1 << 30;   // cut to erase, its cost, the neighbour's width
+            for (int side = 0; side < 2; side++) {
+                if (side == 0 ? q == 0 : q + 2 >= kb.size()) continue;
+                const int a = side == 0 ? kb[q - 1] : kb[q + 1], b = side == 0 ? kb[q] : kb[q + 2];
+                const int nr = rank(a, b), nw = b - a;
+                if (r == 2 && nr != 2 && nw >= kThin) continue;
+                if (cost[nr] < best_cost || (cost[nr] == best_cost && nw < best_w)) {
+                    best = side == 0 ? (int)q : (int)q + 1;
+                    best_cost = cost[nr];
+                    best_w = nw;
+                }
+            }
+            if (best < 0) continue;   // stays thin
+            kb.erase(kb.begin() + best);
+            changed = true;
+            break;
+        }
+    }
+}
+
+}  // namespace cb2

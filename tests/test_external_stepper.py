@@ -101,13 +101,16 @@ def test_state_arrays_round_trip_on_device(lib, ref_lib):
     core's (FP32 state against f64: relative L2 <= 2e-4; the CPML and Debye
     recursions are driven by differences of nearly equal field values -
     neighbouring points, or one point before and after its update - so their
-    FP32 rounding is larger than the fields'); the reference's
-    arrays written into the engine's through the same pointers are taken up,
-    and 300 more steps on both keep the E and H fields within relative L2 1e-5."""
+    FP32 rounding is larger than the fields'). The reference's arrays and
+    fields written into the engine through the same pointers are taken up:
+    150 steps later the E and H fields are within relative L2 1e-5 of the
+    reference, and no further from it than a second engine run that never
+    took the reference's state."""
     G, _ = scenes.lossy_scene(lib)
+    G2, _ = scenes.lossy_scene(lib)
     R, _ = scenes.lossy_scene(ref_lib)
-    G.step(600)
-    R.step(600)
+    for x in (G, G2, R):
+        x.step(600)
     keys = [(0, c, w) for c in range(3) for w in range(2)] + [(1, c, w) for c in range(3) for w in range(2)]
     keys += [(2, 0, 0), (4, 0, 0)]
     for k in keys:
@@ -120,9 +123,10 @@ def test_state_arrays_round_trip_on_device(lib, ref_lib):
         _state(G, *k)[:] = _state(R, *k)
     for c in range(6):
         G.fieldView(c)[:] = R.field(c)
-    G.step(300)
-    R.step(300)
-    for fam in (range(3), range(3, 6)):   # relative to the family's norm (the longitudinal Ex is small)
-        num = np.sqrt(sum(np.linalg.norm(G.field(c) - R.field(c)) ** 2 for c in fam))
+    for x in (G, G2, R):
+        x.step(150)
+    for fam in (range(3), range(3, 6)):
         den = np.sqrt(sum(np.linalg.norm(R.field(c)) ** 2 for c in fam))
-        assert num / den < 1e-5, list(fam)
+        err = np.sqrt(sum(np.linalg.norm(G.field(c) - R.field(c)) ** 2 for c in fam)) / den
+        err2 = np.sqrt(sum(np.linalg.norm(G2.field(c) - R.field(c)) ** 2 for c in fam)) / den
+        assert err < 1e-5 and err <= err2, (list(fam), err, err2)
