@@ -206,95 +206,80 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
-def batch_compare(lib, runs: int, seed: int = 2026) -> dict:
-    """Batched uneven instances (a bounded stand-in for the 96-board mix): runs/2
-    seeded boards with cells log-uniform in 5e4-1e6, steps uniform in 2000-6000,
-    both excitations each; one at a time with cem_step (the plain path; set-up
-    and device state excluded) against one batch (graph-captured batched
-    launches, tuned once; device state created by add, outside the timing).
-    Results must be bit-identical; reports solves/hour and cell-updates/s."""
-    import numpy as np
-    from courant_b200 import boards, serve
-    rng = np.random.Generator(np.random.PCG64(seed))
-    half = max(runs // 2, 1)
-    cells = np.exp(rng.uniform(np.log(5e4), np.log(1e6), half))
-    steps = rng.integers(2000, 6000, half)
-    spec = [(q, float(cells[q]), int(steps[q]), ex) for q in range(half) for ex in (1, 2)]
-
-    def build():
-        return [boards.seeded_board(lib, q, cl, ports="lumped", nf=16, excite=ex) for q, cl, _, ex in spec]
-
-    sims = build()
-    work = sum(m["cells"] * n for (_, m), (_, _, n, _) in zip(sims, spec))
-    for s, _ in sims:   # device state outside the timed region, as for the batch members (add)
-        s.prepareDevice()
-    t0 = time.perf_counter()
-    for (s, _), (_, _, n, _) in zip(sims, spec):
-        s.step(n)
-        s.synchronize()   # one at a time: cem_step returns before its device work ends
-    t_plain = time.perf_counter() - t0
-    plain = [serve.results(s, m)["S21"] for s, m in sims]
-    for s, _ in sims:
-        s.destroy()
-    sims = build()
-    b = lib.createBatch()
-    b.tune(True)
-    for (s, _), (_, _, n, _) in zip(sims, spec):
-        b.add(s, n)
-    t0 = time.perf_counter()
-    while b.run(1 << 30):
-        pass
-    t_batch = time.perf_counter() - t0
-    st = b.stats()
-    same = all(np.array_equal(a, serve.results(s, m)["S21"]) for a, (s, m) in zip(plain, sims))
-    b.destroy()
-    for s, _ in sims:
-        s.destroy()
-    n = len(spec)
-    return {"runs": n, "cell_updates": work, "same_results": same,
-            "plain": {"wall_s": t_plain, "solves_per_hour": n / t_plain * 3600, "cell_updates_per_s": work / t_plain},
-            "batched": {"wall_s": t_batch, "solves_per_hour": n / t_batch * 3600, "cell_updates_per_s": work / t_batch,
-                        "graph_steps": st["chunk"], "work_order": st["order"]},
-            "speedup": t_plain / t_batch,
-            "note": "wall time of the stepping only (set-up and S-parameters excluded); inputs resident"}
-
-
-def serve_compare(lib, n: int, rate: float, seed: int = 7) -> dict:
-    """Serving (a bounded stand-in for the Poisson request stream): n requests at
-    `rate` per second, seeded boards with cells log-uniform in 1e5-2e6, steps
-    uniform in 2000-6000, a quarter with 2D mode ports, the rest lumped, 16
-    frequencies; the plain FIFO loop (set-up, steps, S-parameters one request at
-    a time) against the continuously batching server. Times are wall clock from
-    arrival to S-parameters."""
+def _mix_requests(spec, nf):
+    """serve.Request objects for (seed, cells, steps, excite) tuples: seeded
+    boards of the large configuration's generator with 2D mode ports."""
     import functools
-    import numpy as np
     from courant_b200 import boards, serve
-    rng = np.random.Generator(np.random.PCG64(seed))
-    cells = np.exp(rng.uniform(np.log(1e5), np.log(2e6), n))
-    steps = rng.integers(2000, 6000, n)
-    kinds = rng.integers(0, 4, n)
-    arr = np.cumsum(rng.exponential(1 / rate, n))
-    arr -= arr[0]
+    return [serve.Request(functools.partial(boards.seeded_board, seed=sd, cells=cl, ports="mode", nf=nf, excite=ex),
+                          int(st), tag=(sd, ex)) for sd, cl, st, ex in spec]
 
-    def req(q):
-        ports = "mode" if kinds[q] == 0 else "lumped"
-        return serve.Request(functools.partial(boards.seeded_board, seed=100 + q, cells=float(cells[q]), ports=ports,
-                                               nf=16), int(steps[q]))
 
+def _compare(lib, spec, arrivals, nf) -> dict:
+    """The same requests through the plain FIFO loop (set-up, steps and
+    S-parameters one request at a time, each waiting for its arrival) and
+    through the continuously batching server; solves/hour, latencies and mean
+    stage times of both, and whether every result is the same."""
+    import numpy as np
+    from courant_b200 import serve
     t0 = time.perf_counter()
-    plain = serve.plain_loop(lib, [req(q) for q in range(n)], list(arr))
+    plain = serve.plain_loop(lib, _mix_requests(spec, nf), list(arrivals))
     sp = serve.summary(plain, t0, time.perf_counter())
     srv = serve.Server(lib, chunk=512, builders=8, finishers=8)
     t0 = time.perf_counter()
-    got = serve.serve_all(srv, [req(q) for q in range(n)], list(arr))
+    got = serve.serve_all(srv, _mix_requests(spec, nf), list(arrivals))
     t1 = time.perf_counter()
     srv.close()
     ss = serve.summary(got, t0, t1)
     same = all((a.result is None) == (g.result is None) and
-               (a.result is None or np.array_equal(a.result["S21"], g.result["S21"])) for a, g in zip(plain, got))
-    return {"requests": n, "rate_per_s": rate, "same_results": same, "plain_fifo": sp, "served": ss,
+               (a.result is None or all(np.array_equal(a.result[k], g.result[k]) for k in ("S1", "S2")))
+               for a, g in zip(plain, got))
+    return {"requests": len(spec), "same_results": same, "plain_fifo": sp, "served": ss,
             "gpu_busy_s": srv.gpu_ms / 1e3,
             "solves_per_hour_vs_plain": ss["solves_per_hour"] / sp["solves_per_hour"] if sp["solves_per_hour"] else None}
+
+
+def batch_compare(lib, boards_n: int, seed: int = 2026) -> dict:
+    """Batched uneven instances, the 96-board configuration bounded to
+    `boards_n` boards: seeded boards of the large configuration's generator
+    (2D mode ports, 16 frequencies) with cells log-uniform in 5e4-8e6, both
+    excitations each, steps uniform in 1 000-4 000 (a tenth of the
+    configuration's 10k-40k, so that the comparison takes minutes). All runs
+    are there at the start. Plain: one run at a time (set-up, steps,
+    S-parameters); batched: the server (host set-up on builder threads, device
+    state on loader threads, all runs advancing together in batched launches,
+    S-parameters on finisher threads). Results must be bit-identical."""
+    import numpy as np
+    rng = np.random.Generator(np.random.PCG64(seed))
+    cells = np.exp(rng.uniform(np.log(5e4), np.log(8e6), boards_n))
+    steps = rng.integers(1000, 4000, boards_n)
+    spec = [(1000 + q, float(cells[q]), int(steps[q]), ex) for q in range(boards_n) for ex in (1, 2)]
+    out = _compare(lib, spec, [0.0] * len(spec), nf=16)
+    out["bound"] = (f"{boards_n} of 96 boards x 2 excitations, steps 1k-4k instead of 10k-40k, 16 frequencies; "
+                    "solves/hour over the whole job (set-up, steps, S-parameters)")
+    return out
+
+
+def serve_compare(lib, n: int, rates: list, seed: int = 7) -> dict:
+    """Serving, the Poisson request stream bounded to `n` requests per rate:
+    seeded boards of the large configuration's generator with cells
+    log-uniform in 1e5-2e7, 2 mode ports (port 1 driven), 16 frequencies,
+    steps uniform in 1 000-5 000 (a tenth of 10k-50k), arriving as a Poisson
+    stream at each rate of the sweep; the plain FIFO loop against the
+    continuously batching server under a 160 GB HBM budget. Times are wall
+    clock from arrival to S-parameters."""
+    import numpy as np
+    out = {"bound": f"{n} requests per rate, rates {rates} of the 0.05-2 req/s sweep, steps 1k-5k instead of "
+                    "10k-50k, 2 ports (of 1-4), 16 frequencies", "rates": {}}
+    for rate in rates:
+        rng = np.random.Generator(np.random.PCG64(seed + int(rate * 1000)))
+        cells = np.exp(rng.uniform(np.log(1e5), np.log(2e7), n))
+        steps = rng.integers(1000, 5000, n)
+        arr = np.cumsum(rng.exponential(1 / rate, n))
+        arr -= arr[0]
+        spec = [(500 + q, float(cells[q]), int(steps[q]), 1) for q in range(n)]
+        out["rates"][str(rate)] = _compare(lib, spec, list(arr), nf=16)
+    return out
 
 
 class Ranks:
@@ -441,7 +426,7 @@ def run_b200(args) -> None:
         batching = batch_compare(lib, args.batch_runs)
     if rank == 0 and world == 1 and args.serve_requests > 0:
         log("serving comparison ...")
-        serving = serve_compare(lib, args.serve_requests, args.serve_rate)
+        serving = serve_compare(lib, args.serve_requests, [float(r) for r in args.serve_rates.split(",")])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -494,9 +479,10 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch-runs", type=int, default=16, help="runs in the batched-vs-plain comparison (0: skip)")
-    ap.add_argument("--serve-requests", type=int, default=12, help="requests in the serving comparison (0: skip)")
-    ap.add_argument("--serve-rate", type=float, default=8.0, help="request arrival rate of the serving comparison, 1/s")
+    ap.add_argument("--batch-runs", type=int, default=12,
+                    help="boards (two excitations each) in the batched-vs-plain comparison (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=10, help="requests per rate in the serving comparison (0: skip)")
+    ap.add_argument("--serve-rates", default="0.5,2", help="Poisson arrival rates of the serving comparison, 1/s")
     args = ap.parse_args()
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
     if args.impl == "reference":

@@ -27,7 +27,10 @@
 //  * The eigenpair nearest sigma = (k0 n_guess)^2 comes from shifted inverse
 //    iteration: converged when the eigenvalue estimate sigma + 1/<x, y> changes
 //    by less than tol relatively and the phase-aligned iterate by less than
-//    1e-10, the reference's stopping rule.
+//    1e-10, the reference's stopping rule. When that has not happened within
+//    maxit iterations (a second mode nearly as close to the shift), the shift
+//    moves onto the current estimate and the band is factorised again, up to
+//    three times; the reference's solver gives up there.
 #include "sim.hpp"
 
 #include <algorithm>
@@ -390,7 +393,7 @@ void cem_mode2d_set_pml(cem_mode2d *m, int which, const double *sigma, const dou
     m->pml_a[which].assign(alpha, alpha + len);
 }
 
-// 0: converged; 1: not within maxit iterations (the last iterate is kept); -1: singular
+// 0: converged; 1: not within maxit iterations and three refined shifts (the last iterate is kept); -1: singular
 int cem_mode2d_solve(cem_mode2d *m, double f, double neff_guess, const double *start, int maxit, double tol) {
     const int ny = m->ny, nz = m->nz;
     const double w = 2 * M_PI * f, k0 = w / CEM_C0;
@@ -399,30 +402,33 @@ int cem_mode2d_solve(cem_mode2d *m, double f, double neff_guess, const double *s
     const Numbering o = number_unknowns(*m);
     const int n = o.n;
     if (n == 0) return -1;
-    // rows of A - sigma I and the band they need
+    // rows of A and the band they need
     std::vector<Row> rows(n);
     int half = 0;
     for (int g = 0; g < n; g++) {
         const int pt = o.where[g] >> 1, which = o.where[g] & 1;
         const int j = which == U ? pt / (nz + 1) : pt / nz, k = which == U ? pt % (nz + 1) : pt % nz;
         rows[g] = assemble_row(*m, c, o, w, which, j, k);
-        rows[g].add(g, -sigma);
+        rows[g].add(g, 0.0);   // the diagonal always has an entry for the shift
         for (int q = 0; q < rows[g].n; q++) half = std::max(half, std::abs(rows[g].col[q] - g));
     }
     Band B;
     B.n = n;
     B.kl = B.ku = half;
     B.width = 2 * half + half + 1;
-    B.a.assign((size_t)n * B.width * 2, 0.0);
-    for (int g = 0; g < n; g++)
-        for (int q = 0; q < rows[g].n; q++) {
-            double *e = B.at(g, rows[g].col[q]);
-            e[0] += rows[g].val[q].real();
-            e[1] += rows[g].val[q].imag();
-        }
-    rows.clear();
-    rows.shrink_to_fit();
-    if (!band_factor(B)) return -1;
+    // LU of A - shift I
+    auto factor = [&](cplx shift) {
+        B.a.assign((size_t)n * B.width * 2, 0.0);
+        for (int g = 0; g < n; g++)
+            for (int q = 0; q < rows[g].n; q++) {
+                const cplx v = rows[g].val[q] - (rows[g].col[q] == g ? shift : cplx(0.0));
+                double *e = B.at(g, rows[g].col[q]);
+                e[0] += v.real();
+                e[1] += v.imag();
+            }
+        return band_factor(B);
+    };
+    if (!factor(sigma)) return -1;
 
     // start vector: the given field (API layout: E_u then E_v, complex) or a fixed pseudo-random one
     std::vector<cplx> x(n), y(n);
@@ -442,26 +448,38 @@ int cem_mode2d_solve(cem_mode2d *m, double f, double neff_guess, const double *s
     double nx = norm2(x);
     if (!(nx > 0)) return -1;
     for (cplx &v : x) v /= nx;
-    cplx lam = sigma, lam_prev = 0;
-    int rc = 1;
-    for (int it = 0; it < maxit; it++) {
-        y = x;
-        band_solve(B, y);
-        const cplx mu = inner(x, y);
-        lam = sigma + 1.0 / mu;
-        const double ny2 = norm2(y);
-        for (cplx &v : y) v /= ny2;
-        // change of the iterate with its global phase aligned to the previous one
-        const cplx ph = inner(y, x);
-        const cplx rot = std::abs(ph) > 0 ? ph / std::abs(ph) : cplx(1.0);
-        double d = 0;
-        for (int g = 0; g < n; g++) d += std::norm(y[g] * rot - x[g]);
-        x.swap(y);
-        if (it >= 2 && std::abs(lam - lam_prev) < tol * std::abs(lam) && std::sqrt(d) < 1e-10) {
-            rc = 0;
-            break;
+    cplx lam = sigma;
+    // inverse iteration with shift `shift`, from x; true when converged
+    auto iterate = [&](cplx shift, int its) {
+        cplx lam_prev = 0;
+        for (int it = 0; it < its; it++) {
+            y = x;
+            band_solve(B, y);
+            const cplx mu = inner(x, y);
+            lam = shift + 1.0 / mu;
+            const double ny2 = norm2(y);
+            for (cplx &v : y) v /= ny2;
+            // change of the iterate with its global phase aligned to the previous one
+            const cplx ph = inner(y, x);
+            const cplx rot = std::abs(ph) > 0 ? ph / std::abs(ph) : cplx(1.0);
+            double d = 0;
+            for (int g = 0; g < n; g++) d += std::norm(y[g] * rot - x[g]);
+            x.swap(y);
+            if (it >= 2 && std::abs(lam - lam_prev) < tol * std::abs(lam) && std::sqrt(d) < 1e-10) return true;
+            lam_prev = lam;
         }
-        lam_prev = lam;
+        return false;
+    };
+    int rc = iterate(sigma, maxit) ? 0 : 1;
+    // Where a second mode lies nearly as close to the shift, inverse iteration
+    // crawls and stops at maxit (the reference's solver returns there). This
+    // solver then moves the shift onto the estimate of the mode it has been
+    // converging to and iterates again (up to three times): with the shift at
+    // the eigenvalue the other modes fall away at once.
+    for (int refine = 0; rc == 1 && refine < 3; refine++) {
+        const cplx shift = lam;
+        if (!factor(shift)) break;
+        if (iterate(shift, 60)) rc = 0;
     }
     // largest component real and positive; scatter into the API arrays
     int imax = 0;

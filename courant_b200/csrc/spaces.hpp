@@ -13,10 +13,11 @@ namespace cb2 {
 // joins a neighbour, whose class the joined range then takes. rank(ks, ke):
 // 2 when [ks, ke) reaches a z CPML slab (general kernel), 1 when it meets a
 // Debye box (lean Debye kernel, which also handles points outside the box),
-// 0 otherwise (lean kernel). The preferred neighbour is a Debye one, then a
-// plain one, then a CPML one (the thinner on a tie); a thin CPML segment never
-// joins a thick CPML-free neighbour, which would turn the whole thick segment
-// general, and then stays as it is.
+// 0 otherwise (lean kernel). A thin segment never joins a thick neighbour of
+// lower rank (that would move the whole thick segment to a costlier kernel:
+// a thin Debye box above a thick plain region stays thin); among the
+// neighbours it may join, a Debye one is preferred, then a plain one, then a
+// CPML one (the thinner on a tie); with none it stays as it is.
 template <class Rank>
 void merge_thin_segments(std::vector<int> &kb, Rank rank) {
     constexpr int kThin = 16;
@@ -31,10 +32,11 @@ void merge_thin_segments(std::vector<int> &kb, Rank rank) {
                 if (side == 0 ? q == 0 : q + 2 >= kb.size()) continue;
                 const int a = side == 0 ? kb[q - 1] : kb[q + 1], b = side == 0 ? kb[q] : kb[q + 2];
                 const int nr = rank(a, b), nw = b - a;
-                if (r == 2 && nr != 2 && nw >= kThin) continue;
-                if (cost[nr] < best_cost || (cost[nr] == best_cost && nw < best_w)) {
+                const int joined = r > nr ? r : nr;
+                if (nw >= kThin && joined > nr) continue;
+                if (cost[joined] < best_cost || (cost[joined] == best_cost && nw < best_w)) {
                     best = side == 0 ? (int)q : (int)q + 1;
-                    best_cost = cost[nr];
+                    best_cost = cost[joined];
                     best_w = nw;
                 }
             }

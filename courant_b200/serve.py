@@ -47,15 +47,12 @@ def footprint(sim: Sim) -> int:
 
 
 def results(sim: Sim, meta: dict) -> dict:
-    """S11 and S21 of a two-port with port 1 excited: from the modal waves of
-    mode ports, or from the port spectra of lumped ports."""
-    if "modeports" in meta:
-        p1, p2 = meta["modeports"]
-        w1, w2 = sim.modePortWaves(p1), sim.modePortWaves(p2)
-        return {"S11": w1["b"] / w1["a"], "S21": w2["b"] / w1["a"]}
-    p1, p2 = meta["ports"]
-    s11, s21 = s_params(sim.portV(p1), sim.portI(p1), sim.portV(p2), sim.portI(p2), 50.0)
-    return {"S11": s11, "S21": s21}
+    """The S-matrix column of the driven port e (meta["excite"]): "S1" = S_1e
+    and "S2" = S_2e, from the modal waves of mode ports or from the port
+    spectra of lumped ports (50 ohm)."""
+    from .scenes import two_port_s
+    col = two_port_s(sim, meta)
+    return {"S1": col["b"][0], "S2": col["b"][1], "excite": meta.get("excite", 1)}
 
 
 @dataclass
@@ -70,6 +67,10 @@ class Request:
     error: str | None = None
     cells: int = 0
     event: threading.Event = field(default_factory=threading.Event)
+    # stage ends (perf_counter): host set-up, device state, last step on the GPU
+    built: float = 0.0
+    loaded: float = 0.0
+    stepped: float = 0.0
 
 
 class Server:
@@ -107,6 +108,7 @@ class Server:
     def _build(self, r: Request):
         try:
             sim, meta = r.build(self.lib)
+            r.built = time.perf_counter()
             r.cells = meta.get("cells", sim.nx * sim.ny * sim.nz)
             nbytes = footprint(sim)
             if nbytes > self.budget:
@@ -124,6 +126,7 @@ class Server:
         r, sim, meta, nbytes = item
         try:
             sim.prepareDevice(self.device)
+            r.loaded = time.perf_counter()
             with self.lock:
                 self.loaded.append(item)
         except Exception as e:
@@ -185,6 +188,7 @@ class Server:
         for h, item in list(self.members.items()):
             sim = item[1]
             if self.batch.left(sim) == 0:
+                item[0].stepped = time.perf_counter()
                 self.batch.remove(sim)
                 del self.members[h]
                 self.finish_pool.submit(self._finish, item)
@@ -244,8 +248,13 @@ def plain_loop(lib: Courant, requests: list[Request], arrivals: list[float]) -> 
         r.arrival = t0 + at
         try:
             sim, meta = r.build(lib)
+            r.built = time.perf_counter()
             r.cells = meta.get("cells", sim.nx * sim.ny * sim.nz)
+            sim.prepareDevice()
+            r.loaded = time.perf_counter()
             sim.step(r.steps)
+            sim.synchronize()
+            r.stepped = time.perf_counter()
             r.result = results(sim, meta)
             sim.destroy()
         except Exception as e:
@@ -281,4 +290,17 @@ def summary(reqs: list[Request], t_start: float, t_end: float) -> dict:
             "cell_updates_per_s": cells / wall if wall > 0 else None,
             "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
             "p95_s": float(np.percentile(lat, 95)) if len(lat) else None,
-            "p99_s": float(np.percentile(lat, 99)) if len(lat) else None}
+            "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+            "stage_means_s": stage_means(reqs)}
+
+
+def stage_means(reqs: list[Request]) -> dict:
+    """Mean seconds per stage of the finished requests: waiting and host
+    set-up (arrival to built), device state (to loaded), steps including the
+    wait for the GPU (to the last step), results (S-parameters and freeing)."""
+    ok = [r for r in reqs if r.error is None and r.built and r.loaded and r.stepped]
+    if not ok:
+        return {}
+    mean = lambda v: float(np.mean(v))
+    return {"setup": mean([r.built - r.arrival for r in ok]), "device": mean([r.loaded - r.built for r in ok]),
+            "steps": mean([r.stepped - r.loaded for r in ok]), "results": mean([r.done - r.stepped for r in ok])}

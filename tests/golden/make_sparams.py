@@ -5,7 +5,7 @@ Run here, where oracle/_ref has been built from the reference sources
 (`make -C oracle ref`):
 
     python tests/golden/make_sparams.py c1            # ~1 min on 8 threads
-    python tests/golden/make_sparams.py c2            # ~2 h on 8 threads
+    python tests/golden/make_sparams.py c2            # ~3 h on 8 threads (or --excite 1/2 in parallel, then --merge)
 
 For each excitation (port 1 driven, then port 2) the reference steps the
 configuration for its full step count (c1: 20 000, c2: 40 000) and the excited
@@ -64,9 +64,19 @@ def run(c: Courant, name: str, excite: int) -> dict:
 
 
 def main() -> None:
+    """make_sparams.py NAME            both excitations, then the fixture
+    make_sparams.py NAME --excite E    one excitation into sparams_NAME.eE.json (to run the two in parallel)
+    make_sparams.py NAME --merge       the fixture from the two one-excitation files"""
     name = sys.argv[1]
     c = Courant(REF_LIB)
-    runs = [run(c, name, e) for e in (1, 2)]
+    if "--excite" in sys.argv:
+        e = int(sys.argv[sys.argv.index("--excite") + 1])
+        (OUT / f"sparams_{name}.e{e}.json").write_text(json.dumps(run(c, name, e)))
+        return
+    if "--merge" in sys.argv:
+        runs = [json.loads((OUT / f"sparams_{name}.e{e}.json").read_text()) for e in (1, 2)]
+    else:
+        runs = [run(c, name, e) for e in (1, 2)]
     gold = {"source": "skyhoffert/CourantEM 20261017.0 solver core, built by oracle/Makefile",
             "config": name, "kw": {k: (list(v) if isinstance(v, tuple) else v)
                                     for k, v in scenes.CONFIGS[name]["kw"].items()},

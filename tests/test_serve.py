@@ -39,7 +39,7 @@ def test_served_results_equal_alone(lib):
         srv.close()
     for a, g in zip(alone, got):
         assert g.error is None, g.error
-        for k in ("S11", "S21"):
+        for k in ("S1", "S2"):
             assert np.array_equal(a.result[k], g.result[k]), k
     s = serve.summary(got, min(r.arrival for r in got), max(r.done for r in got))
     assert s["solves"] == len(MIX) and s["p50_s"] <= s["p99_s"]
@@ -128,7 +128,7 @@ def test_failed_batch_fails_its_requests_and_serving_goes_on(monkeypatch):
         sims.append(s)
         return s, {"cells": 512}
 
-    monkeypatch.setattr(serve, "results", lambda sim, meta: {"S11": np.zeros(1), "S21": np.zeros(1)})
+    monkeypatch.setattr(serve, "results", lambda sim, meta: {"S1": np.zeros(1), "S2": np.zeros(1)})
     _FakeBatch.made = 0
     srv = serve.Server(_FakeLib(), budget_bytes=1e9, chunk=16, builders=1, finishers=1)
     try:

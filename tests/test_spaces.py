@@ -41,3 +41,8 @@ def test_thick_segments_stay(case):
 def test_no_cuts_and_single_segment(case):
     assert case(68, (0, 0), (0, 0), []) == [0, 68]
     assert case(12, (0, 0), (0, 0), []) == [0, 12]
+
+
+def test_thin_box_does_not_turn_a_thick_plain_segment_into_debye(case):
+    # E of the lossy 2-port line: Debye boxes k 0-11 under 64 plain node groups, z CPML from 76
+    assert case(88, (76, 87), (0, 12), [12, 76]) == [0, 12, 76, 88]
