@@ -143,6 +143,8 @@ _EXT_PROTOS = [
     ("cemx_select_device", _i, [_i]),
     ("cemx_release_device", _i, [_p]),
     ("cemx_use_fused", _i, [_p, _i]),
+    ("cemx_tune", _i, [_p, _i]),
+    ("cemx_tune_state", _i, [_p, _dp, _i]),
     ("cemx_energy_noalloc", _i, [_p, _dp]),
     ("cemx_prepare_device", _i, [_p, _i]),
     ("cemx_batch_create", _p, [_i]),
@@ -494,6 +496,16 @@ class Sim:
     def useFused(self, on: bool = True) -> bool:
         """Select the single-pass fused H+E kernel (True) or the separate kernels."""
         return bool(self.c.ex.cemx_use_fused(self.h, int(on)))
+
+    def tune(self, on: bool = True) -> bool:
+        """Choose this simulation's launch shape per grid shape (cemx_tune)."""
+        return bool(self.c.ex.cemx_tune(self.h, int(on)))
+
+    def tuneState(self) -> dict:
+        v = np.zeros(6)
+        self._check(self.c.ex.cemx_tune_state(self.h, _ptr(v), 6), "tune_state")
+        return {"tuned": bool(v[0]), "from_cache": bool(v[1]), "thin": int(v[2]), "side_stream": bool(v[3]),
+                "graph_steps": int(v[4]), "ms_per_step": float(v[5])}
 
     def prepareDevice(self, device: int = -1):
         """Create the device state now rather than at the first step."""

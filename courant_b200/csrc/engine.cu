@@ -36,6 +36,8 @@
 #include <thread>
 #include <map>
 #include <atomic>
+#include <sys/stat.h>
+#include <array>
 #include <chrono>
 #include <mutex>
 #include <string>
@@ -1733,10 +1735,22 @@ struct Device {
     cudaEvent_t fork = nullptr, join = nullptr;
     // runs of kGraphSteps whole steps replay one captured graph (CEM_B200_GRAPHS=0: never)
     bool use_graphs = true;
+    // launch shape, chosen by the tuner per grid shape (defaults otherwise):
+    // k segments thinner than `thin` points join a neighbour; general blocks on
+    // the second stream beside the others (`side_on`) or after them on the main
+    // one; `graph_steps` steps per replayed graph
+    int thin = 16;
+    bool side_on = true;
+    int graph_steps = 32;
+    bool tune = false, tuned = false, tuned_from_cache = false;
+    double tuned_ms = 0;
+    cudaEvent_t tev[2] = {nullptr, nullptr};   // tuner timing
     cudaGraphExec_t graph = nullptr;
 
     ~Device() {
         if (graph) cudaGraphExecDestroy(graph);
+        for (cudaEvent_t e : tev)
+            if (e) cudaEventDestroy(e);
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
         if (side) cudaStreamDestroy(side);
@@ -2317,7 +2331,7 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
         for (const int *bx : boxes)
             if (ke > bx[2] && ks < bx[2] + bx[5]) return 1;
         return 0;
-    });
+    }, D.thin);
     struct Rect { int ks, ke, js, je; };
     std::vector<Rect> cls[kSpaces];
     for (size_t q = 0; q + 1 < kb.size(); q++) {
@@ -2559,6 +2573,8 @@ bool create_device_impl(cem_sim *s) {
     if (const char *e = std::getenv("CEM_B200_FUSED")) D.use_fused = e[0] == '1';
     if (const char *e = std::getenv("CEM_B200_GRAPHS")) D.use_graphs = e[0] != '0';
     if (s->kernel_choice >= 0) D.use_fused = s->kernel_choice == 1;
+    if (const char *e = std::getenv("CEM_B200_TUNE")) D.tune = e[0] == '1';
+    if (s->tune_choice >= 0) D.tune = s->tune_choice == 1;
     CB2_CHECK(s, cudaStreamCreateWithFlags(&D.stream, cudaStreamNonBlocking));
     CB2_CHECK(s, cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
     CB2_CHECK(s, cudaEventCreateWithFlags(&D.fork, cudaEventDisableTiming));
@@ -2959,13 +2975,14 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
             t_begin(0);
             const int2 *w;
             const unsigned n = span(0, a, b, w);
-            if (n) {
+            if (n && D.side_on) {
                 fork();
                 k_update_h<<<n, blk, 0, D.side>>>(D.sa[D.cur], w);
                 cudaEventRecord(D.join, D.side);
             }
             fast(0, a, b, k_update_h_fast);
-            if (n) join();
+            if (n && !D.side_on) k_update_h<<<n, blk, 0, D.stream>>>(D.sa[D.cur], w);
+            if (n && D.side_on) join();
             t_end();
         }
     }
@@ -2980,14 +2997,15 @@ bool launch_step(cem_sim *s, int phase_mask, int i0, int i1) {
             t_begin(1);
             const int2 *w;
             const unsigned n = span(1, a, b, w);
-            if (n) {
+            if (n && D.side_on) {
                 fork();
                 kEKernels[s->npole]<<<n, blk, 0, D.side>>>(D.sa[D.cur], w);
                 cudaEventRecord(D.join, D.side);
             }
             fast(1, a, b, k_update_e_fast);
             fast(1, a, b, kEDKernels[s->npole], kDebye);
-            if (n) join();
+            if (n && !D.side_on) kEKernels[s->npole]<<<n, blk, 0, D.stream>>>(D.sa[D.cur], w);
+            if (n && D.side_on) join();
             t_end();
         }
     }
@@ -3064,13 +3082,14 @@ bool run_steps(cem_sim *s, long n) {
     Device &D = *s->dev;
     const bool graphs = D.use_graphs && !D.use_fused && !g_timer;
     for (long it = 0; it < n;) {
-        if (graphs && n - it >= kGraphSteps && D.ring_count + kGraphSteps <= kRing) {
+        const int gs = D.graph_steps;
+        if (graphs && n - it >= gs && D.ring_count + gs <= kRing) {
             if (!D.graph) {
                 const int rc = D.ring_count;
                 const long st = s->step;
                 CB2_CHECK(s, cudaStreamBeginCapture(D.stream, cudaStreamCaptureModeThreadLocal));
                 bool ok = true;
-                for (int q = 0; q < kGraphSteps && ok; q++) ok = launch_step(s, 1 | 4 | 8, 0, s->n[0] + 1);
+                for (int q = 0; q < gs && ok; q++) ok = launch_step(s, 1 | 4 | 8, 0, s->n[0] + 1);
                 cudaGraph_t g = nullptr;
                 const cudaError_t ec = cudaStreamEndCapture(D.stream, &g);
                 D.ring_count = rc;
@@ -3086,9 +3105,9 @@ bool run_steps(cem_sim *s, long n) {
                 CB2_CHECK(s, ei);
             }
             CB2_CHECK(s, cudaGraphLaunch(D.graph, D.stream));
-            D.ring_count += kGraphSteps;
-            s->step += kGraphSteps;
-            it += kGraphSteps;
+            D.ring_count += gs;
+            s->step += gs;
+            it += gs;
         } else {
             if (!launch_step(s, 1 | 4 | 8, 0, s->n[0] + 1)) return false;
             it++;
@@ -3098,11 +3117,135 @@ bool run_steps(cem_sim *s, long n) {
     return true;
 }
 
+// ------------------------------------------------------------------- tuner
+//
+// The launch shape of a simulation (thin-segment threshold of the thread
+// spaces, general blocks on the second stream or after the others, steps per
+// replayed graph) is chosen per grid shape: measured on the simulation's own
+// first steps (every choice computes the same bits, so these are ordinary
+// steps) and kept in a cache file, one line per grid shape, that later
+// processes read instead of measuring again.
+
+std::mutex g_shape_mu;
+bool g_shape_loaded = false;
+std::map<std::string, std::array<double, 4>> g_shapes;   // key -> thin, side, graph steps, ms per step
+
+std::string shape_cache_path() {
+    if (const char *p = std::getenv("CEM_B200_TUNE_CACHE")) return p;
+    std::string base;
+    if (const char *x = std::getenv("XDG_CACHE_HOME")) base = x;
+    else if (const char *h = std::getenv("HOME")) base = std::string(h) + "/.cache";
+    else base = "/tmp";
+    return base + "/courant-b200/launch-shapes.txt";
+}
+
+std::string shape_key(const cem_sim *s) {
+    char k[160];
+    std::snprintf(k, sizeof k, "%dx%dx%d/p%d/sibc%d/pml%d.%d.%d.%d.%d.%d", s->n[0], s->n[1], s->n[2], s->npole,
+                  s->nsb > 0, s->npml[0], s->npml[1], s->npml[2], s->npml[3], s->npml[4], s->npml[5]);
+    return k;
+}
+
+void load_shapes() {   // g_shape_mu held
+    if (g_shape_loaded) return;
+    g_shape_loaded = true;
+    FILE *f = std::fopen(shape_cache_path().c_str(), "r");
+    if (!f) return;
+    char key[200];
+    double v[4];
+    while (std::fscanf(f, "%199s %lf %lf %lf %lf", key, &v[0], &v[1], &v[2], &v[3]) == 5) g_shapes[key] = {v[0], v[1], v[2], v[3]};
+    std::fclose(f);
+}
+
+void store_shape(const std::string &key, const std::array<double, 4> &v) {   // g_shape_mu held
+    g_shapes[key] = v;
+    const std::string path = shape_cache_path();
+    for (size_t q = 1; q < path.size(); q++)   // mkdir -p of the directory
+        if (path[q] == '/') mkdir(path.substr(0, q).c_str(), 0755);
+    if (FILE *f = std::fopen(path.c_str(), "a")) {
+        std::fprintf(f, "%s %g %g %g %.6g\n", key.c_str(), v[0], v[1], v[2], v[3]);
+        std::fclose(f);
+    }
+}
+
+bool apply_shape(cem_sim *s, Device &D, int thin, bool side, int graph) {
+    const bool respace = thin != D.thin;
+    if (respace) {
+        D.thin = thin;
+        if (!build_spaces(s, D, 0) || !build_spaces(s, D, 1)) return false;
+        fill_args(s, D);
+    }
+    if (respace || graph != D.graph_steps) {
+        if (D.graph) cudaGraphExecDestroy(D.graph);
+        D.graph = nullptr;
+        D.graph_steps = graph;
+    }
+    D.side_on = side;
+    return true;
+}
+
+// device milliseconds per step of `n` steps (after `warm` untimed ones)
+bool shape_ms(cem_sim *s, long warm, long n, double *ms, long *used) {
+    Device &D = *s->dev;
+    if (!D.tev[0]) {
+        CB2_CHECK(s, cudaEventCreate(&D.tev[0]));
+        CB2_CHECK(s, cudaEventCreate(&D.tev[1]));
+    }
+    if (!run_steps(s, warm)) return false;
+    CB2_CHECK(s, cudaEventRecord(D.tev[0], D.stream));
+    if (!run_steps(s, n)) return false;
+    CB2_CHECK(s, cudaEventRecord(D.tev[1], D.stream));
+    CB2_CHECK(s, cudaEventSynchronize(D.tev[1]));
+    float f = 0;
+    CB2_CHECK(s, cudaEventElapsedTime(&f, D.tev[0], D.tev[1]));
+    *ms = f / n;
+    *used += warm + n;
+    return true;
+}
+
+// choose the launch shape of s (cache, else coordinate descent over the
+// choices, 576 steps); `used` returns the steps it ran
+bool tune_shape(cem_sim *s, long *used) {
+    Device &D = *s->dev;
+    const std::string key = shape_key(s);
+    std::lock_guard<std::mutex> lock(g_shape_mu);
+    load_shapes();
+    auto it = g_shapes.find(key);
+    D.tuned = true;
+    if (it != g_shapes.end()) {
+        D.tuned_from_cache = true;
+        D.tuned_ms = it->second[3];
+        return apply_shape(s, D, (int)it->second[0], it->second[1] != 0, (int)it->second[2]);
+    }
+    int thin = D.thin, graph = D.graph_steps;
+    bool side = D.side_on;
+    double best;
+    if (!shape_ms(s, 32, 64, &best, used)) return false;
+    auto trial = [&](int t, bool sd, int g) {
+        double ms;
+        if (!apply_shape(s, D, t, sd, g) || !shape_ms(s, 32, 64, &ms, used)) return false;
+        if (ms < 0.995 * best) { best = ms; thin = t; side = sd; graph = g; }
+        return apply_shape(s, D, thin, side, graph);
+    };
+    for (int t : {8, 32}) if (!trial(t, side, graph)) return false;
+    if (!trial(thin, !side, graph)) return false;
+    for (int g : {16, 64}) if (!trial(thin, side, g)) return false;
+    D.tuned_ms = best;
+    store_shape(key, {(double)thin, side ? 1.0 : 0.0, (double)graph, best});
+    return true;
+}
+
 }  // namespace
 
 int engine_step(cem_sim *s, long n) {
     if (n <= 0) return 0;
     if (!begin_device_op(s)) return -1;
+    Device &D = *s->dev;
+    if (D.tune && !D.tuned && !D.use_fused && n >= 2048 && !g_timer) {
+        long used = 0;
+        if (!tune_shape(s, &used)) return -1;
+        n -= used;
+    }
     if (!run_steps(s, n)) return -1;
     if (!end_device_op(s)) return -1;
     return 0;
@@ -3481,6 +3624,19 @@ bool batch_launch(cemx_batch *b, int n) {
 std::mutex g_tune_mu;
 std::map<std::string, std::pair<int, int>> g_tuned;
 
+// cache-file key of a batch composition: FNV-1a hash of its signature and the member count
+std::string batch_key(const std::string &sig) {
+    unsigned long long h = 1469598103934665603ull;
+    int members = 0;
+    for (char c : sig) {
+        h = (h ^ (unsigned char)c) * 1099511628211ull;
+        members += c == ';';
+    }
+    char k[64];
+    std::snprintf(k, sizeof k, "batch/%016llx/%d", h, members);
+    return k;
+}
+
 std::string batch_signature(const cemx_batch *b) {
     std::vector<std::string> v;
     for (int m : b->active) {
@@ -3603,6 +3759,30 @@ int cemx_use_fused(cem_sim *s, int on) {
     return prev;
 }
 
+int cemx_tune(cem_sim *s, int on) {
+    if (!s) { set_error("null simulation"); return -1; }
+    const int prev = s->dev ? (s->dev->tune ? 1 : 0) : (s->tune_choice >= 0 ? s->tune_choice : 0);
+    s->tune_choice = on ? 1 : 0;
+    if (s->dev) s->dev->tune = on != 0;
+    return prev;
+}
+
+int cemx_tune_state(const cem_sim *s, double *out, int n) {
+    if (!s || !out) { set_error("null argument"); return -1; }
+    double v[6] = {0, 0, 16, 1, 32, 0};
+    if (s->dev) {
+        const Device &D = *s->dev;
+        v[0] = D.tuned;
+        v[1] = D.tuned_from_cache;
+        v[2] = D.thin;
+        v[3] = D.side_on;
+        v[4] = D.graph_steps;
+        v[5] = D.tuned_ms;
+    }
+    for (int q = 0; q < n && q < 6; q++) out[q] = v[q];
+    return 0;
+}
+
 int cemx_energy_noalloc(cem_sim *s, double *out) {
     if (!s || !out) { set_error("cemx_energy_noalloc: null argument"); return -1; }
     if (!s->finalized) { set_error("not finalized"); return -1; }
@@ -3718,10 +3898,16 @@ int cemx_batch_run(cemx_batch *b, long max_steps) {
             const std::string sig = batch_signature(b);
             std::pair<int, int> best{b->chunk, b->order};
             bool cached = false;
-            {
+            {   // this process's choices, then the launch-shape cache file
                 std::lock_guard<std::mutex> lock(g_tune_mu);
                 auto it = g_tuned.find(sig);
                 if (it != g_tuned.end()) { best = it->second; cached = true; }
+            }
+            if (!cached) {
+                std::lock_guard<std::mutex> lock(g_shape_mu);
+                load_shapes();
+                auto it = g_shapes.find(batch_key(sig));
+                if (it != g_shapes.end()) { best = {(int)it->second[0], (int)it->second[1]}; cached = true; }
             }
             if (!cached) {
                 long minleft = max_steps - done;
@@ -3761,8 +3947,12 @@ int cemx_batch_run(cemx_batch *b, long max_steps) {
                         }
                         if (ms / ch < best_ms) { best_ms = ms / ch; best = {ch, order}; }
                     }
-                std::lock_guard<std::mutex> lock(g_tune_mu);
-                g_tuned[sig] = best;
+                {
+                    std::lock_guard<std::mutex> lock(g_tune_mu);
+                    g_tuned[sig] = best;
+                }
+                std::lock_guard<std::mutex> lock(g_shape_mu);
+                store_shape(batch_key(sig), {(double)best.first, (double)best.second, 0.0, best_ms});
             }
             b->tuned = true;
             if (b->order != best.second) { b->order = best.second; b->dirty = true; }

@@ -143,6 +143,7 @@ struct cem_sim {
     // With neither bit set the state is all zeros (freshly finalized).
     unsigned host_valid = 0, dev_valid = 0, exposed = 0;
     int kernel_choice = -1;   // -1: environment default, 0: separate H/E kernels, 1: fused
+    int tune_choice = -1;     // -1: environment default (CEM_B200_TUNE), 0: default launch shape, 1: tuned
 
     std::unique_ptr<cb2::Device, void (*)(cb2::Device *)> dev{nullptr, cb2::device_release};
 };

@@ -9,7 +9,8 @@ namespace cb2 {
 // The k axis of a node plane is cut into segments at `kb` (sorted, first 0,
 // last the end of the k range); one thread moves four consecutive k, and the
 // threads of a segment's rows follow one another. A segment thinner than four
-// groups (16 points) leaves most lanes of a warp on different rows, so it
+// groups (kThin = 16 points by default; the tuner tries others) leaves most
+// lanes of a warp on different rows, so it
 // joins a neighbour, whose class the joined range then takes. rank(ks, ke):
 // 2 when [ks, ke) reaches a z CPML slab (general kernel), 1 when it meets a
 // Debye box (lean Debye kernel, which also handles points outside the box),
@@ -19,8 +20,7 @@ namespace cb2 {
 // neighbours it may join, a Debye one is preferred, then a plain one, then a
 // CPML one (the thinner on a tie); with none it stays as it is.
 template <class Rank>
-void merge_thin_segments(std::vector<int> &kb, Rank rank) {
-    constexpr int kThin = 16;
+void merge_thin_segments(std::vector<int> &kb, Rank rank, int kThin = 16) {
     static const int cost[3] = {1, 0, 2};   // by rank: plain, box, slab
     for (bool changed = true; changed && kb.size() > 2;) {
         changed = false;

@@ -103,3 +103,33 @@ def test_batch_rejects_misuse(lib):
     assert b.run(100) == 0 and s.steps == 10
     b.destroy()
     s.destroy()
+
+
+@pytest.mark.gpu
+def test_launch_shape_tuner_chooses_caches_and_keeps_the_bits(lib, tmp_path, monkeypatch):
+    """cemx_tune: the first long cem_step call times the launch-shape choices
+    on the simulation's own steps and writes the choice for the grid shape to
+    the cache file; a second simulation of the same shape takes it from the
+    file; fields are the bits of an untuned run."""
+    cache = tmp_path / "shapes.txt"
+    monkeypatch.setenv("CEM_B200_TUNE_CACHE", str(cache))
+    from courant_b200 import boards
+    kw = dict(seed=77, cells=3e5, ports="lumped", nf=4, steps=3000)
+    plain, _ = boards.seeded_board(lib, **kw)
+    a, _ = boards.seeded_board(lib, **kw)
+    b, _ = boards.seeded_board(lib, **kw)
+    a.tune(True)
+    b.tune(True)
+    for x in (plain, a):
+        x.step(3000)
+    st = a.tuneState()
+    assert st["tuned"] and not st["from_cache"] and st["thin"] in (8, 16, 32) and st["graph_steps"] in (16, 32, 64)
+    lines = cache.read_text().splitlines()
+    assert len(lines) == 1 and lines[0].split()[0].startswith(f"{a.nx}x{a.ny}x{a.nz}/")
+    b.step(3000)
+    sb = b.tuneState()
+    assert sb["tuned"] and sb["from_cache"] and (sb["thin"], sb["graph_steps"]) == (st["thin"], st["graph_steps"])
+    for c in range(6):
+        assert np.array_equal(a.field(c), plain.field(c)) and np.array_equal(b.field(c), plain.field(c)), c
+    for x in (plain, a, b):
+        x.destroy()
