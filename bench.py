@@ -1,27 +1,32 @@
 #!/usr/bin/env python
 """Throughput benchmark of the FDTD time-stepping path (courant.h cem_step).
 
-Workload (default, the every-kernel lossy 2-port configuration): a grounded
-coplanar waveguide on a Djordjevic-Sarkar substrate (eps_r 4.3, tan d 0.02 at
-1 GHz) fitted by 6 Debye poles, 35 um copper with Huray-rough surface
-impedance (sigma 5.8e7 S/m), a 20 um solder mask (eps_r 3.5), 2D eigenmode
-ports, on a 416 x 161 x 86 (5.76 M cell) non-uniform grid with 8-cell CPML,
-400 DFT frequencies to 40 GHz. Synthetic geometry generated here; fields
-start at zero.
+Workload (default `c3`, the large configuration): a seeded 4-layer board from
+this package's generator (courant_b200/boards.py): three cores 0.2-1.0 mm
+thick with eps_r 3.0-4.5, each a 4-pole Djordjevic-Sarkar Debye fit; 20
+microstrip/stripline traces 0.1-0.5 mm wide with 45-degree jogs, 30
+through-vias, a ground plane with clearances; 2D eigenmode ports on the port
+trace; the reference's rule-based non-uniform mesh (restated in
+courant_b200/mesher.py) sized to about 1500 x 1000 x 64 cells (97 M); 8-cell
+CPML on five faces; 201 DFT frequencies to 20 GHz. Synthetic geometry from a
+recorded seed; fields start at zero. `c1` and `c2` are the GCPW lines of
+courant_b200/scenes.CONFIGS, `c3s` the generator at 500 x 349 x 64 (profiling).
 
 One benchmark step = `chunk` FDTD time steps (default 500, the run-control
-interval of the reference's GCPW driver). `value` = cell-updates per second
+interval of the reference's board runner). `value` = cell-updates per second
 (cells nx*ny*nz x time steps x ranks / max-over-ranks device time), timed
-with CUDA events on the engine's stream. The field state (~1.5 GB) exceeds
-L2, so no flush is needed between steps. `e2e` = the same metric through the
-C ABI for one whole excitation (40 000 steps) with the plan and state
-uploaded from host memory inside the timed region and the spectra read back
-to the host after every chunk.
+with CUDA events on the engine's stream. The state (about 12 GB for c3)
+exceeds L2, so no flush is needed between steps. `e2e` = the same metric
+through the C ABI for 10 000 steps with the plan and state uploaded from host
+memory inside the timed region and the spectra and energy read back to the
+host after every chunk.
 
-On one GPU the line also carries `batching` (a mix of seeded boards stepped
-one at a time with cem_step against one batch) and `serving` (a Poisson stream
-of board requests through the plain FIFO loop against the continuously
-batching server, p50/p95/p99 time-to-S-parameters and solves/hour).
+On one GPU the line also carries `batching` (the 96-board mix, bounded: both
+excitations of 12 boards of 5e4-8e6 cells, one run at a time against the
+batching server) and `serving` (Poisson request streams at 0.5 and 2 req/s,
+bounded to 10 requests each: the plain FIFO loop against the continuously
+batching server, p50/p95/p99 time-to-S-parameters and solves/hour); each
+names its bound.
 
 --impl reference times the reference's own CPU core (oracle/_ref, OpenMP on
 all host cores) on the same workload, a bounded sample of steps per
@@ -48,7 +53,7 @@ def _workloads() -> dict:
     from courant_b200 import scenes
     w = {k: dict(desc=v["desc"], kw=v["kw"], ref_chunk=200 if k == "c1" else 20) for k, v in scenes.CONFIGS.items()}
     w["c3"] = dict(desc="seeded 4-layer board, 4-pole Debye cores, 20 traces, 30 vias, mode ports, "
-                        "non-uniform mesh 1500x1014x64",
+                        "non-uniform mesh of about 1500x1000x64 cells",
                    board=dict(seed=2026, cells=96e6, ports="mode", nf=201, fmax=20e9, steps=30000,
                               target=(1500, 1000, 64)),
                    ref_chunk=1, e2e_steps=10000)
@@ -209,10 +214,9 @@ def run_reference(args) -> None:
 def _mix_requests(spec, nf):
     """serve.Request objects for (seed, cells, steps, excite) tuples: seeded
     boards of the large configuration's generator with 2D mode ports."""
-    import functools
     from courant_b200 import boards, serve
-    return [serve.Request(functools.partial(boards.seeded_board, seed=sd, cells=cl, ports="mode", nf=nf, excite=ex),
-                          int(st), tag=(sd, ex)) for sd, cl, st, ex in spec]
+    return [serve.Request(boards.SeededBoard(sd, cl, ports="mode", nf=nf, excite=ex), int(st), tag=(sd, ex))
+            for sd, cl, st, ex in spec]
 
 
 def _compare(lib, spec, arrivals, nf) -> dict:
@@ -225,7 +229,7 @@ def _compare(lib, spec, arrivals, nf) -> dict:
     t0 = time.perf_counter()
     plain = serve.plain_loop(lib, _mix_requests(spec, nf), list(arrivals))
     sp = serve.summary(plain, t0, time.perf_counter())
-    srv = serve.Server(lib, chunk=512, builders=8, finishers=8)
+    srv = serve.Server(lib, chunk=512, builders=8, finishers=8, planners=8)
     t0 = time.perf_counter()
     got = serve.serve_all(srv, _mix_requests(spec, nf), list(arrivals))
     t1 = time.perf_counter()

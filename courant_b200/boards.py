@@ -149,14 +149,23 @@ def realize(lay: Layout, Lx: float, Ly: float, feed: float) -> Geometry:
 def place_vias(geo: Geometry, lay: Layout, count: int) -> None:
     """The first `count` candidate positions that keep a via clear of every
     trace (0.2 mm) and of the board ends."""
+    # every trace segment as (x0, y0, x1, y1, half width)
+    seg = np.array([(x0, y0, x1, y1, w / 2) for _, w, pts in geo.traces
+                    for (x0, y0), (x1, y1) in zip(pts[:-1], pts[1:])], dtype=np.float64).reshape(-1, 5)
     out = []
     for (u, v), r in zip(lay.via_uv, lay.via_r):
         if len(out) >= count:
             break
         x, y = _snap(geo.end + u * (geo.Lx - 2 * geo.end)), _snap(0.03 * geo.Ly + v * 0.94 * geo.Ly)
-        ok = all(_dist_polyline(x, y, pts) > w / 2 + r + 0.2e-3 for _, w, pts in geo.traces)
-        ok = ok and all(math.hypot(x - a, y - b) > r + q + 0.3e-3 for a, b, q in out)
-        if ok:
+        if seg.size:
+            dx, dy = seg[:, 2] - seg[:, 0], seg[:, 3] - seg[:, 1]
+            L2 = dx * dx + dy * dy
+            t = np.clip(np.where(L2 > 0, ((x - seg[:, 0]) * dx + (y - seg[:, 1]) * dy) / np.where(L2 > 0, L2, 1), 0),
+                        0.0, 1.0)
+            d = np.hypot(x - seg[:, 0] - t * dx, y - seg[:, 1] - t * dy)
+            if np.any(d <= seg[:, 4] + r + 0.2e-3):
+                continue
+        if all(math.hypot(x - a, y - b) > r + q + 0.3e-3 for a, b, q in out):
             out.append((float(x), float(y), float(r)))
     geo.vias = out
 
@@ -217,19 +226,39 @@ def _mesh_z(geo, fmax, hmin, npml):
     return mesher.with_pml(mesher.mesh_axis(fz, hmin, h_air), npml, h_air / 2, lo=False, hi=True)
 
 
-def _search(f, lo, hi, target, increasing, iters=18):
-    """Bisection of a monotone integer-valued f for the argument giving `target`."""
-    best = None
+def _search(f, lo, hi, target, increasing, iters=10):
+    """Argument in [lo, hi] for which the monotone integer-valued f comes
+    closest to `target`: secant steps on log(arg) with the bracket kept, then
+    the best of those tried."""
+    import math as _m
+    tried = {}
+
+    def ev(v):
+        if v not in tried:
+            tried[v] = f(v)
+        return tried[v]
+    a, b = lo, hi
+    fa, fb = ev(a), ev(b)
+    x = _m.sqrt(a * b)
     for _ in range(iters):
-        mid = math.sqrt(lo * hi)
-        v = f(mid)
-        if best is None or abs(v - target) < abs(best[1] - target):
-            best = (mid, v)
-        if (v < target) == increasing:
-            lo = mid
+        fx = ev(x)
+        if fx == target:
+            break
+        if (fx < target) == increasing:
+            a, fa = x, fx
         else:
-            hi = mid
-    return best[0]
+            b, fb = x, fx
+        # secant on log(argument) against the value, inside the bracket
+        la, lb = _m.log(a), _m.log(b)
+        if fb != fa:
+            t = (target - fa) / (fb - fa)
+            nx_ = _m.exp(la + min(max(t, 0.05), 0.95) * (lb - la))
+        else:
+            nx_ = _m.sqrt(a * b)
+        if abs(_m.log(nx_ / x)) < 1e-9:
+            break
+        x = nx_
+    return min(tried, key=lambda v: (abs(tried[v] - target), v))
 
 
 def plan_mesh(lay: Layout, cells: float, fmax: float, npml: int, vias: int, feed: float,
@@ -243,7 +272,7 @@ def plan_mesh(lay: Layout, cells: float, fmax: float, npml: int, vias: int, feed
     nx_t, ny_t, nz_t = target
     probe = realize(lay, 0.1, 0.07, feed)
     h_air = min(mesher.lambda_over_20(fmax, 1.0), 200e-6)
-    hmin = _search(lambda h: len(_mesh_z(probe, fmax, h, npml)) - 1, 5e-6, h_air, nz_t, increasing=False)
+    hmin = _search(lambda h: len(_mesh_z(probe, fmax, h, npml)) - 1, 5e-6, h_air, nz_t, increasing=False, iters=14)
 
     def ny_of(Ly):
         geo = realize(lay, 1.5 * Ly, Ly, feed)
@@ -251,7 +280,7 @@ def plan_mesh(lay: Layout, cells: float, fmax: float, npml: int, vias: int, feed
         _, fy, _, h_air = axis_features(geo, fmax, hmin)
         return len(mesher.mesh_axis(fy, hmin, h_air)) - 1 + 2 * npml
 
-    Ly = _search(ny_of, 2e-3, 2.0, ny_t, increasing=True, iters=16)
+    Ly = _search(ny_of, 2e-3, 2.0, ny_t, increasing=True)
 
     def nx_of(Lx):
         geo = realize(lay, Lx, Ly, feed)
@@ -259,7 +288,7 @@ def plan_mesh(lay: Layout, cells: float, fmax: float, npml: int, vias: int, feed
         fx, _, _, h_air = axis_features(geo, fmax, hmin)
         return len(mesher.mesh_axis(fx, hmin, h_air)) - 1 + 2 * npml
 
-    Lx = _search(nx_of, 3e-3, 3.0, nx_t, increasing=True, iters=16)
+    Lx = _search(nx_of, 3e-3, 3.0, nx_t, increasing=True)
     geo = realize(lay, Lx, Ly, feed)
     place_vias(geo, lay, vias)
     fx, fy, fz, h_air = axis_features(geo, fmax, hmin)
@@ -330,6 +359,118 @@ def hammerstad_neff(w: float, h: float, er: float) -> float:
     return math.sqrt(e)
 
 
+@dataclass
+class BoardPlan:
+    """Everything of a seeded board that needs no solver library: node lines,
+    stackup, copper edge masks per layer, via cells, port placement. It is
+    plain numpy data, so a process pool can make it (the server's planners)
+    and any thread turn it into a simulation with board_sim()."""
+    seed: int
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    zl: np.ndarray
+    eps: np.ndarray
+    kl: list
+    layers: list          # (k plane, mask_u, mask_v)
+    via_cells: list       # (i0, j0, mask over cells i, j; L1 to L4)
+    ports: str
+    port: dict            # mode-port definition without dir/iSrc/iMon/xRef, or lumped placement
+    Lx: float
+    meta: dict
+    npml: int
+    nf: int
+    fmax: float
+    steps: int | None
+    cfl: float
+    excite: int
+
+
+def plan_board(seed: int, cells: float = 2e6, *, ports: str = "mode", nf: int = 32, fmax: float = 20e9,
+               steps: int | None = None, traces: int = 20, vias: int = 30, npml: int = 8, cfl: float = 0.99,
+               excite: int = 1, target: tuple | None = None) -> BoardPlan:
+    """The library-free part of seeded_board (its arguments, less the library)."""
+    ntr = max(3, min(traces, int(round((cells / 2e4) ** 0.5))))
+    nvia = max(2, min(vias, int(cells / 1e5)))
+    lay = draw_layout(seed, ntr, 4 * nvia)
+    feed = 4e-3 if ports == "mode" else 0.0
+    geo, hmin, x, y, z = plan_mesh(lay, cells, fmax, npml, nvia, feed, target)
+    nx, ny, nz = len(x) - 1, len(y) - 1, len(z) - 1
+    zl = geo.zl
+    kl = [_nearest(z, v) for v in zl]
+    # L2 plane with clearances, then the trace layers (the bottom copper is the PEC floor)
+    layers = [(kl[1], *_plane_masks(x, y, geo.clear))]
+    for layer in (2, 3):
+        sel = [(w, pts) for ly, w, pts in geo.traces if ly == layer]
+        if sel:
+            layers.append((kl[layer], *_trace_masks(x, y, sel)))
+    # via barrels: solid PEC cells inside the drill radius, L1 to L4 (boardsim.ts :281-297)
+    via_cells = []
+    for vx, vy, r in geo.vias:
+        i0, i1 = max(0, _nearest(x, vx - r) - 1), min(nx - 1, _nearest(x, vx + r) + 1)
+        j0, j1 = max(0, _nearest(y, vy - r) - 1), min(ny - 1, _nearest(y, vy + r) + 1)
+        cx = 0.5 * (x[i0:i1 + 1] + x[i0 + 1:i1 + 2])
+        cy = 0.5 * (y[j0:j1 + 1] + y[j0 + 1:j1 + 2])
+        inside = (cx[:, None] - vx) ** 2 + (cy[None, :] - vy) ** 2 <= r * r
+        if inside.any() and kl[3] > 0:
+            via_cells.append((i0, j0, inside))
+    _, w0, pts0 = geo.traces[0]
+    yc = pts0[0][1]
+    kh = kl[3]
+    if ports == "mode":
+        jl, jr = _nearest(y, yc - w0 / 2), _nearest(y, yc + w0 / 2)
+        ja = max(0, (jl if y[jl] <= yc - w0 / 2 else jl - 1) - 1)
+        jb = min(ny - 1, jr if y[jr] >= yc + w0 / 2 else jr + 1)
+        er_eff = float(np.average(geo.eps[1:], weights=np.diff(zl)[1:]))
+        port = dict(j0=0, j1=ny, k0=0, k1=nz, vj=_nearest(y, yc), vk0=kl[1], vk1=kh, vsign=-1, ja=ja, jb=jb,
+                    ka=kh - 1, kb=kh, f0=0.5 * fmax, neff0=hammerstad_neff(w0, float(zl[3] - zl[1]), er_eff))
+    else:
+        port = dict(j=_nearest(y, yc), k0=kl[1], k1=kh)
+    meta = {"seed": seed, "dims": (nx, ny, nz), "cells": nx * ny * nz, "excite": excite, "hmin": hmin,
+            "board_mm": (geo.Lx * 1e3, geo.Ly * 1e3), "traces": len(geo.traces), "vias": len(geo.vias),
+            "mesh": {a: mesher.report(v) for a, v in (("x", x), ("y", y), ("z", z))}}
+    return BoardPlan(seed, x, y, z, zl, np.asarray(geo.eps), kl, layers, via_cells, ports, port, geo.Lx, meta, npml,
+                     nf, fmax, steps, cfl, excite)
+
+
+def board_sim(c: Courant, b: BoardPlan):
+    """The finalized simulation of a board plan on library `c`, and its metadata."""
+    x, y, z = b.x, b.y, b.z
+    nx = len(x) - 1
+    s = c.createSim(x, y, z)
+    for f in (0, 1, 2, 3, 5):
+        s.setBoundary(f, CPML, b.npml)
+    fits = [c.fitDjordjevicSarkar(float(e), 0.02, 1e9, 1e8, b.fmax, 4) for e in b.eps]
+    s.setDebyePoles(fits[0].fp)
+    big = 1.0
+    for q in range(3):
+        s.materialBoxDebye(-big, big, -big, big, float(b.zl[q]), float(b.zl[q + 1]), fits[q])
+    for k, mu, mv in b.layers:
+        s.pecEdgesPlane(Z, k, mu, mv)
+    for i0, j0, inside in b.via_cells:
+        s.pecCells(i0, j0, 0, np.repeat(inside[:, :, None], b.kl[3], axis=2).astype(np.uint8))
+    tau = math.sqrt(6.9) / (math.pi * 1.25 * b.fmax)
+    freqs = np.linspace(b.fmax / b.nf, b.fmax, b.nf)
+    meta = dict(b.meta, tau=tau, freqs=freqs)
+    if b.ports == "mode":
+        mon = 2.5e-3
+        i1, i2 = b.npml + 2, nx - b.npml - 2
+        p1 = s.addModePort(dict(b.port, dir=1, iSrc=i1, iMon=_nearest(x, x[i1] + mon), xRef=0.0))
+        p2 = s.addModePort(dict(b.port, dir=-1, iSrc=i2, iMon=_nearest(x, x[i2] - mon) - 1, xRef=b.Lx))
+        s.setModeExcitation(p1 if b.excite == 1 else p2, 4.5 * tau, tau)
+        meta["modeports"] = [p1, p2]
+    else:
+        pt = b.port
+        p1 = s.addLumpedPort(Z, b.npml + 4, pt["j"], pt["k0"], pt["k1"], -1, 50.0)     # L2 ground to the L4 trace
+        p2 = s.addLumpedPort(Z, nx - b.npml - 4, pt["j"], pt["k0"], pt["k1"], -1, 50.0)
+        s.setGaussian(p1 if b.excite == 1 else p2, 1.0, 4.5 * tau, tau)
+        meta["ports"] = [p1, p2]
+    s.setFrequencies(freqs)
+    s.finalize(b.cfl)
+    meta["steps"] = int(b.steps if b.steps is not None else min(40000, max(4000, int(12 * tau / s.dt) * 10)))
+    return s, meta
+
+
 def seeded_board(c: Courant, seed: int, cells: float = 2e6, *, ports: str = "mode", nf: int = 32,
                  fmax: float = 20e9, steps: int | None = None, traces: int = 20, vias: int = 30,
                  npml: int = 8, cfl: float = 0.99, excite: int = 1, target: tuple | None = None):
@@ -339,67 +480,24 @@ def seeded_board(c: Courant, seed: int, cells: float = 2e6, *, ports: str = "mod
     small boards so features keep a few cells between them; `excite` (1 or
     2) picks the driven port, the two excitations of a full 2-port
     measurement."""
-    ntr = max(3, min(traces, int(round((cells / 2e4) ** 0.5))))
-    nvia = max(2, min(vias, int(cells / 1e5)))
-    lay = draw_layout(seed, ntr, 4 * nvia)
-    feed = 4e-3 if ports == "mode" else 0.0
-    geo, hmin, x, y, z = plan_mesh(lay, cells, fmax, npml, nvia, feed, target)
-    nx, ny, nz = len(x) - 1, len(y) - 1, len(z) - 1
-    s = c.createSim(x, y, z)
-    for f in (0, 1, 2, 3, 5):
-        s.setBoundary(f, CPML, npml)
-    fits = [c.fitDjordjevicSarkar(float(e), 0.02, 1e9, 1e8, fmax, 4) for e in geo.eps]
-    s.setDebyePoles(fits[0].fp)
-    big = 1.0
-    zl = geo.zl
-    for q in range(3):
-        s.materialBoxDebye(-big, big, -big, big, float(zl[q]), float(zl[q + 1]), fits[q])
-    kl = [_nearest(z, v) for v in zl]
-    # L2 plane with clearances, then the trace layers (the bottom copper is the PEC floor)
-    mu, mv = _plane_masks(x, y, geo.clear)
-    s.pecEdgesPlane(Z, kl[1], mu, mv)
-    for layer in (2, 3):
-        sel = [(w, pts) for ly, w, pts in geo.traces if ly == layer]
-        if sel:
-            mu, mv = _trace_masks(x, y, sel)
-            s.pecEdgesPlane(Z, kl[layer], mu, mv)
-    # via barrels: solid PEC cells inside the drill radius, L1 to L4 (boardsim.ts :281-297)
-    for vx, vy, r in geo.vias:
-        i0, i1 = max(0, _nearest(x, vx - r) - 1), min(nx - 1, _nearest(x, vx + r) + 1)
-        j0, j1 = max(0, _nearest(y, vy - r) - 1), min(ny - 1, _nearest(y, vy + r) + 1)
-        cx = 0.5 * (x[i0:i1 + 1] + x[i0 + 1:i1 + 2])
-        cy = 0.5 * (y[j0:j1 + 1] + y[j0 + 1:j1 + 2])
-        inside = (cx[:, None] - vx) ** 2 + (cy[None, :] - vy) ** 2 <= r * r
-        if inside.any() and kl[3] > 0:
-            s.pecCells(i0, j0, 0, np.repeat(inside[:, :, None], kl[3], axis=2).astype(np.uint8))
-    tau = math.sqrt(6.9) / (math.pi * 1.25 * fmax)
-    freqs = np.linspace(fmax / nf, fmax, nf)
-    _, w0, pts0 = geo.traces[0]
-    yc = pts0[0][1]
-    kh = kl[3]
-    meta = {"seed": seed, "dims": (nx, ny, nz), "cells": nx * ny * nz, "tau": tau, "freqs": freqs, "excite": excite,
-            "hmin": hmin, "board_mm": (geo.Lx * 1e3, geo.Ly * 1e3), "traces": len(geo.traces), "vias": len(geo.vias),
-            "mesh": {a: mesher.report(v) for a, v in (("x", x), ("y", y), ("z", z))}}
-    if ports == "mode":
-        jl, jr = _nearest(y, yc - w0 / 2), _nearest(y, yc + w0 / 2)
-        ja = max(0, (jl if y[jl] <= yc - w0 / 2 else jl - 1) - 1)
-        jb = min(ny - 1, jr if y[jr] >= yc + w0 / 2 else jr + 1)
-        er_eff = float(np.average(geo.eps[1:], weights=np.diff(zl)[1:]))
-        d = dict(j0=0, j1=ny, k0=0, k1=nz, vj=_nearest(y, yc), vk0=kl[1], vk1=kh, vsign=-1, ja=ja, jb=jb,
-                 ka=kh - 1, kb=kh, f0=0.5 * fmax, neff0=hammerstad_neff(w0, float(zl[3] - zl[1]), er_eff))
-        mon = 2.5e-3
-        i1 = npml + 2
-        i2 = nx - npml - 2
-        p1 = s.addModePort(dict(d, dir=1, iSrc=i1, iMon=_nearest(x, x[i1] + mon), xRef=0.0))
-        p2 = s.addModePort(dict(d, dir=-1, iSrc=i2, iMon=_nearest(x, x[i2] - mon) - 1, xRef=geo.Lx))
-        s.setModeExcitation(p1 if excite == 1 else p2, 4.5 * tau, tau)
-        meta["modeports"] = [p1, p2]
-    else:
-        p1 = s.addLumpedPort(Z, npml + 4, _nearest(y, yc), kl[1], kh, -1, 50.0)     # L2 ground to the L4 trace
-        p2 = s.addLumpedPort(Z, nx - npml - 4, _nearest(y, yc), kl[1], kh, -1, 50.0)
-        s.setGaussian(p1 if excite == 1 else p2, 1.0, 4.5 * tau, tau)
-        meta["ports"] = [p1, p2]
-    s.setFrequencies(freqs)
-    s.finalize(cfl)
-    meta["steps"] = int(steps if steps is not None else min(40000, max(4000, int(12 * tau / s.dt) * 10)))
-    return s, meta
+    return board_sim(c, plan_board(seed, cells, ports=ports, nf=nf, fmax=fmax, steps=steps, traces=traces, vias=vias,
+                                 npml=npml, cfl=cfl, excite=excite, target=target))
+
+
+class SeededBoard:
+    """A seeded board request in two parts: `plan()` (no library, picklable,
+    for a process pool) and `realize(lib, plan)` (board_sim); calling it with
+    a library does both."""
+
+    def __init__(self, seed: int, cells: float = 2e6, **kw):
+        self.seed, self.cells, self.kw = seed, cells, kw
+
+    def plan(self) -> BoardPlan:
+        return plan_board(self.seed, self.cells, **self.kw)
+
+    @staticmethod
+    def realize(c: Courant, plan: BoardPlan):
+        return board_sim(c, plan)
+
+    def __call__(self, c: Courant):
+        return board_sim(c, self.plan())

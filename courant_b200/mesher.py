@@ -72,17 +72,14 @@ def _fixed_lines(feat: AxisFeatures, h0: float) -> tuple[list, list]:
     return lines, refine
 
 
-def _size(x: np.ndarray, feat: AxisFeatures, refine: np.ndarray, h0: float, hmax: float, g: float) -> np.ndarray:
-    """The local cell-size cap of mesher.ts :91-97 at the points x."""
-
-    def dist(a, b):
-        return np.where(x < a, a - x, np.where(x > b, x - b, 0.0))
-
+def _size(x: np.ndarray, caps: np.ndarray, refine: np.ndarray, h0: float, hmax: float, g: float) -> np.ndarray:
+    """The local cell-size cap of mesher.ts :91-97 at the points x. caps: one
+    row (a, b, h) per max_cell region and per span (h = (b - a) / n)."""
     s = np.full(x.shape, hmax)
-    for a, b, h in feat.max_cell:
-        s = np.minimum(s, h + g * dist(a, b))
-    for a, b, n in feat.spans:
-        s = np.minimum(s, (b - a) / n + g * dist(a, b))
+    if caps.size:
+        a, b, h = caps[:, 0:1], caps[:, 1:2], caps[:, 2:3]
+        d = np.where(x < a, a - x, np.where(x > b, x - b, 0.0))
+        s = np.minimum(s, (h + g * d).min(axis=0))
     if refine.size:
         # nearest refinement point per sample: sorted search instead of a loop over all points
         idx = np.clip(np.searchsorted(refine, x), 1, refine.size - 1) if refine.size > 1 else np.zeros(x.shape, int)
@@ -98,12 +95,14 @@ def mesh_axis(feat: AxisFeatures, hmin: float, hmax: float, ratio: float = 1.3) 
     h0 = hmin
     lines, refine = _fixed_lines(feat, h0)
     refine = np.unique(np.asarray(refine, dtype=np.float64))
+    caps = np.array([(a, b, h) for a, b, h in feat.max_cell] + [(a, b, (b - a) / n) for a, b, n in feat.spans],
+                    dtype=np.float64).reshape(-1, 3)
     g = 0.8 * (ratio - 1)
     nodes = [lines[0]]
     for a, b in zip(lines[:-1], lines[1:]):
         M = max(64, math.ceil((b - a) / (h0 / 8)))
         xs = a + (b - a) * np.arange(M + 1) / M
-        inv = 1.0 / _size(xs, feat, refine, h0, hmax, g)
+        inv = 1.0 / _size(xs, caps, refine, h0, hmax, g)
         cum = np.concatenate([[0.0], np.cumsum((xs[1:] - xs[:-1]) * 0.5 * (inv[:-1] + inv[1:]))])
         I = cum[-1]
         n = max(1, math.ceil(I - 1e-6))

@@ -75,7 +75,7 @@ class Request:
 
 class Server:
     def __init__(self, lib: Courant, budget_bytes: float = 160e9, chunk: int = 512, builders: int = 4,
-                 finishers: int = 4, device: int = -1, tune: bool = True):
+                 finishers: int = 4, device: int = -1, tune: bool = True, planners: int = 0):
         self.lib = lib
         self.budget = int(budget_bytes)
         self.chunk = chunk
@@ -90,6 +90,15 @@ class Server:
         self.used = 0
         self.finished: list[Request] = []
         self.build_pool = ThreadPoolExecutor(builders)
+        # library-free board planning (requests whose build has .plan and
+        # .realize, boards.SeededBoard) in processes of their own, beside the
+        # builder threads: the mesher's Python work needs no library and
+        # would otherwise hold the interpreter lock the builders share
+        self.planners = None
+        if planners:
+            import multiprocessing
+            from concurrent.futures import ProcessPoolExecutor
+            self.planners = ProcessPoolExecutor(planners, mp_context=multiprocessing.get_context("spawn"))
         self.load_pool = ThreadPoolExecutor(2)
         self.finish_pool = ThreadPoolExecutor(finishers)
         self.loaded: list = []         # admitted and on the device, waiting to join the batch
@@ -107,7 +116,10 @@ class Server:
 
     def _build(self, r: Request):
         try:
-            sim, meta = r.build(self.lib)
+            if self.planners is not None and hasattr(r.build, "plan") and hasattr(r.build, "realize"):
+                sim, meta = r.build.realize(self.lib, self.planners.submit(r.build.plan).result())
+            else:
+                sim, meta = r.build(self.lib)
             r.built = time.perf_counter()
             r.cells = meta.get("cells", sim.nx * sim.ny * sim.nz)
             nbytes = footprint(sim)
@@ -234,6 +246,8 @@ class Server:
         self.build_pool.shutdown(wait=True)
         self.load_pool.shutdown(wait=True)
         self.finish_pool.shutdown(wait=True)
+        if self.planners is not None:
+            self.planners.shutdown(wait=True)
         self.batch.destroy()
 
 

@@ -142,3 +142,19 @@ def test_failed_batch_fails_its_requests_and_serving_goes_on(monkeypatch):
         assert srv.thread.is_alive() and srv.used == 0
     finally:
         srv.close()
+
+
+def test_board_plan_in_a_process_gives_the_same_board(lib):
+    """A seeded board planned in a spawned process (the server's planners)
+    and realized here has the plan of one built in one go."""
+    import multiprocessing
+    from concurrent.futures import ProcessPoolExecutor
+    from tests_util import cmp_plans
+    req = boards.SeededBoard(21, 8e4, ports="mode", nf=4)
+    with ProcessPoolExecutor(1, mp_context=multiprocessing.get_context("spawn")) as pool:
+        plan = pool.submit(req.plan).result()
+    a, ma = req.realize(lib, plan)
+    b, mb = req(lib)
+    assert ma["dims"] == mb["dims"] and cmp_plans(a.plan(), b.plan()) == []
+    a.destroy()
+    b.destroy()
