@@ -212,11 +212,22 @@ def run_reference(args) -> None:
 
 
 def _mix_requests(spec, nf):
-    """serve.Request objects for (seed, cells, steps, excite) tuples: seeded
-    boards of the large configuration's generator with 2D mode ports."""
+    """serve.Request objects for (seed, cells, steps, excite[, nports]) tuples:
+    seeded boards of the large configuration's generator with 2D mode ports
+    (2 unless the tuple names a count)."""
     from courant_b200 import boards, serve
-    return [serve.Request(boards.SeededBoard(sd, cl, ports="mode", nf=nf, excite=ex), int(st), tag=(sd, ex))
-            for sd, cl, st, ex in spec]
+    return [serve.Request(boards.SeededBoard(t[0], t[1], ports="mode", nf=nf, excite=t[3],
+                                             nports=t[4] if len(t) > 4 else 2), int(t[2]), tag=(t[0], t[3]))
+            for t in spec]
+
+
+def _same(a: dict | None, b: dict | None) -> bool:
+    """Two request results hold the same S-parameters, bit for bit."""
+    import numpy as np
+    if a is None or b is None:
+        return a is None and b is None
+    keys = [k for k in a if k.startswith("S")]
+    return keys == [k for k in b if k.startswith("S")] and all(np.array_equal(a[k], b[k]) for k in keys)
 
 
 def _compare(lib, spec, arrivals, nf) -> dict:
@@ -235,9 +246,7 @@ def _compare(lib, spec, arrivals, nf) -> dict:
     t1 = time.perf_counter()
     srv.close()
     ss = serve.summary(got, t0, t1)
-    same = all((a.result is None) == (g.result is None) and
-               (a.result is None or all(np.array_equal(a.result[k], g.result[k]) for k in ("S1", "S2")))
-               for a, g in zip(plain, got))
+    same = all(_same(a.result, g.result) for a, g in zip(plain, got))
     return {"requests": len(spec), "same_results": same, "plain_fifo": sp, "served": ss,
             "gpu_busy_s": srv.gpu_ms / 1e3,
             "solves_per_hour_vs_plain": ss["solves_per_hour"] / sp["solves_per_hour"] if sp["solves_per_hour"] else None}
@@ -267,21 +276,22 @@ def batch_compare(lib, boards_n: int, seed: int = 2026) -> dict:
 def serve_compare(lib, n: int, rates: list, seed: int = 7) -> dict:
     """Serving, the Poisson request stream bounded to `n` requests per rate:
     seeded boards of the large configuration's generator with cells
-    log-uniform in 1e5-2e7, 2 mode ports (port 1 driven), 16 frequencies,
+    log-uniform in 1e5-2e7, 1-4 mode ports (uniform; port 1 driven), 16 frequencies,
     steps uniform in 1 000-5 000 (a tenth of 10k-50k), arriving as a Poisson
     stream at each rate of the sweep; the plain FIFO loop against the
     continuously batching server under a 160 GB HBM budget. Times are wall
     clock from arrival to S-parameters."""
     import numpy as np
     out = {"bound": f"{n} requests per rate, rates {rates} of the 0.05-2 req/s sweep, steps 1k-5k instead of "
-                    "10k-50k, 2 ports (of 1-4), 16 frequencies", "rates": {}}
+                    "10k-50k, 16 frequencies", "rates": {}}
     for rate in rates:
         rng = np.random.Generator(np.random.PCG64(seed + int(rate * 1000)))
         cells = np.exp(rng.uniform(np.log(1e5), np.log(2e7), n))
         steps = rng.integers(1000, 5000, n)
         arr = np.cumsum(rng.exponential(1 / rate, n))
         arr -= arr[0]
-        spec = [(500 + q, float(cells[q]), int(steps[q]), 1) for q in range(n)]
+        nports = rng.integers(1, 5, n)
+        spec = [(500 + q, float(cells[q]), int(steps[q]), 1, int(nports[q])) for q in range(n)]
         out["rates"][str(rate)] = _compare(lib, spec, list(arr), nf=16)
     return out
 

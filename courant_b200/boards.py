@@ -26,10 +26,11 @@ Djordjevic-Sarkar (tan d 0.02 at 1 GHz) Debye fit sharing one set of poles
 traces of width 0.1-0.5 mm running along x with random 45-degree bends
 (centres, widths, jogs, clearances and vias on a 50 um routing grid),
 through-vias (L1 to L4) placed clear of the traces. Trace 0 (on L4) is the
-port trace: it runs straight through both port planes, and the board ends
-next to the port planes hold nothing but it and the L2 plane, so the port
-cross-sections are uniform. All randomness comes from numpy's PCG64 seeded
-with `seed`.
+port trace of ports 1 and 2: it runs straight through both port planes, and
+the board ends next to the port planes hold nothing but it and the L2 plane,
+so the port cross-sections are uniform. A board of 3 or 4 ports also runs the
+trace of the row farthest from trace 0 straight through, on L3, for ports 3
+and 4. All randomness comes from numpy's PCG64 seeded with `seed`.
 
 Size: the minimum cell and the board's extent are searched so that the mesh
 has about the requested number of cells with the 1500 x 1000 x 64 aspect of
@@ -109,8 +110,17 @@ def _snap(v: float) -> float:
     return round(v / GRID) * GRID
 
 
-def realize(lay: Layout, Lx: float, Ly: float, feed: float) -> Geometry:
+def second_port_trace(lay: Layout) -> int:
+    """The trace of ports 3 and 4: the one whose row lies farthest from trace 0's."""
+    return int(np.argmax(np.abs(lay.rows - lay.rows[0])))
+
+
+def realize(lay: Layout, Lx: float, Ly: float, feed: float, nports: int = 2) -> Geometry:
+    """The layout on a board of Lx x Ly: trace 0 (and, for 3 or 4 ports, the
+    second port trace, listed second) straight through both board ends, the
+    others with their jogs."""
     ntr = len(lay.widths)
+    t2 = second_port_trace(lay) if nports >= 3 else -1
     band = Ly / ntr
     end = max(0.06 * Lx, 3e-3)
     zl = np.concatenate([[0.0], np.cumsum(lay.cores)])
@@ -119,8 +129,9 @@ def realize(lay: Layout, Lx: float, Ly: float, feed: float) -> Geometry:
         w = max(GRID * 2, _snap(float(lay.widths[t])))
         y0 = _snap(float(lay.rows[t]) * Ly)
         layer = 3 if t % 2 == 0 else 2
-        if t == 0:
-            traces.append((layer, w, [(-feed - 1.0, y0), (Lx + feed + 1.0, y0)]))
+        if t == 0 or t == t2:
+            layer = 3 if t == 0 else 2                      # the second port trace is a stripline on L3
+            traces.insert(min(t, 1), (layer, w, [(-feed - 1.0, y0), (Lx + feed + 1.0, y0)]))
             continue
         xa, xb = end + 1e-3, Lx - end - 1e-3
         if xb <= xa:
@@ -262,7 +273,7 @@ def _search(f, lo, hi, target, increasing, iters=10):
 
 
 def plan_mesh(lay: Layout, cells: float, fmax: float, npml: int, vias: int, feed: float,
-              target: tuple | None = None):
+              target: tuple | None = None, nports: int = 2):
     """Minimum cell, board extent and node lines for about `cells` cells:
     hmin sets nz, then Ly sets ny and Lx sets nx (aspect 1.5 : 1)."""
     if target is None:
@@ -270,12 +281,12 @@ def plan_mesh(lay: Layout, cells: float, fmax: float, npml: int, vias: int, feed
         ny_t = math.sqrt(cells / nz_t / 1.5)
         target = (1.5 * ny_t, ny_t, nz_t)
     nx_t, ny_t, nz_t = target
-    probe = realize(lay, 0.1, 0.07, feed)
+    probe = realize(lay, 0.1, 0.07, feed, nports)
     h_air = min(mesher.lambda_over_20(fmax, 1.0), 200e-6)
     hmin = _search(lambda h: len(_mesh_z(probe, fmax, h, npml)) - 1, 5e-6, h_air, nz_t, increasing=False, iters=14)
 
     def ny_of(Ly):
-        geo = realize(lay, 1.5 * Ly, Ly, feed)
+        geo = realize(lay, 1.5 * Ly, Ly, feed, nports)
         place_vias(geo, lay, vias)
         _, fy, _, h_air = axis_features(geo, fmax, hmin)
         return len(mesher.mesh_axis(fy, hmin, h_air)) - 1 + 2 * npml
@@ -283,13 +294,13 @@ def plan_mesh(lay: Layout, cells: float, fmax: float, npml: int, vias: int, feed
     Ly = _search(ny_of, 2e-3, 2.0, ny_t, increasing=True)
 
     def nx_of(Lx):
-        geo = realize(lay, Lx, Ly, feed)
+        geo = realize(lay, Lx, Ly, feed, nports)
         place_vias(geo, lay, vias)
         fx, _, _, h_air = axis_features(geo, fmax, hmin)
         return len(mesher.mesh_axis(fx, hmin, h_air)) - 1 + 2 * npml
 
     Lx = _search(nx_of, 3e-3, 3.0, nx_t, increasing=True)
-    geo = realize(lay, Lx, Ly, feed)
+    geo = realize(lay, Lx, Ly, feed, nports)
     place_vias(geo, lay, vias)
     fx, fy, fz, h_air = axis_features(geo, fmax, hmin)
     hp = h_air / 2
@@ -359,6 +370,18 @@ def hammerstad_neff(w: float, h: float, er: float) -> float:
     return math.sqrt(e)
 
 
+def covered_neff(w: float, h: float, er: float, d: float, er_cover: float) -> float:
+    """Estimated effective index of a microstrip under a dielectric cover of
+    thickness d (air above it), the shift of its mode solve: Hammerstad's
+    filling factor q = (e_ms - 1) / (er - 1) splits the field between the
+    substrate and the half-space above; under an infinite cover that half-space
+    holds er_cover, and the air share of a finite cover decays as exp(-2 d / h)."""
+    e_ms = hammerstad_neff(w, h, er) ** 2
+    q = (e_ms - 1) / (er - 1)
+    e_full = q * er + (1 - q) * er_cover
+    return math.sqrt(e_full - (e_full - e_ms) * math.exp(-2 * d / h))
+
+
 @dataclass
 class BoardPlan:
     """Everything of a seeded board that needs no solver library: node lines,
@@ -375,7 +398,8 @@ class BoardPlan:
     layers: list          # (k plane, mask_u, mask_v)
     via_cells: list       # (i0, j0, mask over cells i, j; L1 to L4)
     ports: str
-    port: dict            # mode-port definition without dir/iSrc/iMon/xRef, or lumped placement
+    port: list            # per port: mode-port definition without dir/iSrc/iMon/xRef, or lumped placement;
+                          # "end" 0 (x-low) or 1 (x-high)
     Lx: float
     meta: dict
     npml: int
@@ -388,13 +412,15 @@ class BoardPlan:
 
 def plan_board(seed: int, cells: float = 2e6, *, ports: str = "mode", nf: int = 32, fmax: float = 20e9,
                steps: int | None = None, traces: int = 20, vias: int = 30, npml: int = 8, cfl: float = 0.99,
-               excite: int = 1, target: tuple | None = None) -> BoardPlan:
+               excite: int = 1, target: tuple | None = None, nports: int = 2) -> BoardPlan:
     """The library-free part of seeded_board (its arguments, less the library)."""
+    if not 1 <= nports <= 4 or not 1 <= excite <= nports:
+        raise ValueError(f"a board has 1 to 4 ports and drives one of them (nports {nports}, excite {excite})")
     ntr = max(3, min(traces, int(round((cells / 2e4) ** 0.5))))
     nvia = max(2, min(vias, int(cells / 1e5)))
     lay = draw_layout(seed, ntr, 4 * nvia)
     feed = 4e-3 if ports == "mode" else 0.0
-    geo, hmin, x, y, z = plan_mesh(lay, cells, fmax, npml, nvia, feed, target)
+    geo, hmin, x, y, z = plan_mesh(lay, cells, fmax, npml, nvia, feed, target, nports)
     nx, ny, nz = len(x) - 1, len(y) - 1, len(z) - 1
     zl = geo.zl
     kl = [_nearest(z, v) for v in zl]
@@ -414,19 +440,42 @@ def plan_board(seed: int, cells: float = 2e6, *, ports: str = "mode", nf: int = 
         inside = (cx[:, None] - vx) ** 2 + (cy[None, :] - vy) ** 2 <= r * r
         if inside.any() and kl[3] > 0:
             via_cells.append((i0, j0, inside))
-    _, w0, pts0 = geo.traces[0]
-    yc = pts0[0][1]
-    kh = kl[3]
-    if ports == "mode":
-        jl, jr = _nearest(y, yc - w0 / 2), _nearest(y, yc + w0 / 2)
-        ja = max(0, (jl if y[jl] <= yc - w0 / 2 else jl - 1) - 1)
-        jb = min(ny - 1, jr if y[jr] >= yc + w0 / 2 else jr + 1)
-        er_eff = float(np.average(geo.eps[1:], weights=np.diff(zl)[1:]))
-        port = dict(j0=0, j1=ny, k0=0, k1=nz, vj=_nearest(y, yc), vk0=kl[1], vk1=kh, vsign=-1, ja=ja, jb=jb,
-                    ka=kh - 1, kb=kh, f0=0.5 * fmax, neff0=hammerstad_neff(w0, float(zl[3] - zl[1]), er_eff))
-    else:
-        port = dict(j=_nearest(y, yc), k0=kl[1], k1=kh)
+    # ports: 1 and 2 at the x-low and x-high ends of trace 0 (L4), 3 and 4 at those of the
+    # second port trace (L3). The two traces are the only copper of the port planes but the
+    # L2 plane. A section holding both has two quasi-TEM modes: trace 0's ports keep the
+    # whole section (their shift lies near trace 0's mode, the lower index of the two), and
+    # the second trace's cross-section stops at a wall between the traces, one trace-0
+    # height beyond trace 0's strip edge (the midpoint at most), so that its solve sees
+    # one line.
+    ysplit = None
+    if nports >= 3:
+        (_, w0, p0), (_, _, p1) = geo.traces[0], geo.traces[1]
+        y0, y1 = p0[0][1], p1[0][1]
+        ysplit = y0 + math.copysign(min(w0 / 2 + float(zl[3] - zl[1]), abs(y1 - y0) / 2), y1 - y0)
+    port = []
+    for q in range(nports):
+        layer, w, pts = geo.traces[q // 2]
+        yc, kh = pts[0][1], kl[layer]
+        if ports == "mode":
+            jl, jr = _nearest(y, yc - w / 2), _nearest(y, yc + w / 2)
+            ja = max(0, (jl if y[jl] <= yc - w / 2 else jl - 1) - 1)
+            jb = min(ny - 1, jr if y[jr] >= yc + w / 2 else jr + 1)
+            j0, j1 = 0, ny
+            if q >= 2:
+                js = _nearest(y, ysplit)
+                j0, j1 = (js, ny) if yc > ysplit else (0, js)
+            if layer == 3:      # microstrip over cores 1 and 2
+                er = float(np.average(geo.eps[1:3], weights=np.diff(zl)[1:3]))
+                neff0 = hammerstad_neff(w, float(zl[3] - zl[1]), er)
+            else:               # core 1 below, core 2 over it, air above
+                neff0 = covered_neff(w, float(zl[2] - zl[1]), float(geo.eps[1]), float(zl[3] - zl[2]),
+                                     float(geo.eps[2]))
+            port.append(dict(j0=j0, j1=j1, k0=0, k1=nz, vj=_nearest(y, yc), vk0=kl[1], vk1=kh, vsign=-1, ja=ja,
+                             jb=jb, ka=kh - 1, kb=kh, f0=0.5 * fmax, neff0=neff0, end=q % 2))
+        else:
+            port.append(dict(j=_nearest(y, yc), k0=kl[1], k1=kh, end=q % 2))
     meta = {"seed": seed, "dims": (nx, ny, nz), "cells": nx * ny * nz, "excite": excite, "hmin": hmin,
+            "nports": nports,
             "board_mm": (geo.Lx * 1e3, geo.Ly * 1e3), "traces": len(geo.traces), "vias": len(geo.vias),
             "mesh": {a: mesher.report(v) for a, v in (("x", x), ("y", y), ("z", z))}}
     return BoardPlan(seed, x, y, z, zl, np.asarray(geo.eps), kl, layers, via_cells, ports, port, geo.Lx, meta, npml,
@@ -452,19 +501,24 @@ def board_sim(c: Courant, b: BoardPlan):
     tau = math.sqrt(6.9) / (math.pi * 1.25 * b.fmax)
     freqs = np.linspace(b.fmax / b.nf, b.fmax, b.nf)
     meta = dict(b.meta, tau=tau, freqs=freqs)
+    ids = []
     if b.ports == "mode":
         mon = 2.5e-3
         i1, i2 = b.npml + 2, nx - b.npml - 2
-        p1 = s.addModePort(dict(b.port, dir=1, iSrc=i1, iMon=_nearest(x, x[i1] + mon), xRef=0.0))
-        p2 = s.addModePort(dict(b.port, dir=-1, iSrc=i2, iMon=_nearest(x, x[i2] - mon) - 1, xRef=b.Lx))
-        s.setModeExcitation(p1 if b.excite == 1 else p2, 4.5 * tau, tau)
-        meta["modeports"] = [p1, p2]
+        for pt in b.port:
+            d = {k: v for k, v in pt.items() if k != "end"}
+            if pt["end"] == 0:
+                ids.append(s.addModePort(dict(d, dir=1, iSrc=i1, iMon=_nearest(x, x[i1] + mon), xRef=0.0)))
+            else:
+                ids.append(s.addModePort(dict(d, dir=-1, iSrc=i2, iMon=_nearest(x, x[i2] - mon) - 1, xRef=b.Lx)))
+        s.setModeExcitation(ids[b.excite - 1], 4.5 * tau, tau)
+        meta["modeports"] = ids
     else:
-        pt = b.port
-        p1 = s.addLumpedPort(Z, b.npml + 4, pt["j"], pt["k0"], pt["k1"], -1, 50.0)     # L2 ground to the L4 trace
-        p2 = s.addLumpedPort(Z, nx - b.npml - 4, pt["j"], pt["k0"], pt["k1"], -1, 50.0)
-        s.setGaussian(p1 if b.excite == 1 else p2, 1.0, 4.5 * tau, tau)
-        meta["ports"] = [p1, p2]
+        for pt in b.port:      # the L2 ground to the trace
+            i = b.npml + 4 if pt["end"] == 0 else nx - b.npml - 4
+            ids.append(s.addLumpedPort(Z, i, pt["j"], pt["k0"], pt["k1"], -1, 50.0))
+        s.setGaussian(ids[b.excite - 1], 1.0, 4.5 * tau, tau)
+        meta["ports"] = ids
     s.setFrequencies(freqs)
     s.finalize(b.cfl)
     meta["steps"] = int(b.steps if b.steps is not None else min(40000, max(4000, int(12 * tau / s.dt) * 10)))
@@ -473,15 +527,17 @@ def board_sim(c: Courant, b: BoardPlan):
 
 def seeded_board(c: Courant, seed: int, cells: float = 2e6, *, ports: str = "mode", nf: int = 32,
                  fmax: float = 20e9, steps: int | None = None, traces: int = 20, vias: int = 30,
-                 npml: int = 8, cfl: float = 0.99, excite: int = 1, target: tuple | None = None):
+                 npml: int = 8, cfl: float = 0.99, excite: int = 1, target: tuple | None = None,
+                 nports: int = 2):
     """Finalized board simulation and its metadata (dims, cells, ports,
     frequencies, step count, mesh report). `cells` sets the grid size (or
     `target` = (nx, ny, nz) directly); `traces` and `vias` scale down for
-    small boards so features keep a few cells between them; `excite` (1 or
-    2) picks the driven port, the two excitations of a full 2-port
-    measurement."""
+    small boards so features keep a few cells between them; `nports` (1 to
+    4) ports, 1 and 2 at the x-low and x-high ends of trace 0 (L4), 3 and 4
+    at those of trace 1 (L3); `excite` picks the driven port, one column of
+    the S-matrix per excitation."""
     return board_sim(c, plan_board(seed, cells, ports=ports, nf=nf, fmax=fmax, steps=steps, traces=traces, vias=vias,
-                                 npml=npml, cfl=cfl, excite=excite, target=target))
+                                 npml=npml, cfl=cfl, excite=excite, target=target, nports=nports))
 
 
 class SeededBoard:

@@ -243,21 +243,24 @@ def config_line(c: Courant, name: str, excite: int = 1, **over):
     return gcpw_line(c, **dict(CONFIGS[name]["kw"], excite=excite, **over))
 
 
-def two_port_s(s, meta: dict) -> dict:
-    """The excited column of the modal or lumped S-matrix: the waves at both
-    ports divided by the incident wave at the driven port. Mode ports use
+def s_column(s, meta: dict) -> dict:
+    """The excited column of the modal or lumped S-matrix: the waves at every
+    port divided by the incident wave at the driven port. Mode ports use
     cem_mode_port_waves (a, b at the reference planes, normalised to each port's
     own Z0); lumped ports use V and I with the 50-ohm port resistance."""
     e = meta.get("excite", 1) - 1
     if "modeports" in meta:
         w = [s.modePortWaves(p) for p in meta["modeports"]]
         a = w[e]["a"]
-        return {"b": [w[0]["b"] / a, w[1]["b"] / a], "z0": [w[0]["z0"], w[1]["z0"]], "beta": [w[0]["beta"], w[1]["beta"]]}
+        return {"b": [x["b"] / a for x in w], "z0": [x["z0"] for x in w], "beta": [x["beta"] for x in w]}
     v = [s.portV(p) for p in meta["ports"]]
     i = [s.portI(p) for p in meta["ports"]]
     sq = np.sqrt(50.0)
     a = (v[e] + 50.0 * i[e]) / (2 * sq)
-    return {"b": [(v[q] - 50.0 * i[q]) / (2 * sq) / a for q in range(2)]}
+    return {"b": [(v[q] - 50.0 * i[q]) / (2 * sq) / a for q in range(len(v))]}
+
+
+two_port_s = s_column
 
 
 def modeport_scene(c: Courant):

@@ -47,12 +47,14 @@ def footprint(sim: Sim) -> int:
 
 
 def results(sim: Sim, meta: dict) -> dict:
-    """The S-matrix column of the driven port e (meta["excite"]): "S1" = S_1e
-    and "S2" = S_2e, from the modal waves of mode ports or from the port
+    """The S-matrix column of the driven port e (meta["excite"]): "S<q>" =
+    S_qe for every port q, from the modal waves of mode ports or from the port
     spectra of lumped ports (50 ohm)."""
-    from .scenes import two_port_s
-    col = two_port_s(sim, meta)
-    return {"S1": col["b"][0], "S2": col["b"][1], "excite": meta.get("excite", 1)}
+    from .scenes import s_column
+    col = s_column(sim, meta)
+    out = {f"S{q + 1}": b for q, b in enumerate(col["b"])}
+    out["excite"] = meta.get("excite", 1)
+    return out
 
 
 @dataclass

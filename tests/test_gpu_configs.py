@@ -44,7 +44,7 @@ def column_errors(col, ref_run, excite):
     f = np.asarray(ref_run["freqs"])
     sel = f >= 1e9
     out = {}
-    for q in range(2):
+    for q in range(len(ref_run["S"])):
         g, r = np.asarray(col["b"][q])[sel], _c(ref_run["S"][q])[sel]
         name = f"S{q + 1}{excite}"
         transmit = q + 1 != excite
@@ -125,15 +125,17 @@ def test_c2_full_run_sparams(lib, excite):
     check(errs)
 
 
-@pytest.mark.parametrize("excite", [1, 2])
-def test_large_board_generator_scaled_against_reference(lib, ref_lib, excite):
+@pytest.mark.parametrize("nports,excite", [(2, 1), (2, 2), (4, 3), (1, 1)])
+def test_large_board_generator_scaled_against_reference(lib, ref_lib, nports, excite):
     """A board from the large configuration's generator (4-layer stackup with
     4-pole Debye cores, traces with 45-degree jogs, vias, plane clearances,
     rule-based non-uniform mesh, 2D mode ports) at 2.5e5 cells, 5 000 steps,
-    16 frequencies, both excitations: the modal S-matrix columns against the
-    reference core run on the same plan beside it, within the gate."""
+    16 frequencies: both excitations of the 2-port board, the second trace
+    driven on a 4-port one, and a 1-port one; the modal S-matrix columns
+    against the reference core run on the same plan beside it, within the
+    gate."""
     from courant_b200 import boards
-    kw = dict(seed=31, cells=2.5e5, ports="mode", nf=16, steps=5000, excite=excite)
+    kw = dict(seed=31, cells=2.5e5, ports="mode", nf=16, steps=5000, excite=excite, nports=nports)
     s, meta = boards.seeded_board(lib, **kw)
     r, mr = boards.seeded_board(ref_lib, **kw)
     assert meta["dims"] == mr["dims"] and meta["cells"] >= 2e5
@@ -144,5 +146,5 @@ def test_large_board_generator_scaled_against_reference(lib, ref_lib, excite):
     ref = {"freqs": list(meta["freqs"]),
            "S": [[[complex(v).real, complex(v).imag] for v in b] for b in rcol["b"]]}
     errs = column_errors(col, ref, excite)
-    print("board excite", excite, meta["dims"], errs)
+    print("board ports", nports, "excite", excite, meta["dims"], errs)
     check(errs)

@@ -38,15 +38,18 @@ def test_gcpw_plan_live_against_reference(lib, ref_lib):
     assert a.conductorFitError() == b.conductorFitError()
 
 
-@pytest.mark.parametrize("ports", ["mode", "lumped"])
-def test_seeded_board_plan_live_against_reference(lib, ref_lib, ports):
+@pytest.mark.parametrize("ports,nports,excite", [("mode", 2, 1), ("lumped", 2, 1), ("mode", 1, 1),
+                                                  ("mode", 3, 3), ("mode", 4, 2), ("lumped", 4, 4)])
+def test_seeded_board_plan_live_against_reference(lib, ref_lib, ports, nports, excite):
     """The seeded board generator builds the same plan on both libraries
     (4-pole Debye stackup, ground plane with clearances, staircased traces,
-    vias, mode or lumped ports)."""
+    vias, 1 to 4 mode or lumped ports, any of them driven)."""
     from courant_b200 import boards
-    a, ma = boards.seeded_board(ref_lib, 11, 6e4, ports=ports, nf=4)
-    b, mb = boards.seeded_board(lib, 11, 6e4, ports=ports, nf=4)
+    kw = dict(ports=ports, nf=4, nports=nports, excite=excite)
+    a, ma = boards.seeded_board(ref_lib, 11, 6e4, **kw)
+    b, mb = boards.seeded_board(lib, 11, 6e4, **kw)
     assert ma["dims"] == mb["dims"] and ma["steps"] == mb["steps"]
+    assert len(mb["modeports" if ports == "mode" else "ports"]) == nports
     pa, pb = a.plan(), b.plan()
     assert cmp_plans(pa, pb, skip=("modeSource",)) == []
     assert mode_source_diff(pa["modeSource"], pb["modeSource"]) < MODE_TOL
