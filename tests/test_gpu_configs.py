@@ -125,17 +125,20 @@ def test_c2_full_run_sparams(lib, excite):
     check(errs)
 
 
-@pytest.mark.parametrize("nports,excite", [(2, 1), (2, 2), (4, 3), (1, 1)])
-def test_large_board_generator_scaled_against_reference(lib, ref_lib, nports, excite):
+@pytest.mark.parametrize("seed,nports,excite", [(31, 2, 1), (31, 2, 2), (32, 4, 3), (31, 1, 1)])
+def test_large_board_generator_scaled_against_reference(lib, ref_lib, seed, nports, excite):
     """A board from the large configuration's generator (4-layer stackup with
     4-pole Debye cores, traces with 45-degree jogs, vias, plane clearances,
     rule-based non-uniform mesh, 2D mode ports) at 2.5e5 cells, 5 000 steps,
     16 frequencies: both excitations of the 2-port board, the second trace
     driven on a 4-port one, and a 1-port one; the modal S-matrix columns
     against the reference core run on the same plan beside it, within the
-    gate."""
+    gate. (The 4-port board is seed 32: on seed 31 the reference's own mode
+    solver does not converge for the second trace's port at one of the 16
+    frequencies within its 300 iterations, and this library's, which refines
+    its shift when an iteration stalls, does.)"""
     from courant_b200 import boards
-    kw = dict(seed=31, cells=2.5e5, ports="mode", nf=16, steps=5000, excite=excite, nports=nports)
+    kw = dict(seed=seed, cells=2.5e5, ports="mode", nf=16, steps=5000, excite=excite, nports=nports)
     s, meta = boards.seeded_board(lib, **kw)
     r, mr = boards.seeded_board(ref_lib, **kw)
     assert meta["dims"] == mr["dims"] and meta["cells"] >= 2e5
