@@ -141,6 +141,9 @@ struct StepArgs {
     const float *wsrc[2];    // mode-source weights of Ey and Ez on plane i_src
     const long long *dstep;
     const float *srcv;       // lumped Vs and modal Vm at this step's H time, FP32 (source_values)
+    // [H, E]: k ranges [zt[u][0], zt[u][1]) and [zt[u][2], zt[u][3]) (four-point groups) where the
+    // lean kernels' rows reach into a z CPML slab and take its auxiliaries (empty: they never do)
+    int zt[2][4];
     // thread spaces last: batched kernels stage the arguments before them
     Space sp[2][4];          // [H, E][kFast, kGeneral, kAll, kDebye]
     int p0[2], p1[2];        // interior node planes of H and E
@@ -829,9 +832,23 @@ __device__ __forceinline__ void e_vec(const StepArgs &a, int i, const RowPos &r,
     e_points<C, P>(a, i, j, k4, E + q, w, h2, h2m, h1, h1m, ev, mv, sv);
 }
 
+// whether the group at k4 of a lean kernel's row lies in a z tail (StepArgs::zt)
+__device__ __forceinline__ bool in_ztail(const int (&zt)[4], int k4) {
+    return (k4 >= zt[0] && k4 < zt[1]) || (k4 >= zt[2] && k4 < zt[3]);
+}
+
+// Where of a z-tail group: lean rows lie on interior planes outside the y
+// slabs, so only the z planes of the four points are looked up (the x and y
+// ones are -1 by construction, which the compiler sees)
+__device__ __forceinline__ Where ztail_where(const int *plane_z, int k4) {
+    const int4 pk = __ldg(reinterpret_cast<const int4 *>(plane_z + k4));
+    return Where{-1, -1, pk, -1, max(max(pk.x, pk.y), max(pk.z, pk.w)) >= 0};
+}
+
 // H component C at points k4 .. k4+3 of row (i, j) of a fast piece: the
-// short path of h_points (no auxiliaries), every rounding the same. All
-// lanes of the warp call it (the k+1 neighbours move by shuffle).
+// short path of h_points (no auxiliaries), every rounding the same; groups of
+// a z tail take h_points itself. All lanes of the warp call it (the k+1
+// neighbours move by shuffle).
 template <int C>
 __device__ __forceinline__ void h_lean(const StepArgs &a, int i, const RowPos &p) {
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
@@ -855,6 +872,10 @@ __device__ __forceinline__ void h_lean(const StepArgs &a, int i, const RowPos &p
     if (A1 == 2) e2n = next_k(e2, E2 + q, row && k4 + 4 <= nz, !p.cont);
     if (A2 == 2) e1n = next_k(e1, E1 + q, row && k4 + 4 <= nz, !p.cont);
     if (!row) return;
+    if (kz && in_ztail(a.zt[0], k4)) {
+        h_points<C>(a, i, j, k4, H + q, ztail_where(a.pml[2].plane_h, k4), e2, e2n, e1, e1n, h);
+        return;
+    }
     const float ci = __ldg(a.hc[0] + i), cj = __ldg(a.hc[1] + j);
     const float4 ck = ldg4(a.hc[2] + k4);
     float s = 0.f;
@@ -872,10 +893,11 @@ __device__ __forceinline__ void h_lean(const StepArgs &a, int i, const RowPos &p
 
 // E component C at points k4 .. k4+3 of row (i, j) of a fast piece: the
 // short path of e_points (material table, sources; no auxiliaries, no Debye
-// currents), every rounding the same
+// currents), every rounding the same; groups of a z tail take e_points itself
 template <int C>
 __device__ __forceinline__ void e_lean(const StepArgs &a, int i, const RowPos &p, const float2 sv) {
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
+    constexpr bool kz = A1 == 2 || A2 == 2;
     const int ny = a.g.n[1], nz = a.g.n[2];
     const int j = p.j, k4 = p.k4;
     const bool row = p.act && (C == 0 || i >= 1) && (C == 1 ? j < ny : (j >= 1 && j < ny));
@@ -899,6 +921,10 @@ __device__ __forceinline__ void e_lean(const StepArgs &a, int i, const RowPos &p
     if (A1 == 2) h2m = prev_k(h2, H2 + q, row && k4 > 0, first);
     if (A2 == 2) h1m = prev_k(h1, H1 + q, row && k4 > 0, first);
     if (!row) return;
+    if (kz && in_ztail(a.zt[1], k4)) {
+        e_points<C, 0>(a, i, j, k4, E + q, ztail_where(a.pml[2].plane_e, k4), h2, h2m, h1, h1m, ev, mv, sv);
+        return;
+    }
     const float ci = __ldg(a.ec[0] + i), cj = __ldg(a.ec[1] + j);
     const float4 ck = ldg4(a.ec[2] + k4);
     const int mi[4] = {(int)(mv.x & 0xffffu), (int)(mv.x >> 16), (int)(mv.y & 0xffffu), (int)(mv.y >> 16)};
@@ -1694,6 +1720,7 @@ struct Device {
     // component) in plane order; wl_start[u][i] is the first entry of plane i.
     Space sp[2][kSpaces]{};
     int p0[2] = {0, 0}, p1[2] = {0, 0};
+    int zt[2][4] = {};       // z CPML groups the lean kernels' rows reach (StepArgs::zt)
     DevBuf<int2> wl[2];
     std::vector<int> wl_start[2];
     DevBuf<float> wsrc[2];
@@ -1742,6 +1769,8 @@ struct Device {
     int thin = 16;
     bool side_on = true;
     int graph_steps = 32;
+    // the z CPML slabs run inside the lean kernels' rows (CEM_B200_ZTAIL=0: as general blocks)
+    bool ztail = true;
     bool tune = false, tuned = false, tuned_from_cache = false;
     double tuned_ms = 0;
     cudaEvent_t tev[2] = {nullptr, nullptr};   // tuner timing
@@ -2270,9 +2299,15 @@ int space_blocks(const Space &sp) { return (sp.t0[sp.n] + kBlock - 1) / kBlock; 
 // 4, so that the slab's k range holds every 4-point group that reaches into
 // it. The rows are cut at the inner edges of the y slabs and, for E, at the
 // boxes' rows. Interior planes: the longest run of node planes outside the
-// x slabs. A rectangle is general when its k range reaches a z slab, its rows
-// a y slab, or (E) it meets a Debye box whose planes meet the interior ones;
-// consecutive row ranges of one class and k range merge.
+// x slabs. A rectangle is general when its rows reach a y slab, or (E) it
+// meets a Debye box whose planes meet the interior ones, or its k range
+// reaches a z slab while the z slabs are not tails (below); consecutive row
+// ranges of one class and k range merge. Z tails (Device::ztail, when no such
+// box reaches a z slab's k range): k is not cut at the z slabs, so that a
+// row's points above the boxes form one piece up to the top, and the lean
+// kernel takes the slab's auxiliaries for the groups inside it (the general
+// kernel's point code, the same bits); a rectangle holding both z slab and
+// Debye points is general.
 bool build_spaces(cem_sim *s, Device &D, int u) {
     const Geom &g = D.g;
     const int nx = s->n[0], rows = s->n[1] + 1;
@@ -2305,11 +2340,24 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
     std::vector<int> kb{0, kmax}, jb{0, rows};
     auto kcut = [&](int c) { if (c > 0 && c < kmax) kb.push_back(c); };
     auto jcut = [&](int c) { if (c > 0 && c < rows) jb.push_back(c); };
+    for (int q = 0; q < 4; q++) D.zt[u][q] = 0;
     if (s->has_pml) {
         int r[2][2];
         pml_ranges(s, 2, u, r);
+        int zg[2][2] = {{0, 0}, {0, 0}};   // the slabs' group-aligned k ranges
+        bool tails = D.ztail;
         for (int sd = 0; sd < 2; sd++)
-            if (r[sd][1] >= r[sd][0]) { kcut(r[sd][0] / 4 * 4); kcut((r[sd][1] + 1 + 3) / 4 * 4); }
+            if (r[sd][1] >= r[sd][0]) {
+                zg[sd][0] = r[sd][0] / 4 * 4;
+                zg[sd][1] = (r[sd][1] + 1 + 3) / 4 * 4;
+                for (const int *bx : boxes)
+                    if (bx[2] < zg[sd][1] && bx[2] + bx[5] > zg[sd][0]) tails = false;
+            }
+        for (int sd = 0; sd < 2; sd++) {
+            if (zg[sd][1] <= zg[sd][0]) continue;
+            if (tails) { D.zt[u][2 * sd] = zg[sd][0]; D.zt[u][2 * sd + 1] = zg[sd][1]; }
+            else { kcut(zg[sd][0]); kcut(zg[sd][1]); }
+        }
         pml_ranges(s, 1, u, r);
         if (r[0][1] >= r[0][0]) jcut(r[0][1] + 1);
         if (r[1][1] >= r[1][0]) jcut(r[1][0]);
@@ -2334,6 +2382,7 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
     }, D.thin);
     struct Rect { int ks, ke, js, je; };
     std::vector<Rect> cls[kSpaces];
+    const bool tails = D.zt[u][1] > D.zt[u][0] || D.zt[u][3] > D.zt[u][2];
     for (size_t q = 0; q + 1 < kb.size(); q++) {
         const int ks = kb[q], ke = kb[q + 1];
         bool zs = false;
@@ -2341,10 +2390,11 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
         cls[kAll].push_back({ks, ke, 0, rows});
         for (size_t r = 0; r + 1 < jb.size(); r++) {
             const int js = jb[r], je = jb[r + 1];
-            bool pml = zs, deb = false;
+            bool pml = zs && !tails, deb = false;
             for (int j = js; j < je && !pml; j++) pml = slab(1, j);
             for (const int *bx : boxes)
                 deb = deb || (ke > bx[2] && ks < bx[2] + bx[5] && je > bx[1] && js < bx[1] + bx[4]);
+            if (zs && deb) pml = true;
             std::vector<Rect> &v = cls[pml ? kGeneral : (deb ? kDebye : kFast)];
             if (!v.empty() && v.back().ks == ks && v.back().je == js) v.back().je = je;
             else v.push_back({ks, ke, js, je});
@@ -2423,6 +2473,7 @@ void fill_args_for(cem_sim *s, Device &D, int cur) {
         for (int c = 0; c < kSpaces; c++) a.sp[u][c] = D.sp[u][c];
         a.p0[u] = D.p0[u];
         a.p1[u] = D.p1[u];
+        for (int q = 0; q < 4; q++) a.zt[u][q] = D.zt[u][q];
     }
     for (int c = 0; c < 3; c++) {
         a.E[c] = D.E[cur][c].p;
@@ -2572,6 +2623,7 @@ bool create_device_impl(cem_sim *s) {
     CB2_CHECK(s, cudaGetDevice(&D.device));
     if (const char *e = std::getenv("CEM_B200_FUSED")) D.use_fused = e[0] == '1';
     if (const char *e = std::getenv("CEM_B200_GRAPHS")) D.use_graphs = e[0] != '0';
+    if (const char *e = std::getenv("CEM_B200_ZTAIL")) D.ztail = e[0] != '0';
     if (s->kernel_choice >= 0) D.use_fused = s->kernel_choice == 1;
     if (const char *e = std::getenv("CEM_B200_TUNE")) D.tune = e[0] == '1';
     if (s->tune_choice >= 0) D.tune = s->tune_choice == 1;

@@ -133,3 +133,38 @@ def test_launch_shape_tuner_chooses_caches_and_keeps_the_bits(lib, tmp_path, mon
         assert np.array_equal(a.field(c), plain.field(c)) and np.array_equal(b.field(c), plain.field(c)), c
     for x in (plain, a, b):
         x.destroy()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["board", "lossy"])
+def test_z_tails_give_the_bits_of_general_blocks(lib, monkeypatch, which):
+    """The z CPML slab run inside the lean kernels' rows (z tails, the
+    default) and as separate general blocks (CEM_B200_ZTAIL=0) give the same
+    fields and spectra bit for bit, on a seeded board (z-high CPML above air,
+    Debye cores below) and on the lossy scene."""
+    from courant_b200 import boards
+
+    def make():
+        if which == "board":
+            return boards.seeded_board(lib, seed=78, cells=3e5, ports="mode", nf=4, steps=1200)
+        return scenes.lossy_scene(lib)
+    runs = []
+    for zt in ("1", "0"):
+        monkeypatch.setenv("CEM_B200_ZTAIL", zt)
+        s, meta = make()
+        s.step(1200)
+        runs.append((s, meta))
+    (a, ma), (b, _) = runs
+    za, zb = a.sizes(), b.sizes()
+    assert za["h_general_pts"] < zb["h_general_pts"]
+    if which == "board":
+        assert za["e_general_pts"] < zb["e_general_pts"]
+    for c in range(6):
+        assert np.array_equal(a.field(c), b.field(c)), c
+    if "modeports" in ma:
+        for p in ma["modeports"]:
+            assert np.array_equal(a.modePortWaves(p)["b"], b.modePortWaves(p)["b"])
+    for p in ma.get("ports", []):
+        assert np.array_equal(a.portV(p), b.portV(p))
+    a.destroy()
+    b.destroy()
