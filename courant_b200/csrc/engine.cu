@@ -1028,7 +1028,9 @@ __device__ __forceinline__ void e_debye(const StepArgs &a, int i, const RowPos &
 // Resident blocks (of kBlock threads) per SM the update kernels are
 // compiled for: register caps of 51 and 64 per thread for the general H and
 // E kernels at the default 10 and 8 (the rarer CPML and Debye paths spill a
-// little), 32 and 51 for the lean ones at 16 and 10
+// little), 40 and 64 for the lean ones at 12 and 8 (the z-tail path of the
+// lean kernels fits without spilling; at 16 and 10 it spills, and on the
+// large board the step is 5% slower)
 #ifndef CB2_H_MINBLOCKS
 #define CB2_H_MINBLOCKS 10
 #endif
@@ -1037,10 +1039,10 @@ __device__ __forceinline__ void e_debye(const StepArgs &a, int i, const RowPos &
 #endif
 
 #ifndef CB2_HF_MINBLOCKS
-#define CB2_HF_MINBLOCKS 16
+#define CB2_HF_MINBLOCKS 12
 #endif
 #ifndef CB2_EF_MINBLOCKS
-#define CB2_EF_MINBLOCKS 10
+#define CB2_EF_MINBLOCKS 8
 #endif
 
 // H on the fast rectangles of node planes [i0, i0 + gridDim.y); block x:
@@ -2372,17 +2374,18 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
         std::sort(v->begin(), v->end());
         v->erase(std::unique(v->begin(), v->end()), v->end());
     }
-    // thin k segments join a neighbour (spaces.hpp)
+    // thin k segments join a neighbour (spaces.hpp); with z tails a slab
+    // makes a segment general only together with Debye points
+    const bool tails = D.zt[u][1] > D.zt[u][0] || D.zt[u][3] > D.zt[u][2];
     merge_thin_segments(kb, [&](int ks, int ke) {
-        for (int k = ks; k < ke; k++)
-            if (slab(2, k)) return 2;
-        for (const int *bx : boxes)
-            if (ke > bx[2] && ks < bx[2] + bx[5]) return 1;
-        return 0;
+        bool zs = false, deb = false;
+        for (int k = ks; k < ke && !zs; k++) zs = slab(2, k);
+        for (const int *bx : boxes) deb = deb || (ke > bx[2] && ks < bx[2] + bx[5]);
+        if (zs && (!tails || deb)) return 2;
+        return deb ? 1 : 0;
     }, D.thin);
     struct Rect { int ks, ke, js, je; };
     std::vector<Rect> cls[kSpaces];
-    const bool tails = D.zt[u][1] > D.zt[u][0] || D.zt[u][3] > D.zt[u][2];
     for (size_t q = 0; q + 1 < kb.size(); q++) {
         const int ks = kb[q], ke = kb[q + 1];
         bool zs = false;

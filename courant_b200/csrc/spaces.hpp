@@ -11,14 +11,16 @@ namespace cb2 {
 // threads of a segment's rows follow one another. A segment thinner than four
 // groups (kThin = 16 points by default; the tuner tries others) leaves most
 // lanes of a warp on different rows, so it
-// joins a neighbour, whose class the joined range then takes. rank(ks, ke):
-// 2 when [ks, ke) reaches a z CPML slab (general kernel), 1 when it meets a
-// Debye box (lean Debye kernel, which also handles points outside the box),
-// 0 otherwise (lean kernel). A thin segment never joins a thick neighbour of
-// lower rank (that would move the whole thick segment to a costlier kernel:
-// a thin Debye box above a thick plain region stays thin); among the
-// neighbours it may join, a Debye one is preferred, then a plain one, then a
-// CPML one (the thinner on a tie); with none it stays as it is.
+// joins a neighbour, and the joined range takes its own class. rank(ks, ke):
+// 2 when [ks, ke) goes to the general kernel (it reaches a z CPML slab that
+// the lean kernels do not take, or holds both slab and Debye points), 1 when
+// it meets a Debye box (lean Debye kernel, which also handles points outside
+// the box), 0 otherwise (lean kernel). A thin segment never joins a thick
+// neighbour whose rank the joined range would exceed (that would move the
+// whole thick segment to a costlier kernel: a thin Debye box above a thick
+// plain region stays thin); among the neighbours it may join, the one whose
+// joined range is cheapest is taken (Debye, then plain, then general; the
+// thinner on a tie); with none it stays as it is.
 template <class Rank>
 void merge_thin_segments(std::vector<int> &kb, Rank rank, int kThin = 16) {
     static const int cost[3] = {1, 0, 2};   // by rank: plain, box, slab
@@ -26,13 +28,12 @@ void merge_thin_segments(std::vector<int> &kb, Rank rank, int kThin = 16) {
         changed = false;
         for (size_t q = 0; q + 1 < kb.size(); q++) {
             if (kb[q + 1] - kb[q] >= kThin) continue;
-            const int r = rank(kb[q], kb[q + 1]);
             int best = -1, best_cost = 99, best_w = 1 << 30;   // cut to erase, its cost, the neighbour's width
             for (int side = 0; side < 2; side++) {
                 if (side == 0 ? q == 0 : q + 2 >= kb.size()) continue;
                 const int a = side == 0 ? kb[q - 1] : kb[q + 1], b = side == 0 ? kb[q] : kb[q + 2];
                 const int nr = rank(a, b), nw = b - a;
-                const int joined = r > nr ? r : nr;
+                const int joined = rank(side == 0 ? a : kb[q], side == 0 ? kb[q + 1] : b);
                 if (nw >= kThin && joined > nr) continue;
                 if (cost[joined] < best_cost || (cost[joined] == best_cost && nw < best_w)) {
                     best = side == 0 ? (int)q : (int)q + 1;
