@@ -502,10 +502,10 @@ class Sim:
         return bool(self.c.ex.cemx_tune(self.h, int(on)))
 
     def tuneState(self) -> dict:
-        v = np.zeros(6)
-        self._check(self.c.ex.cemx_tune_state(self.h, _ptr(v), 6), "tune_state")
+        v = np.zeros(7)
+        self._check(self.c.ex.cemx_tune_state(self.h, _ptr(v), 7), "tune_state")
         return {"tuned": bool(v[0]), "from_cache": bool(v[1]), "thin": int(v[2]), "side_stream": bool(v[3]),
-                "graph_steps": int(v[4]), "ms_per_step": float(v[5])}
+                "graph_steps": int(v[4]), "ms_per_step": float(v[5]), "z_tails": bool(v[6])}
 
     def prepareDevice(self, device: int = -1):
         """Create the device state now rather than at the first step."""

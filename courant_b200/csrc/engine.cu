@@ -1771,7 +1771,11 @@ struct Device {
     int thin = 16;
     bool side_on = true;
     int graph_steps = 32;
-    // the z CPML slabs run inside the lean kernels' rows (CEM_B200_ZTAIL=0: as general blocks)
+    // the z CPML slabs run inside the lean kernels' rows (z tails) or as general blocks;
+    // by default tails from 2 M cells (CEM_B200_ZTAIL=0/1 forces): on smaller grids the lean
+    // and general kernels each fit in a wave or two and run side by side, and keeping the
+    // slab apart balances the two streams (121 x 62 x 40 line: 16.3 against 18.2 us per step;
+    // 1498 x 1014 x 64 board: 3.21 against 3.01 ms)
     bool ztail = true;
     bool tune = false, tuned = false, tuned_from_cache = false;
     double tuned_ms = 0;
@@ -2626,6 +2630,7 @@ bool create_device_impl(cem_sim *s) {
     CB2_CHECK(s, cudaGetDevice(&D.device));
     if (const char *e = std::getenv("CEM_B200_FUSED")) D.use_fused = e[0] == '1';
     if (const char *e = std::getenv("CEM_B200_GRAPHS")) D.use_graphs = e[0] != '0';
+    D.ztail = (long long)s->n[0] * s->n[1] * s->n[2] >= 2000000;
     if (const char *e = std::getenv("CEM_B200_ZTAIL")) D.ztail = e[0] != '0';
     if (s->kernel_choice >= 0) D.use_fused = s->kernel_choice == 1;
     if (const char *e = std::getenv("CEM_B200_TUNE")) D.tune = e[0] == '1';
@@ -3183,7 +3188,7 @@ bool run_steps(cem_sim *s, long n) {
 
 std::mutex g_shape_mu;
 bool g_shape_loaded = false;
-std::map<std::string, std::array<double, 4>> g_shapes;   // key -> thin, side, graph steps, ms per step
+std::map<std::string, std::array<double, 5>> g_shapes;   // key -> thin, side, graph steps, ms per step, z tails
 
 std::string shape_cache_path() {
     if (const char *p = std::getenv("CEM_B200_TUNE_CACHE")) return p;
@@ -3206,27 +3211,32 @@ void load_shapes() {   // g_shape_mu held
     g_shape_loaded = true;
     FILE *f = std::fopen(shape_cache_path().c_str(), "r");
     if (!f) return;
-    char key[200];
-    double v[4];
-    while (std::fscanf(f, "%199s %lf %lf %lf %lf", key, &v[0], &v[1], &v[2], &v[3]) == 5) g_shapes[key] = {v[0], v[1], v[2], v[3]};
+    // lines: key thin side graph ms [ztail] (lines without the z-tail choice keep the default)
+    char line[400], key[200];
+    while (std::fgets(line, sizeof line, f)) {
+        double v[5] = {0, 0, 0, 0, 1};
+        if (std::sscanf(line, "%199s %lf %lf %lf %lf %lf", key, &v[0], &v[1], &v[2], &v[3], &v[4]) >= 5)
+            g_shapes[key] = {v[0], v[1], v[2], v[3], v[4]};
+    }
     std::fclose(f);
 }
 
-void store_shape(const std::string &key, const std::array<double, 4> &v) {   // g_shape_mu held
+void store_shape(const std::string &key, const std::array<double, 5> &v) {   // g_shape_mu held
     g_shapes[key] = v;
     const std::string path = shape_cache_path();
     for (size_t q = 1; q < path.size(); q++)   // mkdir -p of the directory
         if (path[q] == '/') mkdir(path.substr(0, q).c_str(), 0755);
     if (FILE *f = std::fopen(path.c_str(), "a")) {
-        std::fprintf(f, "%s %g %g %g %.6g\n", key.c_str(), v[0], v[1], v[2], v[3]);
+        std::fprintf(f, "%s %g %g %g %.6g %g\n", key.c_str(), v[0], v[1], v[2], v[3], v[4]);
         std::fclose(f);
     }
 }
 
-bool apply_shape(cem_sim *s, Device &D, int thin, bool side, int graph) {
-    const bool respace = thin != D.thin;
+bool apply_shape(cem_sim *s, Device &D, int thin, bool side, int graph, bool ztail) {
+    const bool respace = thin != D.thin || ztail != D.ztail;
     if (respace) {
         D.thin = thin;
+        D.ztail = ztail;
         if (!build_spaces(s, D, 0) || !build_spaces(s, D, 1)) return false;
         fill_args(s, D);
     }
@@ -3259,7 +3269,7 @@ bool shape_ms(cem_sim *s, long warm, long n, double *ms, long *used) {
 }
 
 // choose the launch shape of s (cache, else coordinate descent over the
-// choices, 576 steps); `used` returns the steps it ran
+// choices, 672 steps); `used` returns the steps it ran
 bool tune_shape(cem_sim *s, long *used) {
     Device &D = *s->dev;
     const std::string key = shape_key(s);
@@ -3270,23 +3280,24 @@ bool tune_shape(cem_sim *s, long *used) {
     if (it != g_shapes.end()) {
         D.tuned_from_cache = true;
         D.tuned_ms = it->second[3];
-        return apply_shape(s, D, (int)it->second[0], it->second[1] != 0, (int)it->second[2]);
+        return apply_shape(s, D, (int)it->second[0], it->second[1] != 0, (int)it->second[2], it->second[4] != 0);
     }
     int thin = D.thin, graph = D.graph_steps;
-    bool side = D.side_on;
+    bool side = D.side_on, zt = D.ztail;
     double best;
     if (!shape_ms(s, 32, 64, &best, used)) return false;
-    auto trial = [&](int t, bool sd, int g) {
+    auto trial = [&](int t, bool sd, int g, bool z) {
         double ms;
-        if (!apply_shape(s, D, t, sd, g) || !shape_ms(s, 32, 64, &ms, used)) return false;
-        if (ms < 0.995 * best) { best = ms; thin = t; side = sd; graph = g; }
-        return apply_shape(s, D, thin, side, graph);
+        if (!apply_shape(s, D, t, sd, g, z) || !shape_ms(s, 32, 64, &ms, used)) return false;
+        if (ms < 0.995 * best) { best = ms; thin = t; side = sd; graph = g; zt = z; }
+        return apply_shape(s, D, thin, side, graph, zt);
     };
-    for (int t : {8, 32}) if (!trial(t, side, graph)) return false;
-    if (!trial(thin, !side, graph)) return false;
-    for (int g : {16, 64}) if (!trial(thin, side, g)) return false;
+    if (!trial(thin, side, graph, !zt)) return false;
+    for (int t : {8, 32}) if (!trial(t, side, graph, zt)) return false;
+    if (!trial(thin, !side, graph, zt)) return false;
+    for (int g : {16, 64}) if (!trial(thin, side, g, zt)) return false;
     D.tuned_ms = best;
-    store_shape(key, {(double)thin, side ? 1.0 : 0.0, (double)graph, best});
+    store_shape(key, {(double)thin, side ? 1.0 : 0.0, (double)graph, best, zt ? 1.0 : 0.0});
     return true;
 }
 
@@ -3824,7 +3835,7 @@ int cemx_tune(cem_sim *s, int on) {
 
 int cemx_tune_state(const cem_sim *s, double *out, int n) {
     if (!s || !out) { set_error("null argument"); return -1; }
-    double v[6] = {0, 0, 16, 1, 32, 0};
+    double v[7] = {0, 0, 16, 1, 32, 0, 1};
     if (s->dev) {
         const Device &D = *s->dev;
         v[0] = D.tuned;
@@ -3833,8 +3844,9 @@ int cemx_tune_state(const cem_sim *s, double *out, int n) {
         v[3] = D.side_on;
         v[4] = D.graph_steps;
         v[5] = D.tuned_ms;
+        v[6] = D.ztail;
     }
-    for (int q = 0; q < n && q < 6; q++) out[q] = v[q];
+    for (int q = 0; q < n && q < 7; q++) out[q] = v[q];
     return 0;
 }
 

@@ -63,9 +63,10 @@ CEM_API int cemx_use_fused(cem_sim *s, int on);
 /* Launch-shape tuner (no counterpart in the reference core). With tuning on,
  * the first cem_step call of at least 2048 steps on a simulation's device
  * state chooses its launch shape - the thin-segment threshold of the update
- * kernels' thread spaces (8, 16 or 32 points), general CPML blocks on a second
+ * kernels' thread spaces (8, 16 or 32 points), the z CPML slabs inside the
+ * lean kernels' rows or as general blocks, general CPML blocks on a second
  * stream or after the others, 16, 32 or 64 steps per replayed CUDA graph - by
- * timing about 576 of those steps under each choice in turn (every choice
+ * timing about 672 of those steps under each choice in turn (every choice
  * computes the same bits, so they are ordinary steps), and records the result
  * per grid shape (cells, poles, surface impedance, CPML faces) in a cache file,
  * $CEM_B200_TUNE_CACHE or ~/.cache/courant-b200/launch-shapes.txt, which later
@@ -75,7 +76,8 @@ CEM_API int cemx_tune(cem_sim *s, int on);
 
 /* The launch shape in use: out[0] tuned (0/1), out[1] taken from the cache,
  * out[2] thin-segment threshold, out[3] second stream (0/1), out[4] steps per
- * graph, out[5] tuned ms per step (0 if not tuned). Returns 0 or -1. */
+ * graph, out[5] tuned ms per step (0 if not tuned), out[6] z tails (the z
+ * CPML slabs inside the lean kernels' rows, 0/1). Returns 0 or -1. */
 CEM_API int cemx_tune_state(const cem_sim *s, double *out, int n);
 
 /* Stored electromagnetic energy of s, like cem_energy (no counterpart in the

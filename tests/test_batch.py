@@ -128,7 +128,8 @@ def test_launch_shape_tuner_chooses_caches_and_keeps_the_bits(lib, tmp_path, mon
     assert len(lines) == 1 and lines[0].split()[0].startswith(f"{a.nx}x{a.ny}x{a.nz}/")
     b.step(3000)
     sb = b.tuneState()
-    assert sb["tuned"] and sb["from_cache"] and (sb["thin"], sb["graph_steps"]) == (st["thin"], st["graph_steps"])
+    assert sb["tuned"] and sb["from_cache"]
+    assert (sb["thin"], sb["graph_steps"], sb["z_tails"]) == (st["thin"], st["graph_steps"], st["z_tails"])
     for c in range(6):
         assert np.array_equal(a.field(c), plain.field(c)) and np.array_equal(b.field(c), plain.field(c)), c
     for x in (plain, a, b):
