@@ -943,8 +943,8 @@ __device__ __forceinline__ void e_lean(const StepArgs &a, int i, const RowPos &p
 }
 
 // E component C at points k4 .. k4+3 of row (i, j) of a Debye piece: no
-// CPML auxiliary on a derivative axis, the points in or beside the
-// component's Debye box. The P pole currents of the four points are read
+// CPML auxiliary on a derivative axis but the z slab of a z tail (whose
+// groups take e_points), the points in or beside the component's Debye box. The P pole currents of the four points are read
 // once as float4 and kept in registers for both sum_p hk_p J_p and their own
 // update, then written once; beta_p/dt comes packed per table entry. Every
 // rounding is that of e_points.
@@ -982,6 +982,11 @@ __device__ __forceinline__ void e_debye(const StepArgs &a, int i, const RowPos &
     if (A1 == 2) h2m = prev_k(h2, H2 + q, row && k4 > 0, first);
     if (A2 == 2) h1m = prev_k(h1, H1 + q, row && k4 > 0, first);
     if (!row) return;
+    // a z tail above the box (tails exist only where no box reaches a z slab)
+    if ((A1 == 2 || A2 == 2) && in_ztail(a.zt[1], k4)) {
+        e_points<C, 0>(a, i, j, k4, E + q, ztail_where(a.pml[2].plane_e, k4), h2, h2m, h1, h1m, ev, mv, sv);
+        return;
+    }
     const float ci = __ldg(a.ec[0] + i), cj = __ldg(a.ec[1] + j);
     const float4 ck = ldg4(a.ec[2] + k4);
     const int mi[4] = {(int)(mv.x & 0xffffu), (int)(mv.x >> 16), (int)(mv.y & 0xffffu), (int)(mv.y >> 16)};
@@ -1777,6 +1782,9 @@ struct Device {
     // slab apart balances the two streams (121 x 62 x 40 line: 16.3 against 18.2 us per step;
     // 1498 x 1014 x 64 board: 3.21 against 3.01 ms)
     bool ztail = true;
+    // with z tails, E rows are not cut at the Debye boxes: a row that meets a box is one
+    // piece of the Debye space, air and tail included (CEM_B200_ROWS=0/1)
+    bool whole_rows = false;
     bool tune = false, tuned = false, tuned_from_cache = false;
     double tuned_ms = 0;
     cudaEvent_t tev[2] = {nullptr, nullptr};   // tuner timing
@@ -2368,9 +2376,12 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
         if (r[0][1] >= r[0][0]) jcut(r[0][1] + 1);
         if (r[1][1] >= r[1][0]) jcut(r[1][0]);
     }
+    const bool tails = D.zt[u][1] > D.zt[u][0] || D.zt[u][3] > D.zt[u][2];
     for (const int *bx : boxes) {
-        kcut(bx[2] / 4 * 4);
-        kcut((bx[2] + bx[5] + 3) / 4 * 4);
+        if (!(tails && D.whole_rows)) {
+            kcut(bx[2] / 4 * 4);
+            kcut((bx[2] + bx[5] + 3) / 4 * 4);
+        }
         jcut(bx[1]);
         jcut(bx[1] + bx[4]);
     }
@@ -2379,13 +2390,12 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
         v->erase(std::unique(v->begin(), v->end()), v->end());
     }
     // thin k segments join a neighbour (spaces.hpp); with z tails a slab
-    // makes a segment general only together with Debye points
-    const bool tails = D.zt[u][1] > D.zt[u][0] || D.zt[u][3] > D.zt[u][2];
+    // makes no segment general (the lean and Debye kernels take its groups)
     merge_thin_segments(kb, [&](int ks, int ke) {
         bool zs = false, deb = false;
         for (int k = ks; k < ke && !zs; k++) zs = slab(2, k);
         for (const int *bx : boxes) deb = deb || (ke > bx[2] && ks < bx[2] + bx[5]);
-        if (zs && (!tails || deb)) return 2;
+        if (zs && !tails) return 2;
         return deb ? 1 : 0;
     }, D.thin);
     struct Rect { int ks, ke, js, je; };
@@ -2401,7 +2411,6 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
             for (int j = js; j < je && !pml; j++) pml = slab(1, j);
             for (const int *bx : boxes)
                 deb = deb || (ke > bx[2] && ks < bx[2] + bx[5] && je > bx[1] && js < bx[1] + bx[4]);
-            if (zs && deb) pml = true;
             std::vector<Rect> &v = cls[pml ? kGeneral : (deb ? kDebye : kFast)];
             if (!v.empty() && v.back().ks == ks && v.back().je == js) v.back().je = je;
             else v.push_back({ks, ke, js, je});
@@ -2632,6 +2641,7 @@ bool create_device_impl(cem_sim *s) {
     if (const char *e = std::getenv("CEM_B200_GRAPHS")) D.use_graphs = e[0] != '0';
     D.ztail = (long long)s->n[0] * s->n[1] * s->n[2] >= 2000000;
     if (const char *e = std::getenv("CEM_B200_ZTAIL")) D.ztail = e[0] != '0';
+    if (const char *e = std::getenv("CEM_B200_ROWS")) D.whole_rows = e[0] == '1';
     if (s->kernel_choice >= 0) D.use_fused = s->kernel_choice == 1;
     if (const char *e = std::getenv("CEM_B200_TUNE")) D.tune = e[0] == '1';
     if (s->tune_choice >= 0) D.tune = s->tune_choice == 1;

@@ -1,7 +1,8 @@
 // Driver of tests/test_spaces.py: k segments of merge_thin_segments for a
 // column given on the command line: end, z-slab ranges and box ranges; a
-// negative END means z tails (a slab is general only together with box
-// points, and the slab is not cut), as engine.cu build_spaces ranks them.
+// negative END means z tails (the slab is not cut and makes no segment
+// general: the lean and Debye kernels take its groups), as engine.cu
+// build_spaces ranks them.
 // usage: spaces_case END S0 S1 B0 B1 [CUT ...]   (empty ranges: S0 = S1)
 #include <cstdio>
 #include <cstdlib>
@@ -16,7 +17,7 @@ int main(int argc, char **argv) {
     kb.push_back(end);
     cb2::merge_thin_segments(kb, [&](int ks, int ke) {
         const bool zs = ke > s0 && ks < s1, box = ke > b0 && ks < b1;
-        if (zs && (!tails || box)) return 2;
+        if (zs && !tails) return 2;
         return box ? 1 : 0;
     });
     for (int v : kb) printf("%d ", v);

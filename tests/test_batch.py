@@ -140,9 +140,11 @@ def test_launch_shape_tuner_chooses_caches_and_keeps_the_bits(lib, tmp_path, mon
 @pytest.mark.parametrize("which", ["board", "lossy"])
 def test_z_tails_give_the_bits_of_general_blocks(lib, monkeypatch, which):
     """The z CPML slab run inside the lean kernels' rows (z tails, the
-    default) and as separate general blocks (CEM_B200_ZTAIL=0) give the same
-    fields and spectra bit for bit, on a seeded board (z-high CPML above air,
-    Debye cores below) and on the lossy scene."""
+    default from 2 M cells, forced here), as separate general blocks
+    (CEM_B200_ZTAIL=0), and inside whole E rows of the Debye space
+    (CEM_B200_ROWS=1) give the same fields and spectra bit for bit, on a
+    seeded board (z-high CPML above air, Debye cores below) and on the lossy
+    scene."""
     from courant_b200 import boards
 
     def make():
@@ -150,22 +152,25 @@ def test_z_tails_give_the_bits_of_general_blocks(lib, monkeypatch, which):
             return boards.seeded_board(lib, seed=78, cells=3e5, ports="mode", nf=4, steps=1200)
         return scenes.lossy_scene(lib)
     runs = []
-    for zt in ("1", "0"):
+    for zt, rows in (("1", "0"), ("0", "0"), ("1", "1")):
         monkeypatch.setenv("CEM_B200_ZTAIL", zt)
+        monkeypatch.setenv("CEM_B200_ROWS", rows)
         s, meta = make()
         s.step(1200)
         runs.append((s, meta))
-    (a, ma), (b, _) = runs
+    (a, ma), (b, _), (w, _) = runs
     za, zb = a.sizes(), b.sizes()
     assert za["h_general_pts"] < zb["h_general_pts"]
     if which == "board":
         assert za["e_general_pts"] < zb["e_general_pts"]
-    for c in range(6):
-        assert np.array_equal(a.field(c), b.field(c)), c
-    if "modeports" in ma:
-        for p in ma["modeports"]:
-            assert np.array_equal(a.modePortWaves(p)["b"], b.modePortWaves(p)["b"])
-    for p in ma.get("ports", []):
-        assert np.array_equal(a.portV(p), b.portV(p))
-    a.destroy()
-    b.destroy()
+        assert w.sizes()["e_fast_pts"] < za["e_fast_pts"]     # whole rows: the air above the cores in the Debye space
+    for x in (b, w):
+        for c in range(6):
+            assert np.array_equal(a.field(c), x.field(c)), c
+        if "modeports" in ma:
+            for p in ma["modeports"]:
+                assert np.array_equal(a.modePortWaves(p)["b"], x.modePortWaves(p)["b"])
+        for p in ma.get("ports", []):
+            assert np.array_equal(a.portV(p), x.portV(p))
+    for x in (a, b, w):
+        x.destroy()

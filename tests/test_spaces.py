@@ -50,13 +50,13 @@ def test_thin_box_does_not_turn_a_thick_plain_segment_into_debye(case):
 
 def test_z_tails_keep_a_thin_box_out_of_the_slab_segment(case):
     # E of the lossy 2-port line with z tails (no cut at the slab): the thin Debye box stays
-    # apart instead of joining the thick air-and-slab segment, which would make both general
+    # apart instead of moving the thick air-and-slab segment into the Debye kernel
     assert case(-88, (76, 87), (0, 12), [12]) == [0, 12, 88]
     # a thin air segment between a thick box and the slab-and-air top joins the box (the Debye
     # kernel takes points outside the box), never making the top general
     assert case(-88, (76, 87), (0, 40), [40, 48]) == [0, 48, 88]
-    # a thin slab-and-air top above a thick box stays apart (joined, both would be general)
-    assert case(-88, (76, 87), (0, 76), [76]) == [0, 76, 88]
+    # a thin slab-and-air top above a thick box joins it (the Debye kernel takes the tail's groups)
+    assert case(-88, (76, 87), (0, 76), [76]) == [0, 88]
 
 
 def test_z_tails_large_board_columns(case):
