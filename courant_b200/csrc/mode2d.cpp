@@ -34,6 +34,9 @@
 #include "sim.hpp"
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -194,80 +197,107 @@ Row assemble_row(const cem_mode2d &m, const Coeffs &c, const Numbering &o, doubl
 
 // Complex band matrix in row-major storage: row r keeps columns
 // [r - kl, r + kl + ku] (the upper kl diagonals receive the pivoting fill),
-// as interleaved (re, im) doubles.
+// real and imaginary parts in two arrays of the same layout, so that the row
+// updates run as plain vector loops.
 struct Band {
     int n = 0, kl = 0, ku = 0, width = 0;
-    std::vector<double> a;
+    std::vector<double> re, im;
+    std::vector<double> lc;   // the multipliers again, column by column (kl complex per column), for the solves
     std::vector<int> piv;
-    double *at(int r, int c) { return &a[((size_t)r * width + (size_t)(c - r + kl)) * 2]; }
+    size_t at(int r, int c) const { return (size_t)r * width + (size_t)(c - r + kl); }
 };
+
+// dst -= l * src over len complex entries (split parts); the loop of the
+// elimination and of nothing else, cloned for AVX2 machines (no contraction:
+// every clone gives the same bits)
+__attribute__((target_clones("arch=x86-64-v3", "default")))
+void row_update(double *__restrict__ dr, double *__restrict__ di, const double *__restrict__ sr,
+                const double *__restrict__ si, double lr, double li, int len) {
+    for (int q = 0; q < len; q++) {
+        dr[q] -= lr * sr[q] - li * si[q];
+        di[q] -= lr * si[q] + li * sr[q];
+    }
+}
 
 // LU with partial pivoting, column by column; multipliers stay in the rows
 // they were computed for (interchanges apply from their step on).
 bool band_factor(Band &B) {
     const int n = B.n, kl = B.kl, reach = B.kl + B.ku;
+    double *re = B.re.data(), *im = B.im.data();
     B.piv.assign(n, 0);
+    B.lc.assign((size_t)n * kl * 2, 0.0);
     for (int j = 0; j < n; j++) {
         const int last = std::min(n - 1, j + kl), cmax = std::min(n - 1, j + reach);
         int p = j;
         double best = -1;
         for (int i = j; i <= last; i++) {
-            const double *x = B.at(i, j);
-            const double mag = std::hypot(x[0], x[1]);
+            const size_t x = B.at(i, j);
+            const double mag = std::hypot(re[x], im[x]);
             if (mag > best) { best = mag; p = i; }
         }
         B.piv[j] = p;
         if (!(best > 0)) return false;
         if (p != j) {
-            double *rj = B.at(j, j), *rp = B.at(p, j);
-            for (int q = 0; q < 2 * (cmax - j + 1); q++) std::swap(rj[q], rp[q]);
+            const size_t rj = B.at(j, j), rp = B.at(p, j);
+            for (int q = 0; q <= cmax - j; q++) {
+                std::swap(re[rj + q], re[rp + q]);
+                std::swap(im[rj + q], im[rp + q]);
+            }
         }
-        const double *pr = B.at(j, j);
-        const double den = pr[0] * pr[0] + pr[1] * pr[1];
-        const double ir = pr[0] / den, ii = -pr[1] / den;   // 1 / pivot
+        const size_t pr = B.at(j, j);
+        const double den = re[pr] * re[pr] + im[pr] * im[pr];
+        const double ir = re[pr] / den, ii = -im[pr] / den;   // 1 / pivot
         const int len = cmax - j;
         for (int i = j + 1; i <= last; i++) {
-            double *ri = B.at(i, j);
-            const double lr = ri[0] * ir - ri[1] * ii, li = ri[0] * ii + ri[1] * ir;
-            ri[0] = lr;
-            ri[1] = li;
+            const size_t ri = B.at(i, j);
+            const double lr = re[ri] * ir - im[ri] * ii, li = re[ri] * ii + im[ri] * ir;
+            re[ri] = lr;
+            im[ri] = li;
+            B.lc[((size_t)j * kl + (i - j - 1)) * 2] = lr;
+            B.lc[((size_t)j * kl + (i - j - 1)) * 2 + 1] = li;
             if (lr == 0 && li == 0) continue;
-            double *__restrict__ dst = ri + 2;
-            const double *__restrict__ src = pr + 2;
-            for (int q = 0; q < len; q++) {
-                const double sr = src[2 * q], si = src[2 * q + 1];
-                dst[2 * q] -= lr * sr - li * si;
-                dst[2 * q + 1] -= lr * si + li * sr;
-            }
+            row_update(re + ri + 1, im + ri + 1, re + pr + 1, im + pr + 1, lr, li, len);
         }
     }
     return true;
 }
 
-// x <- (L U)^-1 P x
-void band_solve(Band &B, std::vector<cplx> &x) {
+// x <- (L U)^-1 P x (complex products written out: (a + ib)(c + id) =
+// (ac - bd) + i(ad + bc), as std::complex forms them, without its NaN checks)
+void band_solve(const Band &B, std::vector<cplx> &xv) {
     const int n = B.n, kl = B.kl, reach = B.kl + B.ku;
+    const double *re = B.re.data(), *im = B.im.data();
+    double *x = reinterpret_cast<double *>(xv.data());
     for (int j = 0; j < n; j++) {
-        if (B.piv[j] != j) std::swap(x[j], x[B.piv[j]]);
-        const cplx xj = x[j];
-        if (xj == 0.0) continue;
-        for (int i = j + 1; i <= std::min(n - 1, j + kl); i++) {
-            const double *l = B.at(i, j);
-            x[i] -= cplx(l[0], l[1]) * xj;
+        const int p = B.piv[j];
+        if (p != j) {
+            std::swap(x[2 * j], x[2 * p]);
+            std::swap(x[2 * j + 1], x[2 * p + 1]);
+        }
+        const double xr = x[2 * j], xi = x[2 * j + 1];
+        if (xr == 0 && xi == 0) continue;
+        const double *l = B.lc.data() + (size_t)j * kl * 2;
+        const int m = std::min(n - 1, j + kl) - j;
+        double *y = x + 2 * (j + 1);
+        for (int q = 0; q < m; q++) {
+            y[2 * q] -= l[2 * q] * xr - l[2 * q + 1] * xi;
+            y[2 * q + 1] -= l[2 * q] * xi + l[2 * q + 1] * xr;
         }
     }
     for (int j = n - 1; j >= 0; j--) {
         const int cmax = std::min(n - 1, j + reach);
-        const double *row = B.at(j, j);
-        double sr = x[j].real(), si = x[j].imag();
+        const size_t row = B.at(j, j);
+        double sr = x[2 * j], si = x[2 * j + 1];
         for (int q = 1; q <= cmax - j; q++) {
-            const double ar = row[2 * q], ai = row[2 * q + 1];
-            const double xr = x[j + q].real(), xi = x[j + q].imag();
+            const double ar = re[row + q], ai = im[row + q];
+            const double xr = x[2 * (j + q)], xi = x[2 * (j + q) + 1];
             sr -= ar * xr - ai * xi;
             si -= ar * xi + ai * xr;
         }
-        const double den = row[0] * row[0] + row[1] * row[1];
-        x[j] = cplx((sr * row[0] + si * row[1]) / den, (si * row[0] - sr * row[1]) / den);
+        const double dr = re[row], di = im[row];
+        const double den = dr * dr + di * di;
+        x[2 * j] = (sr * dr + si * di) / den;
+        x[2 * j + 1] = (si * dr - sr * di) / den;
     }
 }
 
@@ -277,10 +307,14 @@ double norm2(const std::vector<cplx> &x) {
     return std::sqrt(s);
 }
 
-cplx inner(const std::vector<cplx> &a, const std::vector<cplx> &b) {   // sum conj(a) b
-    cplx s = 0;
-    for (size_t q = 0; q < a.size(); q++) s += std::conj(a[q]) * b[q];
-    return s;
+cplx inner(const std::vector<cplx> &a, const std::vector<cplx> &b) {   // sum conj(a) b, written out
+    double sr = 0, si = 0;
+    for (size_t q = 0; q < a.size(); q++) {
+        const double ar = a[q].real(), ai = a[q].imag(), br = b[q].real(), bi = b[q].imag();
+        sr += ar * br - -ai * bi;
+        si += ar * bi + -ai * br;
+    }
+    return cplx(sr, si);
 }
 
 // h = Q e / beta for the API's H_u, H_v arrays
@@ -418,17 +452,22 @@ int cem_mode2d_solve(cem_mode2d *m, double f, double neff_guess, const double *s
     B.width = 2 * half + half + 1;
     // LU of A - shift I
     auto factor = [&](cplx shift) {
-        B.a.assign((size_t)n * B.width * 2, 0.0);
+        B.re.assign((size_t)n * B.width, 0.0);
+        B.im.assign((size_t)n * B.width, 0.0);
         for (int g = 0; g < n; g++)
             for (int q = 0; q < rows[g].n; q++) {
                 const cplx v = rows[g].val[q] - (rows[g].col[q] == g ? shift : cplx(0.0));
-                double *e = B.at(g, rows[g].col[q]);
-                e[0] += v.real();
-                e[1] += v.imag();
+                const size_t e = B.at(g, rows[g].col[q]);
+                B.re[e] += v.real();
+                B.im[e] += v.imag();
             }
         return band_factor(B);
     };
+    static const bool trace = [] { const char *e = std::getenv("CEM_B200_TRACE"); return e && e[0] == '1'; }();
+    const auto t0 = std::chrono::steady_clock::now();
+    int iters = 0, factors = 1;
     if (!factor(sigma)) return -1;
+    const double t_factor = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 
     // start vector: the given field (API layout: E_u then E_v, complex) or a fixed pseudo-random one
     std::vector<cplx> x(n), y(n);
@@ -453,6 +492,7 @@ int cem_mode2d_solve(cem_mode2d *m, double f, double neff_guess, const double *s
     auto iterate = [&](cplx shift, int its) {
         cplx lam_prev = 0;
         for (int it = 0; it < its; it++) {
+            iters++;
             y = x;
             band_solve(B, y);
             const cplx mu = inner(x, y);
@@ -463,7 +503,12 @@ int cem_mode2d_solve(cem_mode2d *m, double f, double neff_guess, const double *s
             const cplx ph = inner(y, x);
             const cplx rot = std::abs(ph) > 0 ? ph / std::abs(ph) : cplx(1.0);
             double d = 0;
-            for (int g = 0; g < n; g++) d += std::norm(y[g] * rot - x[g]);
+            for (int g = 0; g < n; g++) {
+                const double yr = y[g].real(), yi = y[g].imag();
+                const double dr = (yr * rot.real() - yi * rot.imag()) - x[g].real();
+                const double di = (yr * rot.imag() + yi * rot.real()) - x[g].imag();
+                d += dr * dr + di * di;
+            }
             x.swap(y);
             if (it >= 2 && std::abs(lam - lam_prev) < tol * std::abs(lam) && std::sqrt(d) < 1e-10) return true;
             lam_prev = lam;
@@ -478,6 +523,7 @@ int cem_mode2d_solve(cem_mode2d *m, double f, double neff_guess, const double *s
     // the eigenvalue the other modes fall away at once.
     for (int refine = 0; rc == 1 && refine < 3; refine++) {
         const cplx shift = lam;
+        factors++;
         if (!factor(shift)) break;
         if (iterate(shift, 60)) rc = 0;
     }
@@ -492,6 +538,10 @@ int cem_mode2d_solve(cem_mode2d *m, double f, double neff_guess, const double *s
         const int pt = o.where[g] >> 1;
         ((o.where[g] & 1) ? m->ev : m->eu)[pt] = x[g] * fix;
     }
+    if (trace)
+        std::fprintf(stderr, "courant-b200: mode solve f %.4g GHz n %d half %d: first factor %.3f s, %d factors, "
+                     "%d iterations, %.3f s in all, rc %d\n", f * 1e-9, n, half, t_factor, factors, iters,
+                     std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(), rc);
     cplx bt = std::sqrt(lam);
     if (bt.real() < 0) bt = -bt;
     m->beta = bt;
