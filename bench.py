@@ -24,7 +24,7 @@ host after every chunk.
 On one GPU the line also carries `batching` (the 96-board mix, bounded: both
 excitations of 12 boards of 5e4-8e6 cells, one run at a time against the
 batching server) and `serving` (Poisson request streams at 0.5 and 2 req/s,
-bounded to 16 requests each: the plain FIFO loop against the continuously
+bounded to 24 requests each: the plain FIFO loop against the continuously
 batching server, p50/p95/p99 time-to-S-parameters and solves/hour); each
 names its bound.
 
@@ -495,7 +495,7 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-runs", type=int, default=12,
                     help="boards (two excitations each) in the batched-vs-plain comparison (0: skip)")
-    ap.add_argument("--serve-requests", type=int, default=16, help="requests per rate in the serving comparison (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=24, help="requests per rate in the serving comparison (0: skip)")
     ap.add_argument("--serve-rates", default="0.5,2", help="Poisson arrival rates of the serving comparison, 1/s")
     args = ap.parse_args()
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
