@@ -1782,6 +1782,11 @@ struct Device {
     // slab apart balances the two streams (121 x 62 x 40 line: 16.3 against 18.2 us per step;
     // 1498 x 1014 x 64 board: 3.21 against 3.01 ms)
     bool ztail = true;
+    // z tails as rectangles of their own in the lean space (the default; CEM_B200_ZTAIL=1:
+    // inside the rows' other pieces): a row's slab groups follow its other groups in the
+    // same launch, but no warp mixes the two paths (lossy 2-port line: 154.5 against 165.3 us
+    // per step; the large boards equal)
+    bool ztail_split = true;
     // with z tails, E rows are not cut at the Debye boxes: a row that meets a box is one
     // piece of the Debye space, air and tail included (CEM_B200_ROWS=0/1)
     bool whole_rows = false;
@@ -2317,11 +2322,11 @@ int space_blocks(const Space &sp) { return (sp.t0[sp.n] + kBlock - 1) / kBlock; 
 // meets a Debye box whose planes meet the interior ones, or its k range
 // reaches a z slab while the z slabs are not tails (below); consecutive row
 // ranges of one class and k range merge. Z tails (Device::ztail, when no such
-// box reaches a z slab's k range): k is not cut at the z slabs, so that a
-// row's points above the boxes form one piece up to the top, and the lean
-// kernel takes the slab's auxiliaries for the groups inside it (the general
-// kernel's point code, the same bits); a rectangle holding both z slab and
-// Debye points is general.
+// box reaches a z slab's k range): the z slabs make no rectangle general; the
+// lean (and Debye) kernels take the slab's auxiliaries for the groups inside
+// it (the general kernel's point code, the same bits). The slab's groups are
+// rectangles of their own in the lean space (Device::ztail_split, cut after
+// the thin merges) or pieces of the rows above the boxes.
 bool build_spaces(cem_sim *s, Device &D, int u) {
     const Geom &g = D.g;
     const int nx = s->n[0], rows = s->n[1] + 1;
@@ -2398,6 +2403,12 @@ bool build_spaces(cem_sim *s, Device &D, int u) {
         if (zs && !tails) return 2;
         return deb ? 1 : 0;
     }, D.thin);
+    if (tails && D.ztail_split) {   // the slabs' groups as segments of their own, after the thin merges
+        for (int q = 0; q < 4; q += 2)
+            if (D.zt[u][q + 1] > D.zt[u][q]) { kcut(D.zt[u][q]); kcut(D.zt[u][q + 1]); }
+        std::sort(kb.begin(), kb.end());
+        kb.erase(std::unique(kb.begin(), kb.end()), kb.end());
+    }
     struct Rect { int ks, ke, js, je; };
     std::vector<Rect> cls[kSpaces];
     for (size_t q = 0; q + 1 < kb.size(); q++) {
@@ -2640,7 +2651,10 @@ bool create_device_impl(cem_sim *s) {
     if (const char *e = std::getenv("CEM_B200_FUSED")) D.use_fused = e[0] == '1';
     if (const char *e = std::getenv("CEM_B200_GRAPHS")) D.use_graphs = e[0] != '0';
     D.ztail = (long long)s->n[0] * s->n[1] * s->n[2] >= 2000000;
-    if (const char *e = std::getenv("CEM_B200_ZTAIL")) D.ztail = e[0] != '0';
+    if (const char *e = std::getenv("CEM_B200_ZTAIL")) {
+        D.ztail = e[0] != '0';
+        D.ztail_split = e[0] != '1';
+    }
     if (const char *e = std::getenv("CEM_B200_ROWS")) D.whole_rows = e[0] == '1';
     if (s->kernel_choice >= 0) D.use_fused = s->kernel_choice == 1;
     if (const char *e = std::getenv("CEM_B200_TUNE")) D.tune = e[0] == '1';

@@ -139,10 +139,11 @@ def test_launch_shape_tuner_chooses_caches_and_keeps_the_bits(lib, tmp_path, mon
 @pytest.mark.gpu
 @pytest.mark.parametrize("which", ["board", "lossy"])
 def test_z_tails_give_the_bits_of_general_blocks(lib, monkeypatch, which):
-    """The z CPML slab run inside the lean kernels' rows (z tails, the
-    default from 2 M cells, forced here), as separate general blocks
-    (CEM_B200_ZTAIL=0), and inside whole E rows of the Debye space
-    (CEM_B200_ROWS=1) give the same fields and spectra bit for bit, on a
+    """The z CPML slab run inside the lean kernels' rows (z tails,
+    CEM_B200_ZTAIL=1), as rectangles of their own in the lean space
+    (CEM_B200_ZTAIL=2, the form of the default from 2 M cells), as separate
+    general blocks (CEM_B200_ZTAIL=0), and inside whole E rows of the Debye
+    space (CEM_B200_ROWS=1) give the same fields and spectra bit for bit, on a
     seeded board (z-high CPML above air, Debye cores below) and on the lossy
     scene."""
     from courant_b200 import boards
@@ -152,19 +153,20 @@ def test_z_tails_give_the_bits_of_general_blocks(lib, monkeypatch, which):
             return boards.seeded_board(lib, seed=78, cells=3e5, ports="mode", nf=4, steps=1200)
         return scenes.lossy_scene(lib)
     runs = []
-    for zt, rows in (("1", "0"), ("0", "0"), ("1", "1")):
+    for zt, rows in (("1", "0"), ("0", "0"), ("1", "1"), ("2", "0")):
         monkeypatch.setenv("CEM_B200_ZTAIL", zt)
         monkeypatch.setenv("CEM_B200_ROWS", rows)
         s, meta = make()
         s.step(1200)
         runs.append((s, meta))
-    (a, ma), (b, _), (w, _) = runs
+    (a, ma), (b, _), (w, _), (t, _) = runs
     za, zb = a.sizes(), b.sizes()
     assert za["h_general_pts"] < zb["h_general_pts"]
     if which == "board":
         assert za["e_general_pts"] < zb["e_general_pts"]
         assert w.sizes()["e_fast_pts"] < za["e_fast_pts"]     # whole rows: the air above the cores in the Debye space
-    for x in (b, w):
+    assert t.sizes()["e_general_pts"] == za["e_general_pts"]
+    for x in (b, w, t):
         for c in range(6):
             assert np.array_equal(a.field(c), x.field(c)), c
         if "modeports" in ma:
@@ -172,5 +174,5 @@ def test_z_tails_give_the_bits_of_general_blocks(lib, monkeypatch, which):
                 assert np.array_equal(a.modePortWaves(p)["b"], x.modePortWaves(p)["b"])
         for p in ma.get("ports", []):
             assert np.array_equal(a.portV(p), x.portV(p))
-    for x in (a, b, w):
+    for x in (a, b, w, t):
         x.destroy()
