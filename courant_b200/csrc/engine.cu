@@ -944,10 +944,10 @@ __device__ __forceinline__ void e_lean(const StepArgs &a, int i, const RowPos &p
 
 // E component C at points k4 .. k4+3 of row (i, j) of a Debye piece: no
 // CPML auxiliary on a derivative axis but the z slab of a z tail (whose
-// groups take e_points), the points in or beside the component's Debye box. The P pole currents of the four points are read
-// once as float4 and kept in registers for both sum_p hk_p J_p and their own
-// update, then written once; beta_p/dt comes packed per table entry. Every
-// rounding is that of e_points.
+// groups take e_points), the points in or beside the component's Debye box.
+// The P pole currents of the four points are read once as float4 and kept in
+// registers for both sum_p hk_p J_p and their own update, then written once;
+// beta_p/dt comes packed per table entry. Every rounding is that of e_points.
 template <int C, int P>
 __device__ __forceinline__ void e_debye(const StepArgs &a, int i, const RowPos &p, const float2 sv) {
     constexpr int A1 = (C + 1) % 3, A2 = (C + 2) % 3;
@@ -1777,7 +1777,7 @@ struct Device {
     bool side_on = true;
     int graph_steps = 32;
     // the z CPML slabs run inside the lean kernels' rows (z tails) or as general blocks;
-    // by default tails from 2 M cells (CEM_B200_ZTAIL=0/1 forces): on smaller grids the lean
+    // by default tails from 2 M cells (CEM_B200_ZTAIL=0/1/2 forces): on smaller grids the lean
     // and general kernels each fit in a wave or two and run side by side, and keeping the
     // slab apart balances the two streams (121 x 62 x 40 line: 16.3 against 18.2 us per step;
     // 1498 x 1014 x 64 board: 3.21 against 3.01 ms)
@@ -3235,10 +3235,10 @@ void load_shapes() {   // g_shape_mu held
     g_shape_loaded = true;
     FILE *f = std::fopen(shape_cache_path().c_str(), "r");
     if (!f) return;
-    // lines: key thin side graph ms [ztail] (lines without the z-tail choice keep the default)
+    // lines: key thin side graph ms [ztail] (lines without the z-tail choice keep the default: -1)
     char line[400], key[200];
     while (std::fgets(line, sizeof line, f)) {
-        double v[5] = {0, 0, 0, 0, 1};
+        double v[5] = {0, 0, 0, 0, -1};
         if (std::sscanf(line, "%199s %lf %lf %lf %lf %lf", key, &v[0], &v[1], &v[2], &v[3], &v[4]) >= 5)
             g_shapes[key] = {v[0], v[1], v[2], v[3], v[4]};
     }
@@ -3304,7 +3304,8 @@ bool tune_shape(cem_sim *s, long *used) {
     if (it != g_shapes.end()) {
         D.tuned_from_cache = true;
         D.tuned_ms = it->second[3];
-        return apply_shape(s, D, (int)it->second[0], it->second[1] != 0, (int)it->second[2], it->second[4] != 0);
+        const bool zt = it->second[4] < 0 ? D.ztail : it->second[4] != 0;
+        return apply_shape(s, D, (int)it->second[0], it->second[1] != 0, (int)it->second[2], zt);
     }
     int thin = D.thin, graph = D.graph_steps;
     bool side = D.side_on, zt = D.ztail;
