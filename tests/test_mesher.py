@@ -69,3 +69,39 @@ def test_large_board_layout_is_the_large_configuration():
     assert len(geo.traces) == 20 and len(geo.vias) == 30
     for v in (x, y, z):
         assert np.all(np.diff(v) > 0)
+
+
+def test_board_port_counts_and_windows():
+    """1 to 4 ports: ports 1 and 2 on trace 0 (L4) with the whole cross-section, ports 3 and 4 on the
+    second port trace (L3), whose window stops short of trace 0; an excitation outside the ports is refused."""
+    one = boards.plan_board(41, 2e5, ports="mode", nf=2, nports=1)
+    four = boards.plan_board(41, 2e5, ports="mode", nf=2, nports=4, excite=3)
+    ny = len(four.y) - 1
+    assert len(one.port) == 1 and len(four.port) == 4
+    assert [p["end"] for p in four.port] == [0, 1, 0, 1]
+    for p in four.port[:2]:
+        assert (p["j0"], p["j1"]) == (0, ny) and p["vk1"] == four.kl[3]
+    p3 = four.port[2]
+    assert p3["vk1"] == four.kl[2] and (p3["j0"] > 0) != (p3["j1"] < ny)      # one wall, on trace 0's side
+    assert not p3["j0"] <= four.port[0]["vj"] < p3["j1"]                     # trace 0 outside the window
+    assert p3["neff0"] > four.port[0]["neff0"]                               # the covered line is slower
+    for bad in (dict(nports=0), dict(nports=5), dict(nports=2, excite=3)):
+        with pytest.raises(ValueError):
+            boards.plan_board(41, 2e5, ports="mode", nf=2, **bad)
+
+
+def test_s_column_takes_every_port():
+    """The excited column of the S-matrix holds one wave per port (lumped ports at 50 ohm)."""
+    from courant_b200 import scenes
+
+    class Fake:
+        def portV(self, p):
+            return np.array([1.0 + p, 2.0])
+
+        def portI(self, p):
+            return np.array([0.01 * (p + 1), 0.02])
+    for n in (1, 3, 4):
+        col = scenes.s_column(Fake(), {"ports": list(range(n)), "excite": 1})
+        assert len(col["b"]) == n
+        a = (1.0 + 50 * 0.01) / (2 * np.sqrt(50))
+        assert np.isclose(col["b"][0][0], (1.0 - 50 * 0.01) / (2 * np.sqrt(50)) / a)
