@@ -342,6 +342,15 @@ void magnetic_field(cem_mode2d &m, const Coeffs &c, double w) {
 
 namespace cb2 {
 double mode_freq_hint(const cem_mode2d *m) { return m->freq; }
+
+void mode2d_copy_mode(cem_mode2d *dst, const cem_mode2d *src) {
+    dst->freq = src->freq;
+    dst->beta = src->beta;
+    dst->eu = src->eu;
+    dst->ev = src->ev;
+    dst->hu = src->hu;
+    dst->hv = src->hv;
+}
 }
 
 extern "C" {

@@ -126,45 +126,53 @@ namespace {
 // tracked; kappa -> beta by the arcsine mapping of the leapfrog grid, Z0 from
 // the mode's own V and I. (reference modeport.c:146-201)
 //
-// The upward and the downward walk each start with a fresh solve at the
-// frequency nearest f0 and share nothing else, so they run on two threads,
-// each with its own cross-section; the downward walk keeps the port's own
-// cross-section, which ends on the lowest frequency's mode as in a walk up
-// then down. Both walks compute the starting frequency alike; the upward
-// one stores it.
-int port_sweep(const cem_sim *s, ModePort &p, cem_mode2d *xs, int q0, int stepq) {
-    const int nf = s->nf;
+// The walk starts with a fresh solve at the frequency nearest f0 and a solve
+// seeded with it there, as both of the reference's passes do; their results
+// are the same, so they run once, on the port's own cross-section, and the
+// upward walk continues on a second cross-section given a copy of that mode,
+// on its own thread, while the downward walk continues on the port's own one,
+// which ends on the lowest frequency's mode as in a walk up then down.
+
+// the seeded solve at frequency q from xs's last mode, and the port's figures there
+int port_step(const cem_sim *s, ModePort &p, cem_mode2d *xs, int q, std::vector<double> &start) {
     const cem_mode_port_def &d = p.def;
     const int ny = d.j1 - d.j0, nz = d.k1 - d.k0;
-    const int nst = ny * (nz + 1) + (ny + 1) * nz;
-    std::vector<double> start(2 * (size_t)nst);
     const double dx = s->d[0][d.i_mon];
-    cem_mode2d_solve(xs, warp(s, s->freq[q0]), d.neff0, nullptr, 300, 1e-13);
-    for (int q = q0; q >= 0 && q < nf; q += stepq) {
-        const double fw = warp(s, s->freq[q]);
-        const double ng = cem_mode2d_beta(xs) / (2 * M_PI * mode_freq_hint(xs) / CEM_C0);
-        std::memcpy(start.data(), cem_mode2d_eu(xs), 2 * ny * (nz + 1) * sizeof(double));
-        std::memcpy(start.data() + 2 * ny * (nz + 1), cem_mode2d_ev(xs), 2 * (ny + 1) * nz * sizeof(double));
-        if (cem_mode2d_solve(xs, fw, ng, start.data(), 300, 1e-13)) return -1;
-        if (stepq < 0 && q == q0) continue;
-        const cplx kc = cem_mode2d_beta(xs) - cplx(0.0, 1.0) * cem_mode2d_alpha(xs);
-        const cplx b3 = 2 / dx * std::asin(kc * dx / 2.0);
-        p.kappa[2 * q] = std::real(kc); p.kappa[2 * q + 1] = std::imag(kc);
-        p.beta[q] = std::real(b3);
-        p.alpha[q] = -std::imag(b3);
-        if (s->sibc_on) {
-            double zr, zi;
-            cem_conductor_zs(s, s->freq[q], &zr, &zi);
-            p.alpha_c[q] = cem_mode2d_conductor_alpha(xs, zr);
-            p.alpha[q] += p.alpha_c[q];
-        }
-        double V[2], Iv[2];
-        cem_mode2d_vi(xs, d.vj - d.j0, d.vk0 - d.k0, d.vk1 - d.k0, d.ja - d.j0, d.jb - d.j0, d.ka - d.k0, d.kb - d.k0,
-                      V, Iv);
-        // cem_mode2d_vi returns -sum Ez dz; the port voltage is vsign * sum Ez dz
-        const cplx Z = (double)(-d.vsign) * cplx(V[0], V[1]) / cplx(Iv[0], Iv[1]);
-        p.z0[2 * q] = std::real(Z); p.z0[2 * q + 1] = std::imag(Z);
+    const double fw = warp(s, s->freq[q]);
+    const double ng = cem_mode2d_beta(xs) / (2 * M_PI * mode_freq_hint(xs) / CEM_C0);
+    std::memcpy(start.data(), cem_mode2d_eu(xs), 2 * ny * (nz + 1) * sizeof(double));
+    std::memcpy(start.data() + 2 * ny * (nz + 1), cem_mode2d_ev(xs), 2 * (ny + 1) * nz * sizeof(double));
+    if (cem_mode2d_solve(xs, fw, ng, start.data(), 300, 1e-13)) return -1;
+    const cplx kc = cem_mode2d_beta(xs) - cplx(0.0, 1.0) * cem_mode2d_alpha(xs);
+    const cplx b3 = 2 / dx * std::asin(kc * dx / 2.0);
+    p.kappa[2 * q] = std::real(kc); p.kappa[2 * q + 1] = std::imag(kc);
+    p.beta[q] = std::real(b3);
+    p.alpha[q] = -std::imag(b3);
+    if (s->sibc_on) {
+        double zr, zi;
+        cem_conductor_zs(s, s->freq[q], &zr, &zi);
+        p.alpha_c[q] = cem_mode2d_conductor_alpha(xs, zr);
+        p.alpha[q] += p.alpha_c[q];
     }
+    double V[2], Iv[2];
+    cem_mode2d_vi(xs, d.vj - d.j0, d.vk0 - d.k0, d.vk1 - d.k0, d.ja - d.j0, d.jb - d.j0, d.ka - d.k0, d.kb - d.k0,
+                  V, Iv);
+    // cem_mode2d_vi returns -sum Ez dz; the port voltage is vsign * sum Ez dz
+    const cplx Z = (double)(-d.vsign) * cplx(V[0], V[1]) / cplx(Iv[0], Iv[1]);
+    p.z0[2 * q] = std::real(Z); p.z0[2 * q + 1] = std::imag(Z);
+    return 0;
+}
+
+std::vector<double> start_buffer(const ModePort &p) {
+    const int ny = p.def.j1 - p.def.j0, nz = p.def.k1 - p.def.k0;
+    return std::vector<double>(2 * (size_t)(ny * (nz + 1) + (ny + 1) * nz));
+}
+
+// frequencies q0, q0 + stepq, ... to the end of the list, each seeded with the previous mode
+int port_walk(const cem_sim *s, ModePort &p, cem_mode2d *xs, int q0, int stepq) {
+    std::vector<double> start = start_buffer(p);
+    for (int q = q0; q >= 0 && q < s->nf; q += stepq)
+        if (port_step(s, p, xs, q, start)) return -1;
     return 0;
 }
 
@@ -179,17 +187,22 @@ int solve_port_modes(cem_sim *s, ModePort &p) {
     int q0 = 0;
     for (int q = 0; q < nf; q++)
         if (std::fabs(s->freq[q] - d.f0) < std::fabs(s->freq[q0] - d.f0)) q0 = q;
-    cem_mode2d *up = cem_cross_section_x(s, d.i_mon, d.j0, d.j1, d.k0, d.k1);
-    if (!up) return -1;
-    int rc_up = 0;
-    std::thread t([&] { rc_up = port_sweep(s, p, up, q0, 1); });
-    const int rc_down = port_sweep(s, p, p.xs, q0, -1);
-    t.join();
-    cem_mode2d_destroy(up);
-    if (rc_up || rc_down) {
+    auto fail = [] {
         set_error("mode port: eigenmode did not converge at an output frequency");
         return -1;
-    }
+    };
+    std::vector<double> start = start_buffer(p);
+    cem_mode2d_solve(p.xs, warp(s, s->freq[q0]), d.neff0, nullptr, 300, 1e-13);
+    if (port_step(s, p, p.xs, q0, start)) return fail();
+    cem_mode2d *up = cem_cross_section_x(s, d.i_mon, d.j0, d.j1, d.k0, d.k1);
+    if (!up) return -1;
+    mode2d_copy_mode(up, p.xs);
+    int rc_up = 0;
+    std::thread t([&] { rc_up = port_walk(s, p, up, q0 + 1, 1); });
+    const int rc_down = port_walk(s, p, p.xs, q0 - 1, -1);
+    t.join();
+    cem_mode2d_destroy(up);
+    if (rc_up || rc_down) return fail();
     p.solved = true;
     return 0;
 }

@@ -166,6 +166,8 @@ void modeports_release(cem_sim *s);
 double mode_source_value(const cem_sim *s, double t);
 double lumped_source_value(const cem_sim *s, double t);
 double mode_freq_hint(const cem_mode2d *m);
+// the last mode of src (frequency, beta, fields) into dst, a cross-section of the same geometry
+void mode2d_copy_mode(cem_mode2d *dst, const cem_mode2d *src);
 void nnls(int m, int n, const double *A, const double *b, double *x);
 
 // Host views of time-dependent state. Groups let the engine move only what a
