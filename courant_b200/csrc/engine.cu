@@ -1954,10 +1954,17 @@ bool build_tables(cem_sim *s, Device &D) {
         for (size_t e = 0; e < pt.edge.size(); e++) src[pt.axis].push_back({pt.edge[e], pt.cs[e]});
     }
     std::vector<std::vector<std::pair<size_t, int>>> disp(3);
+    {
+        size_t count[3] = {0, 0, 0};
+        for (int e = 0; e < s->ndisp; e++) count[s->d_comp[e]]++;
+        for (int c = 0; c < 3; c++) disp[c].reserve(count[c]);
+    }
     for (int e = 0; e < s->ndisp; e++) disp[s->d_comp[e]].push_back({s->d_idx[e], e});
+    auto by_index = [](const auto &x, const auto &y) { return x.first < y.first; };
     for (int c = 0; c < 3; c++) {   // stable: of equal indices the last one counts, as a map assignment would
-        std::stable_sort(src[c].begin(), src[c].end(), [](const auto &x, const auto &y) { return x.first < y.first; });
-        std::stable_sort(disp[c].begin(), disp[c].end(), [](const auto &x, const auto &y) { return x.first < y.first; });
+        std::stable_sort(src[c].begin(), src[c].end(), by_index);
+        if (!std::is_sorted(disp[c].begin(), disp[c].end(), by_index))   // finalize lists them in index order
+            std::stable_sort(disp[c].begin(), disp[c].end(), by_index);
     }
     // mode-source weights of Ey, Ez on the source plane (reference index j*(nz+1)+k)
     int msrc_i = -1;
@@ -1990,7 +1997,7 @@ bool build_tables(cem_sim *s, Device &D) {
     std::vector<std::unique_ptr<Built>> out;
     for (int c = 0; c < 3; c++) {
         out.emplace_back(new Built(nfields));
-        out[c]->mat.assign(D.Np, 0);
+        big_assign(out[c]->mat, (size_t)D.Np, (unsigned short)0);
     }
     const int nthreads = (int)std::max(1u, std::min(std::thread::hardware_concurrency(), 32u));
     const int nslab = std::max(1, std::min(n[0] + 1, nthreads));

@@ -17,7 +17,26 @@
 #include <string>
 #include <vector>
 
+#include <sys/mman.h>
+
 namespace cb2 {
+
+// A large host array set to n copies of val: capacity reserved first (fresh
+// pages, untouched), advised for transparent huge pages, then filled, so that
+// its first touch faults in 2 MB pages instead of 4 kB ones (set-up of a
+// large grid otherwise spends most of its time in page faults).
+template <class T>
+void big_assign(std::vector<T> &v, size_t n, const T &val) {
+    std::vector<T>().swap(v);
+    v.reserve(n);
+    constexpr uintptr_t kHuge = (uintptr_t)2 << 20;
+    if (n * sizeof(T) >= 2 * kHuge) {
+        const uintptr_t b = reinterpret_cast<uintptr_t>(v.data());
+        const uintptr_t a = (b + kHuge - 1) & ~(kHuge - 1), e = (b + n * sizeof(T)) & ~(kHuge - 1);
+        if (e > a) madvise(reinterpret_cast<void *>(a), e - a, MADV_HUGEPAGE);
+    }
+    v.assign(n, val);
+}
 
 // Limits of the reference core (sim_internal.h:14-15,42-43); kept so the same
 // programs hit the same errors.

@@ -9,6 +9,8 @@
 #include "sim.hpp"
 
 #include <algorithm>
+#include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -186,10 +188,10 @@ cem_sim *cem_create(int nx, int ny, int nz, const double *x, const double *y, co
         s->sj = (size_t)nz + 1;
         s->si = s->sj * ((size_t)ny + 1);
         s->N = s->si * ((size_t)nx + 1);
-        s->eps_r.assign(s->N, 1.0);
-        s->sigma.assign(s->N, 0.0);
-        s->cell_pec.assign(s->N, 0);
-        for (int c = 0; c < 3; c++) s->edge_pec[c].assign(s->N, 0);
+        big_assign(s->eps_r, s->N, 1.0);
+        big_assign(s->sigma, s->N, 0.0);
+        big_assign(s->cell_pec, s->N, (uint8_t)0);
+        for (int c = 0; c < 3; c++) big_assign(s->edge_pec[c], s->N, (uint8_t)0);
     } catch (const std::bad_alloc &) {
         delete s;
         set_error("out of memory");
@@ -371,7 +373,7 @@ int cem_set_debye_poles(cem_sim *s, int npole, const double *f_p) {
     try {
         for (int p = 0; p < npole; p++) {
             s->pole_f[p] = f_p[p];
-            s->cell_deps[p].assign(s->N, 0.0);
+            big_assign(s->cell_deps[p], s->N, 0.0);
         }
     } catch (const std::bad_alloc &) {
         set_error("out of memory");
@@ -574,6 +576,15 @@ extern "C" {
 
 int cem_finalize(cem_sim *s, double cfl) {
     if (s->finalized) { set_error("already finalized"); return -1; }
+    // CEM_B200_TRACE=1: seconds per set-up stage on stderr
+    static const bool trace = [] { const char *e = std::getenv("CEM_B200_TRACE"); return e && e[0] == '1'; }();
+    auto t_last = std::chrono::steady_clock::now();
+    auto tick = [&](const char *what) {
+        if (!trace) return;
+        const auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "courant-b200: finalize %s %.3f s\n", what, std::chrono::duration<double>(now - t_last).count());
+        t_last = now;
+    };
     try {
         if (!s->nf) {
             const double f = 1e9;
@@ -589,13 +600,14 @@ int cem_finalize(cem_sim *s, double cfl) {
         s->has_pml = 0;
         for (int f = 0; f < 6; f++)
             if (s->npml[f]) s->has_pml = 1;
+        tick("cpml profiles");
 
         const int nx = s->n[0], ny = s->n[1], nz = s->n[2];
         // per-edge coefficients, lossy dielectric by the semi-implicit average
         // (reference sim.c:450-465); every edge on its own, node planes in parallel
         for (int c = 0; c < 3; c++) {
-            s->ca[c].assign(s->N, 0.0);
-            s->cb[c].assign(s->N, 0.0);
+            big_assign(s->ca[c], s->N, 0.0);
+            big_assign(s->cb[c], s->N, 0.0);
         }
         parallel_planes(nx + 1, [&](int i0, int i1) {
             for (int c = 0; c < 3; c++)
@@ -615,6 +627,7 @@ int cem_finalize(cem_sim *s, double cfl) {
                         }
         });
 
+        tick("edge coefficients");
         // lumped ports: resistive voltage source spread over the column's edges
         // (reference sim.c:468-492)
         for (LumpedPort &pt : s->port) {
@@ -643,7 +656,7 @@ int cem_finalize(cem_sim *s, double cfl) {
 
         std::vector<uint8_t> is_port;
         if (!s->port.empty() && (s->npole || s->sibc_on)) {
-            is_port.assign(s->N * 3, 0);
+            big_assign(is_port, s->N * 3, (uint8_t)0);
             for (const LumpedPort &pt : s->port)
                 for (size_t q : pt.edge) is_port[pt.axis * s->N + q] = 1;
         }
@@ -651,21 +664,14 @@ int cem_finalize(cem_sim *s, double cfl) {
         // Debye edges: eps -> eps_inf eps0 + sum beta_p / 2 in ca/cb, ADE tables.
         // Lumped-port edges keep their own coefficients. (reference sim.c:501-549)
         if (s->npole) {
-            // each (component, slab of node planes) lists its Debye edges on its own;
-            // the lists join in component, then plane order: the reference's edge order
-            struct Part {
-                std::vector<int> comp;
-                std::vector<size_t> idx;
-                std::vector<double> cbv;
-                std::vector<std::vector<double>> beta;
-            };
+            // each (component, slab of node planes) counts its Debye edges, then
+            // writes them at its offset in the final lists: the lists join in
+            // component, then plane order, the reference's edge order
             const int nslab = std::max(1, std::min(nx + 1, 4 * plane_threads()));
-            std::vector<Part> parts(3 * (size_t)nslab);
-            parallel_tasks((int)parts.size(), [&](int t) {
+            const int ntask = 3 * nslab;
+            auto walk = [&](int t, auto &&edge) {
                 const int c = t / nslab, sl = t % nslab;
                 const int i0 = (int)((long long)(nx + 1) * sl / nslab), i1 = (int)((long long)(nx + 1) * (sl + 1) / nslab);
-                Part &pt = parts[t];
-                pt.beta.resize(s->npole);
                 double dep[kMaxPoles];
                 for (int i = i0; i < i1; i++)
                     for (int j = 0; j <= ny; j++)
@@ -675,49 +681,52 @@ int cem_finalize(cem_sim *s, double cfl) {
                             const size_t q = idx3(s, i, j, k);
                             if (s->cb[c][q] == 0 || (!is_port.empty() && is_port[c * s->N + q])) continue;
                             if (!edge_debye(s, c, i, j, k, dep)) continue;
-                            double er, sg;
-                            int pec;
-                            edge_material(s, c, i, j, k, &er, &sg, &pec);
-                            double einst = er * CEM_EPS0;
-                            for (int p = 0; p < s->npole; p++) {
-                                const double tau = 1.0 / (2 * M_PI * s->pole_f[p]);
-                                const double bt = CEM_EPS0 * dep[p] * s->dt / (tau * (1 + s->dt / (2 * tau)));
-                                pt.beta[p].push_back(bt);
-                                einst += 0.5 * bt;
-                            }
-                            const double h = sg * s->dt / (2 * einst);
-                            s->ca[c][q] = (1 - h) / (1 + h);
-                            s->cb[c][q] = (s->dt / einst) / (1 + h);
-                            pt.comp.push_back(c);
-                            pt.idx.push_back(q);
-                            pt.cbv.push_back(s->cb[c][q]);
+                            edge(c, i, j, k, q, dep);
                         }
+            };
+            std::vector<size_t> first(ntask + 1, 0);
+            parallel_tasks(ntask, [&](int t) {
+                size_t n = 0;
+                walk(t, [&](int, int, int, int, size_t, const double *) { n++; });
+                first[t + 1] = n;
             });
-            size_t total = 0;
-            for (const Part &pt : parts) total += pt.idx.size();
+            for (int t = 0; t < ntask; t++) first[t + 1] += first[t];
+            const size_t total = first[ntask];
             s->ndisp = (int)total;
-            s->d_comp.clear();
-            s->d_idx.clear();
-            s->d_cb.clear();
-            s->d_comp.reserve(total);
-            s->d_idx.reserve(total);
-            s->d_cb.reserve(total);
-            s->d_beta.assign((size_t)s->npole * s->ndisp, 0.0);
-            size_t at = 0;
-            for (const Part &pt : parts) {
-                s->d_comp.insert(s->d_comp.end(), pt.comp.begin(), pt.comp.end());
-                s->d_idx.insert(s->d_idx.end(), pt.idx.begin(), pt.idx.end());
-                s->d_cb.insert(s->d_cb.end(), pt.cbv.begin(), pt.cbv.end());
-                for (int p = 0; p < s->npole; p++)
-                    std::copy(pt.beta[p].begin(), pt.beta[p].end(), s->d_beta.begin() + (size_t)p * s->ndisp + at);
-                at += pt.idx.size();
-            }
+            big_assign(s->d_comp, total, 0);
+            big_assign(s->d_idx, total, (size_t)0);
+            big_assign(s->d_cb, total, 0.0);
+            big_assign(s->d_beta, (size_t)s->npole * total, 0.0);
+            parallel_tasks(ntask, [&](int t) {
+                size_t at = first[t];
+                walk(t, [&](int c, int i, int j, int k, size_t q, const double *dep) {
+                    double er, sg;
+                    int pec;
+                    edge_material(s, c, i, j, k, &er, &sg, &pec);
+                    double einst = er * CEM_EPS0;
+                    for (int p = 0; p < s->npole; p++) {
+                        const double tau = 1.0 / (2 * M_PI * s->pole_f[p]);
+                        const double bt = CEM_EPS0 * dep[p] * s->dt / (tau * (1 + s->dt / (2 * tau)));
+                        s->d_beta[(size_t)p * total + at] = bt;
+                        einst += 0.5 * bt;
+                    }
+                    const double h = sg * s->dt / (2 * einst);
+                    s->ca[c][q] = (1 - h) / (1 + h);
+                    s->cb[c][q] = (s->dt / einst) / (1 + h);
+                    s->d_comp[at] = c;
+                    s->d_idx[at] = q;
+                    s->d_cb[at] = s->cb[c][q];
+                    at++;
+                });
+            });
             for (int p = 0; p < s->npole; p++) {
                 const double tau = 1.0 / (2 * M_PI * s->pole_f[p]);
                 s->d_k[p] = (1 - s->dt / (2 * tau)) / (1 + s->dt / (2 * tau));
             }
         }
+        tick("lumped ports, Debye edges");
         if (sibc_finalize(s, is_port)) return -1;
+        tick("surface impedance");
 
         for (VoltageProbe &p : s->vp) p.acc.assign(2 * s->nf, 0.0);
         for (CurrentProbe &p : s->ip) p.acc.assign(2 * s->nf, 0.0);
@@ -728,6 +737,7 @@ int cem_finalize(cem_sim *s, double cfl) {
             s->finalized = 0;
             return -1;
         }
+        tick("mode ports");
     } catch (const std::bad_alloc &) {
         set_error("out of memory");
         return -1;
