@@ -42,7 +42,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 from pathlib import Path
 
@@ -235,7 +234,6 @@ def _compare(lib, spec, arrivals, nf) -> dict:
     S-parameters one request at a time, each waiting for its arrival) and
     through the continuously batching server; solves/hour, latencies and mean
     stage times of both, and whether every result is the same."""
-    import numpy as np
     from courant_b200 import serve
     t0 = time.perf_counter()
     plain = serve.plain_loop(lib, _mix_requests(spec, nf), list(arrivals))

@@ -20,7 +20,7 @@ import math
 
 import numpy as np
 
-from .api import C0, Courant, DebyeModel
+from .api import Courant, DebyeModel
 
 CPML = 1
 X, Y, Z = 0, 1, 2

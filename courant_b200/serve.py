@@ -27,7 +27,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .api import Courant, Sim, s_params
+from .api import Courant, Sim
 
 
 def footprint(sim: Sim) -> int:
