@@ -60,6 +60,7 @@ int finalize_port(cem_sim *s, ModePort &p) {
             if (!cem_mode2d_solve(p.xs, warp(s, d.f0), p.def.neff0 * tries[t], nullptr, 300, 1e-13)) {
                 ok = true;
                 p.def.neff0 *= tries[t];
+                p.xs_fresh_fw = warp(s, d.f0);
             }
         }
         if (!ok) {
@@ -192,7 +193,11 @@ int solve_port_modes(cem_sim *s, ModePort &p) {
         return -1;
     };
     std::vector<double> start = start_buffer(p);
-    cem_mode2d_solve(p.xs, warp(s, s->freq[q0]), d.neff0, nullptr, 300, 1e-13);
+    // the unseeded solve at the starting frequency: finalize's, when f0 is that frequency (an
+    // unseeded solve depends on nothing but the section, the frequency and the shift)
+    const double fw0 = warp(s, s->freq[q0]);
+    if (p.xs_fresh_fw != fw0) cem_mode2d_solve(p.xs, fw0, d.neff0, nullptr, 300, 1e-13);
+    p.xs_fresh_fw = -1;
     if (port_step(s, p, p.xs, q0, start)) return fail();
     cem_mode2d *up = cem_cross_section_x(s, d.i_mon, d.j0, d.j1, d.k0, d.k1);
     if (!up) return -1;

@@ -80,6 +80,7 @@ struct ModePort {
     std::vector<size_t> src_idx;
     std::vector<double> src_w;            // source profile on the i_src plane
     cem_mode2d *xs = nullptr;             // cross-section at the monitor plane
+    double xs_fresh_fw = -1;              // xs holds the unseeded solve at this warped frequency and neff0 (-1: not)
     std::vector<double> z0, kappa;        // complex, 2*nf
     std::vector<double> beta, alpha, alpha_c;
     bool solved = false;
