@@ -114,3 +114,25 @@ def test_s2_renormalize(lib, ref_lib):
         S = list(rng.normal(size=4) * 0.4 + 1j * rng.normal(size=4) * 0.4)
         z1, z2 = rng.uniform(20, 80, size=2)
         assert lib.renormalize2(S, z1, z2, 50.0) == ref_lib.renormalize2(S, z1, z2, 50.0)
+
+
+@pytest.mark.parametrize("case", ["board4", "modeport"])
+def test_mode_port_walks_against_reference(lib, ref_lib, case):
+    """Port impedance and propagation constant at every output frequency (the
+    walk outward from f0, each solve seeded with the previous mode; this
+    library solves the starting frequency once for both walks and takes
+    finalize's solve there when f0 is an output frequency) agree with the
+    reference's to rounding. No time steps are needed."""
+    from courant_b200 import boards
+
+    def make(c):
+        if case == "board4":
+            return boards.seeded_board(c, 32, 2.5e5, ports="mode", nf=8, nports=4, excite=3)
+        return scenes.modeport_scene(c)
+    (a, ma), (b, _) = make(lib), make(ref_lib)
+    for p in ma["modeports"]:
+        wa, wb = a.modePortWaves(p), b.modePortWaves(p)
+        for k in ("z0", "beta"):
+            assert np.max(np.abs(wa[k] - wb[k]) / np.abs(wb[k])) < 1e-8, (p, k)
+    a.destroy()
+    b.destroy()
